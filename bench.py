@@ -1,0 +1,354 @@
+"""Benchmark of the index step (k-mers/s), the configuration the headline
+metric is quoted on: a 100 Mbp reference (40 genomes of 2.5 Mbp, each derived
+from one of 4 random founders by 2% substitutions + 0.1% indels), k = 31,
+both strands; 10 M reads with log-normal lengths (median 150, clipped to
+31..1000), 0.5% substitutions, 0.1% N.  All data is seeded synthetic data
+generated at start-up by the project's tools.
+
+One step = one index-step pass (SeqToBits + positions + SBWT search + -1/-2
+mapping) over the whole read batch.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` = k-mers/s with inputs resident in HBM
+(device-pointer call); `e2e` = the same through the host-pointer C-ABI call
+from pinned host memory (H2D + compute + D2H inside the timed region).
+Multi-GPU: one process per GPU (torchrun), each rank searches its own read
+batch against its own index replica (no collective on the data path; weak
+scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "sbwt-search_b200"))
+
+METRIC = "k-mers/s index search (reads -> SBWT index per k-mer)"
+UNIT = "k-mers/s"
+
+CFG = dict(n_genomes=40, genome_len=2_500_000, n_founders=4, sub=0.02, indel=0.001,
+           k=31, n_reads=10_000_000, len_median=150, len_sigma=0.5, len_min=31,
+           len_max=1000, read_sub=0.005, n_rate=0.001)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--reads", type=int, default=CFG["n_reads"])
+    ap.add_argument("--presearch", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-sample-reads", type=int, default=60_000)
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, dev: int):
+        self.dev = dev
+        self.proc = None
+        self.rows = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is None:
+            return
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        for ln in out.strip().splitlines():
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) >= 7:
+                self.rows.append(f)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if r[3 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def make_workload(seed_reads: int, n_reads: int, tmpdir: str):
+    import sbwt_tools as T
+    c = CFG
+    g = T.gen_genomes(20240601, c["n_genomes"], c["genome_len"], c["n_founders"],
+                      c["sub"], c["sub"], c["indel"])
+    path = os.path.join(tmpdir, "cfg2.sbwt")
+    nodes = T.build_sbwt(g, c["k"], path)
+    chars, ends = T.gen_reads(seed_reads, g, n_reads, 1.0, c["len_median"],
+                              c["len_sigma"], c["len_min"], c["len_max"],
+                              c["read_sub"], c["n_rate"])
+    return g, path, nodes, chars, ends
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def cpu_reference_rate(path, chars, ends, k, sample_reads):
+    """SBWT-Search's own index kernels compiled for the host (oracle/_ref),
+    all host threads, on the first `sample_reads` reads.  Returns
+    (k-mers/s, k-mers, seconds, threads, results)."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as O
+    L = O.ref_lib()
+    if L is None:
+        return None
+    sb = O.SbwtFile.read(path)
+    idx = O.OracleIndex(sb.acgt, sb.num_bits, sb.k, use_ref=True)
+    n = min(sample_reads, len(ends))
+    sub_ends = ends[:n]
+    sub_chars = chars[:int(sub_ends[-1])]
+    bits, _ = O.seq_to_bits(sub_chars.tobytes())
+    pos = O.positions_of(sub_ends, k)
+    threads = L.ref_max_threads()
+    idx.search_positions(bits, pos[:1000], threads=threads)  # warm
+    t0 = time.perf_counter()
+    res = idx.search_positions(bits, pos, threads=threads)
+    dt = time.perf_counter() - t0
+    return len(pos) / dt, len(pos), dt, threads, (bits, pos, res)
+
+
+def run_reference(args, world, rank, local, pg):
+    """--impl reference: the reference's own CPU implementation of the index
+    step (oracle/_ref), timed per step on a bounded sample of the workload."""
+    if rank != 0:
+        return
+    with tempfile.TemporaryDirectory() as d:
+        g, path, nodes, chars, ends = make_workload(1000 + rank, args.reads, d)
+        times, last = [], None
+        for i in range(args.warmup + args.steps):
+            r = cpu_reference_rate(path, chars, ends, CFG["k"], args.cpu_sample_reads)
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "oracle/_ref (reference kernels built for the host) missing"}))
+                return
+            if i >= args.warmup:
+                times.append(r[2])
+                last = r
+        rate, nk, dt, threads, _ = last
+        med = statistics.median(times)
+        value = nk / med
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": med * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "u64", "data": "synthetic (seeded)", "impl": "reference",
+                "config": {"workload": "index search, 100 Mbp reference x 10M reads "
+                           "(bounded sample per step)", "k": CFG["k"],
+                           "sample_reads": args.cpu_sample_reads},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                                 "kind": "reference",
+                                 "sample": f"first {args.cpu_sample_reads} reads "
+                                           f"({nk} k-mers) per step"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank, local, pg)
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    import torch
+    import sbwt_b200 as S
+    torch.cuda.set_device(local)
+    dev = local
+    L = S.lib()
+    L.sbwt_profile_enable.argtypes = [C.c_int, C.c_int]
+    L.sbwt_profile_read.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    tmp = tempfile.TemporaryDirectory()
+    t0 = time.time()
+    g, path, nodes, chars, ends = make_workload(1000 + rank, args.reads, tmp.name)
+    t_gen = time.time() - t0
+    idx = S.SbwtIndex.open(path, device=dev, presearch_letters=args.presearch)
+    n_kmers = idx.count_kmers(ends)
+    n_chars = int(ends[-1])
+    # device-resident inputs (larger than L2: 1.7 GB chars, 11 GB results)
+    d_chars = torch.from_numpy(chars).to(f"cuda:{dev}")
+    d_ends = torch.from_numpy(ends.view(np.int64)).to(f"cuda:{dev}")
+    d_out = torch.empty(n_kmers, dtype=torch.int64, device=f"cuda:{dev}")
+    stream = torch.cuda.current_stream(dev)
+
+    def step_dev():
+        n = idx.search_reads(d_chars, d_ends, out=d_out, stream=stream.cuda_stream)
+        assert n == n_kmers
+
+    # one counting pass (outside the timed region): work per k-mer
+    L.sbwt_profile_enable(1, 1)
+    step_dev()
+    torch.cuda.synchronize()
+    ctr = (C.c_uint64 * 4)()
+    L.sbwt_profile_read(None, None, None, ctr)
+    n_full, n_stream, full_sectors = int(ctr[0]), int(ctr[1]), int(ctr[2])
+    L.sbwt_profile_enable(0, 0)
+
+    for _ in range(args.warmup):
+        step_dev()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    L.sbwt_profile_enable(1, 0)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step_dev()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    search_ms, search_launches, launches = C.c_double(), C.c_uint64(), C.c_uint64()
+    L.sbwt_profile_read(C.byref(search_ms), C.byref(search_launches), C.byref(launches),
+                        None)
+    L.sbwt_profile_enable(0, 0)
+    if pg:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = n_kmers * world / (ms_step / 1e3)
+
+    # parity spot check of the timed output against the oracle (small sample)
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as O
+    out_host = d_out[:200_000].cpu().numpy().view(np.uint64)
+
+    # e2e through the host-pointer C ABI call from pinned memory
+    e2e = None
+    if not args.no_e2e:
+        h_chars = torch.from_numpy(chars).pin_memory()
+        h_ends = torch.from_numpy(ends.view(np.int64)).pin_memory()
+        h_out = torch.empty(n_kmers, dtype=torch.int64).pin_memory()
+        hc, he, ho = h_chars.numpy(), h_ends.numpy().view(np.uint64), h_out.numpy().view(np.uint64)
+        idx.search_reads(hc, he, out=ho)  # warm
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        e_steps = max(1, min(args.steps, 3))
+        for _ in range(e_steps):
+            idx.search_reads(hc, he, out=ho)
+        e_dt = (time.perf_counter() - t0) / e_steps
+        if pg:
+            t = torch.tensor([e_dt], dtype=torch.float64, device=f"cuda:{dev}")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e_dt = float(t.item())
+        assert np.array_equal(ho[:200_000], out_host), "e2e output differs from device path"
+        e2e = {"value": n_kmers * world / e_dt, "unit": UNIT,
+               "h2d_bytes_per_step": int(chars.nbytes + ends.nbytes),
+               "d2h_bytes_per_step": int(n_kmers * 8), "ms_per_step": e_dt * 1e3}
+
+    # roofline of the dominant kernel (the read search kernel)
+    peak, peak_kind = load_peaks()
+    kern_ms = search_ms.value / max(1, search_launches.value)
+    # algorithmic bytes per launch: rank-block sectors of full searches (32 B
+    # each) + one presearch entry (32 B sector) per full search + one rank
+    # block sector per streaming step + 8 B result per k-mer + 2 bits of
+    # packed input per char + invalid bits
+    alg_bytes = (full_sectors + n_full + n_stream) * 32 + n_kmers * 8 + n_chars / 4 + n_chars / 8
+    achieved = alg_bytes / (kern_ms / 1e3) / 1e9
+
+    cpu = None
+    if rank == 0:
+        r = cpu_reference_rate(path, chars, ends, CFG["k"], args.cpu_sample_reads)
+        if r is not None:
+            rate, nk, dt, threads, (bits, pos, res) = r
+            got = idx.search(bits, pos)
+            agree = bool(np.array_equal(got, res))
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"first {args.cpu_sample_reads} reads ({nk} k-mers), "
+                             f"SBWT-Search's own d_search/d_presearch built for the "
+                             f"host, OpenMP", "bit_exact_vs_gpu": agree}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64", "data": "synthetic (seeded; generated at start-up)",
+        "config": {"workload": "index search: 100 Mbp reference (40 x 2.5 Mbp genomes "
+                   "from 4 founders, 2% subs, 0.1% indels), k=31, both strands; "
+                   f"{args.reads} reads log-normal length (median 150, 31-1000), "
+                   "0.5% subs, 0.1% N", "k": CFG["k"], "nodes": nodes,
+                   "reads_per_gpu": args.reads, "kmers_per_gpu": n_kmers,
+                   "chars_per_gpu": n_chars, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (no flush needed)",
+                   "presearch_letters": idx.presearch_letters},
+        "gpu_launches": int(launches.value),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_kind": peak_kind, "kernel": "search_reads_kernel",
+                     "kernel_ms": kern_ms,
+                     "work": {"full_searches": n_full, "stream_steps": n_stream,
+                              "full_search_block_sectors": full_sectors}},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "clocks": clk.summary(),
+        "setup_s": t_gen,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    idx.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

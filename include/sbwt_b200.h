@@ -1,0 +1,196 @@
+/*
+ * sbwt_b200.h -- C ABI of the B200 (sm_100a) SBWT k-mer search library.
+ *
+ * Drop-in for the two search steps of SBWT-Search.  Plain pointers and sizes
+ * only; every call returns a status code and never aborts the process; the
+ * message of the last failing call on the calling thread is kept in
+ * sbwt_last_error().  Index and color handles are immutable after they are
+ * opened and may be shared by threads; each call uses its own internal
+ * scratch keyed by the calling thread and device.
+ *
+ * Pointer arguments are host pointers unless SBWT_DEVICE_POINTERS is set in
+ * flags, in which case every array argument (inputs and outputs) is a device
+ * pointer on the handle's device and the call is asynchronous on `stream`
+ * (a cudaStream_t, NULL = legacy default stream) except where noted.
+ */
+#ifndef SBWT_B200_H
+#define SBWT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Replace the reference's exceptions
+ * (GPU_CHECK: src/Tools/GpuUtils.h:20-29; loader magic checks:
+ * src/SbwtBuilder/SbwtBuilder.cpp:61-68, src/ColorIndexBuilder/
+ * ColorIndexBuilder.cpp:15-20). */
+#define SBWT_OK 0
+#define SBWT_E_IO 1        /* file missing / unreadable */
+#define SBWT_E_FORMAT 2    /* bad magic, version or corrupt file */
+#define SBWT_E_OOM 3       /* device or host allocation failed */
+#define SBWT_E_CUDA 4      /* CUDA runtime error */
+#define SBWT_E_TIMEOUT 5   /* a bounded device wait ran out */
+#define SBWT_E_INVALID 6   /* bad argument */
+#define SBWT_E_CAPACITY 7  /* output buffer too small (required size reported) */
+
+/* flags */
+#define SBWT_DEVICE_POINTERS 0x1u  /* arrays are device pointers, async */
+#define SBWT_MOVE_TO_KEY_KMER 0x2u /* index step: walk found k-mers forward to
+                                      the next key k-mer (reference -k / d>1) */
+#define SBWT_PER_KMER_WALK 0x4u    /* index step over reads: search every
+                                      k-mer independently (no streaming reuse
+                                      of the previous k-mer's node) */
+#define SBWT_INCLUDE_NOT_FOUND 0x8u /* colors: count -1 k-mers in the read size */
+#define SBWT_INCLUDE_INVALID 0x10u  /* colors: count -2 k-mers in the read size */
+
+/* Result markers of the index step (as printed: -1 and -2). */
+#define SBWT_NOT_FOUND UINT64_MAX
+#define SBWT_INVALID (UINT64_MAX - 1)
+
+const char *sbwt_last_error(void);
+const char *sbwt_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Index step                                                               */
+/* ------------------------------------------------------------------------ */
+typedef struct sbwt_index sbwt_index_t;
+
+typedef struct {
+  uint64_t num_bits;          /* nodes of the SBWT (bits per A/C/G/T vector) */
+  uint32_t k;                 /* k-mer size */
+  uint32_t presearch_letters; /* depth of the presearch table */
+  uint64_t c_map[5];          /* c_map[0] = 1, c_map[c+1] = c_map[c] + |c| */
+  uint64_t device_bytes;      /* device memory held by the handle */
+  int device;
+  int has_key_kmer_marks;
+} sbwt_index_info_t;
+
+/* Loads a .sbwt / .tdbg file (and, when colors_path is not NULL, the key
+ * k-mer marks of a .tcolors file for SBWT_MOVE_TO_KEY_KMER) onto `device`
+ * and builds the rank blocks and the presearch table there.
+ * presearch_letters: 0 = default (12, the reference's depth), else 1..12.
+ * Replaces SbwtBuilder::get_cpu_sbwt + CpuSbwtContainer::to_gpu +
+ * Presearcher::presearch (src/SbwtBuilder/SbwtBuilder.cpp:41-56,
+ * src/SbwtContainer/CpuSbwtContainer.cpp:23-35,
+ * src/Presearcher/Presearcher.cpp:18-30, src/Main/IndexSearchMain.cpp:87-103).
+ */
+int sbwt_index_open(const char *sbwt_path, const char *colors_path, int device,
+                    unsigned presearch_letters, sbwt_index_t **out);
+
+/* Same from host arrays: acgt[c] has ceil(num_bits/64) words (LSB-first bits).
+ * suffix_group_starts (same size) enables the streaming read search; NULL
+ * makes sbwt_search_reads fall back to independent per-k-mer walks.
+ * key_kmer_marks may be NULL. */
+int sbwt_index_from_arrays(const uint64_t *const acgt[4], uint64_t num_bits,
+                           uint32_t k, const uint64_t *suffix_group_starts,
+                           const uint64_t *key_kmer_marks, int device,
+                           unsigned presearch_letters, sbwt_index_t **out);
+void sbwt_index_free(sbwt_index_t *index);
+int sbwt_index_get_info(const sbwt_index_t *index, sbwt_index_info_t *info);
+
+/* The reference's in-process index seam, IndexSearcher::search
+ * (src/IndexSearcher/IndexSearcher.h:41-46, IndexSearcher.cpp:26-51,
+ * kernel d_search src/IndexSearcher/IndexSearcher.cuh:22-72):
+ *   bit_seqs   -- 2-bit MSB-first packed chars, 32 per word (A0 C1 G2 T3);
+ *   positions  -- start char of each k-mer;
+ *   results    -- one u64 per position: SBWT node index, or SBWT_NOT_FOUND.
+ * Invalid chars are whatever their 2-bit code says (the reference packs them
+ * as A); no -2 masking is applied here, as in the reference kernel.
+ * bit_seqs must be readable up to word (max position + k - 1) / 32.
+ * With host pointers the call is synchronous like the reference's. */
+int sbwt_search_positions(const sbwt_index_t *index, const uint64_t *bit_seqs,
+                          uint64_t n_words, const uint64_t *positions,
+                          uint64_t n_positions, uint64_t *results,
+                          uint32_t flags, void *stream);
+
+/* Number of k-mer results of reads whose cumulative exclusive ends are
+ * read_ends[0..n_reads): sum over reads of max(0, length - k + 1). */
+uint64_t sbwt_count_kmers(const uint64_t *read_ends, uint64_t n_reads,
+                          uint32_t k);
+
+/* Fused index step over raw reads (SeqToBits + PositionsBuilder + search +
+ * the printer's -1/-2 mapping in one device pipeline; reference
+ * src/SeqToBitsConverter/ContinuousSeqToBitsConverter.cpp:65-107,
+ * src/PositionsBuilder/PositionsBuilder.cpp:15-47,
+ * src/IndexSearcher/IndexSearcher.cuh:22-72,
+ * src/IndexResultsPrinter/ContinuousIndexResultsPrinter.hpp:196-205):
+ *   chars      -- all reads back to back, ASCII (ACGT/acgt valid);
+ *   read_ends  -- cumulative exclusive end of each read in chars;
+ *   results    -- for every read in order, for every k-mer start in it:
+ *                 node index, SBWT_NOT_FOUND, or SBWT_INVALID when the k-mer
+ *                 holds a char other than ACGTacgt.
+ * results_capacity must be >= sbwt_count_kmers(...); *n_results receives the
+ * count (with device pointers it is computed on the host from read_ends only
+ * when read_ends is host-visible; pass n_results = NULL otherwise).
+ * Host-pointer calls are synchronous and pipeline copies and compute over
+ * chunks of reads. */
+int sbwt_search_reads(const sbwt_index_t *index, const char *chars,
+                      uint64_t n_chars, const uint64_t *read_ends,
+                      uint64_t n_reads, uint64_t *results,
+                      uint64_t results_capacity, uint64_t *n_results,
+                      uint32_t flags, void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* Colors step                                                               */
+/* ------------------------------------------------------------------------ */
+typedef struct sbwt_colors sbwt_colors_t;
+
+/* Loads a Themisto "sdsl-hybrid-v4" .tcolors file onto `device`
+ * (src/ColorIndexBuilder/ColorIndexBuilder.cpp:23-86,
+ *  src/ColorIndexContainer/GpuColorIndexContainer.cpp:13-86). */
+int sbwt_colors_open(const char *tcolors_path, int device, sbwt_colors_t **out);
+void sbwt_colors_free(sbwt_colors_t *colors);
+uint64_t sbwt_colors_num_colors(const sbwt_colors_t *colors);
+
+/* Per-read color counts, the reference's ColorSearcher::search seam
+ * (src/ColorSearcher/ColorSearcher.h:43-48, kernels
+ * src/ColorSearcher/ColorSearcher.cuh:68-206 and
+ * src/ColorSearcher/ColorPostProcessor.cuh:21-43):
+ *   sbwt_idxs   -- found SBWT indexes of all reads back to back;
+ *   idx_offsets -- n_reads + 1 offsets into sbwt_idxs;
+ *   counts      -- n_reads x num_colors u32: k-mers of the read whose color
+ *                  set holds the color. */
+int sbwt_color_counts(const sbwt_colors_t *colors, const uint64_t *sbwt_idxs,
+                      const uint64_t *idx_offsets, uint64_t n_reads,
+                      uint32_t *counts, uint32_t flags, void *stream);
+
+/* Pseudoalignment: counts + the tau threshold of the reference's printer
+ * (src/ColorResultsPrinter/ContinuousColorResultsPrinter.hpp:235-263):
+ *   size = found + [SBWT_INCLUDE_NOT_FOUND] not_found + [SBWT_INCLUDE_INVALID]
+ *          invalid;  minimum = (u64)ceil((double)size * tau);
+ *   a read lists every color (ascending) whose count >= minimum, none when
+ *   minimum == 0.
+ * not_found / invalid: per-read counts (may be NULL when the matching flag is
+ * off).  Output: ids[ids_offsets[r] .. ids_offsets[r+1]) (u32 color ids).
+ * If ids_capacity is too small the call returns SBWT_E_CAPACITY with the
+ * offsets filled in (ids_offsets[n_reads] = required size). */
+int sbwt_pseudoalign(const sbwt_colors_t *colors, const uint64_t *sbwt_idxs,
+                     const uint64_t *idx_offsets, const uint64_t *not_found,
+                     const uint64_t *invalid, uint64_t n_reads, double tau,
+                     uint32_t flags, uint32_t *ids, uint64_t ids_capacity,
+                     uint64_t *ids_offsets, void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* Tuning and instrumentation (no counterpart in the reference)              */
+/* ------------------------------------------------------------------------ */
+/* Process-wide launch configuration used by the search calls (0 = default):
+ * presearch depth (<= the handle's), 256-thread blocks per SM, k-mer slots
+ * per work tile, chars per chunk of the host-pointer pipeline. */
+int sbwt_set_launch_config(uint32_t presearch_letters, uint32_t blocks_per_sm,
+                           uint64_t tile, uint64_t chunk_chars);
+/* Off by default.  When enabled, every search-kernel launch is timed with
+ * CUDA events on its own stream and this library's kernel launches are
+ * counted; count_work also counts full searches / streaming steps / rank
+ * block sectors of the read search kernel. */
+int sbwt_profile_enable(int enabled, int count_work);
+/* Reads and resets the totals (any pointer may be NULL). */
+int sbwt_profile_read(double *search_ms, uint64_t *search_launches,
+                      uint64_t *launches, uint64_t counters[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SBWT_B200_H */

@@ -1,0 +1,166 @@
+// C ABI entry points (include/sbwt_b200.h): argument checks, status codes,
+// thread-local last-error message.  No exception crosses this boundary.
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "common.hpp"
+#include "formats.hpp"
+#include "index_internal.hpp"
+
+namespace sbwt {
+static thread_local std::string g_last_error;
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+LaunchConfig &default_launch_config() {
+  static LaunchConfig cfg;
+  return cfg;
+}
+}  // namespace sbwt
+
+using namespace sbwt;
+
+extern "C" {
+
+const char *sbwt_last_error(void) { return g_last_error.c_str(); }
+const char *sbwt_version(void) { return "sbwt-b200 0.1 (sm_100a)"; }
+
+int sbwt_index_from_arrays(const uint64_t *const acgt[4], uint64_t num_bits,
+                           uint32_t k, const uint64_t *suffix_group_starts,
+                           const uint64_t *key_kmer_marks, int device,
+                           unsigned presearch_letters, sbwt_index_t **out) {
+  if (!acgt || !out) {
+    set_last_error("null argument");
+    return SBWT_E_INVALID;
+  }
+  *out = nullptr;
+  return guarded([&] {
+    for (int c = 0; c < 4; ++c)
+      if (!acgt[c]) throw Error(SBWT_E_INVALID, "null bitvector");
+    auto impl = std::make_unique<IndexImpl>(acgt, num_bits, k, suffix_group_starts,
+                                            key_kmer_marks, device, presearch_letters);
+    *out = new sbwt_index{impl.release()};
+  });
+}
+
+int sbwt_index_open(const char *sbwt_path, const char *colors_path, int device,
+                    unsigned presearch_letters, sbwt_index_t **out) {
+  if (!sbwt_path || !out) {
+    set_last_error("null argument");
+    return SBWT_E_INVALID;
+  }
+  *out = nullptr;
+  return guarded([&] {
+    SbwtFile f;
+    try {
+      f = read_sbwt(sbwt_path);
+    } catch (const std::runtime_error &e) {
+      std::string m = e.what();
+      throw Error(m.rfind("Unable to open", 0) == 0 ? SBWT_E_IO : SBWT_E_FORMAT, m);
+    }
+    BitVector keys;
+    if (colors_path) {
+      try {
+        keys = read_key_kmer_marks(colors_path);
+      } catch (const std::runtime_error &e) {
+        std::string m = e.what();
+        throw Error(m.rfind("Unable to open", 0) == 0 ? SBWT_E_IO : SBWT_E_FORMAT, m);
+      }
+      if (keys.num_bits < f.acgt[0].num_bits)
+        throw Error(SBWT_E_FORMAT, "key k-mer marks shorter than the SBWT");
+    }
+    const u64 *acgt[4] = {f.acgt[0].words.data(), f.acgt[1].words.data(),
+                          f.acgt[2].words.data(), f.acgt[3].words.data()};
+    const u64 *sg = f.suffix_group_starts.num_bits == f.acgt[0].num_bits
+                        ? f.suffix_group_starts.words.data()
+                        : nullptr;
+    auto impl = std::make_unique<IndexImpl>(
+        acgt, f.acgt[0].num_bits, (u32)f.k, sg,
+        colors_path ? keys.words.data() : nullptr, device, presearch_letters);
+    *out = new sbwt_index{impl.release()};
+  });
+}
+
+void sbwt_index_free(sbwt_index_t *index) {
+  if (!index) return;
+  delete index->impl;
+  delete index;
+}
+
+int sbwt_index_get_info(const sbwt_index_t *index, sbwt_index_info_t *info) {
+  if (!index || !info) {
+    set_last_error("null argument");
+    return SBWT_E_INVALID;
+  }
+  const IndexImpl &x = *index->impl;
+  info->num_bits = x.num_bits;
+  info->k = x.k;
+  info->presearch_letters = x.p_max;
+  for (int c = 0; c < 5; ++c) info->c_map[c] = x.c_map[c];
+  info->device_bytes = x.device_bytes;
+  info->device = x.device;
+  info->has_key_kmer_marks = x.view.key_marks != nullptr;
+  return SBWT_OK;
+}
+
+int sbwt_search_positions(const sbwt_index_t *index, const uint64_t *bit_seqs,
+                          uint64_t n_words, const uint64_t *positions,
+                          uint64_t n_positions, uint64_t *results, uint32_t flags,
+                          void *stream) {
+  if (!index || (n_positions && (!bit_seqs || !positions || !results))) {
+    set_last_error("null argument");
+    return SBWT_E_INVALID;
+  }
+  return guarded([&] {
+    if (!(flags & SBWT_DEVICE_POINTERS)) {
+      const u64 cap = n_words * 32;
+      for (u64 i = 0; i < n_positions; ++i)
+        if (positions[i] > cap || cap - positions[i] < index->impl->k)
+          throw Error(SBWT_E_INVALID, "a k-mer position lies past the end of bit_seqs");
+    }
+    index->impl->search_positions(bit_seqs, n_words, positions, n_positions, results,
+                                  flags, static_cast<cudaStream_t>(stream),
+                                  default_launch_config());
+  });
+}
+
+uint64_t sbwt_count_kmers(const uint64_t *read_ends, uint64_t n_reads, uint32_t k) {
+  if (!read_ends || k == 0) return 0;
+  uint64_t n = 0;
+  if (guarded([&] { n = count_kmers_host(read_ends, n_reads, k, 0); }) != SBWT_OK)
+    return 0;
+  return n;
+}
+
+int sbwt_search_reads(const sbwt_index_t *index, const char *chars, uint64_t n_chars,
+                      const uint64_t *read_ends, uint64_t n_reads, uint64_t *results,
+                      uint64_t results_capacity, uint64_t *n_results, uint32_t flags,
+                      void *stream) {
+  if (!index || (n_reads && (!read_ends || !results)) || (n_chars && !chars)) {
+    set_last_error("null argument");
+    return SBWT_E_INVALID;
+  }
+  return guarded([&] {
+    if ((flags & SBWT_MOVE_TO_KEY_KMER) && !index->impl->view.key_marks)
+      throw Error(SBWT_E_INVALID, "SBWT_MOVE_TO_KEY_KMER needs key k-mer marks");
+    if (!(flags & SBWT_DEVICE_POINTERS) && n_reads && read_ends[n_reads - 1] > n_chars)
+      throw Error(SBWT_E_INVALID, "read_ends exceed n_chars");
+    index->impl->search_reads(chars, n_chars, read_ends, n_reads, results,
+                              results_capacity, n_results, flags,
+                              static_cast<cudaStream_t>(stream),
+                              default_launch_config());
+  });
+}
+
+// Tuning hook used by the autotuner and the benchmark (not part of the
+// reference-facing surface): sets the process-wide launch configuration.
+int sbwt_set_launch_config(uint32_t presearch_letters, uint32_t blocks_per_sm,
+                           uint64_t tile, uint64_t chunk_chars) {
+  LaunchConfig &c = default_launch_config();
+  c.presearch_letters = presearch_letters;
+  c.blocks_per_sm = blocks_per_sm ? blocks_per_sm : 8;
+  c.tile = tile;
+  c.chunk_chars = chunk_chars;
+  return SBWT_OK;
+}
+
+}  // extern "C"

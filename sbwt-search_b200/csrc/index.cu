@@ -1,0 +1,941 @@
+// Index step on the B200: device SBWT (rank blocks + presearch pyramid),
+// device SeqToBits / PositionsBuilder equivalents, and the search kernels.
+//
+// Reference behaviour restated (SBWT-Search, paths in its src/):
+//   d_presearch            Presearcher/Presearcher.cuh:19-41
+//   d_search<move_to_key>  IndexSearcher/IndexSearcher.cuh:22-72
+//   CharToBits/convert_int SeqToBitsConverter/CharToBits.h:33-40,
+//                          SeqToBitsConverter/ContinuousSeqToBitsConverter.cpp:91-107
+//   build_positions        PositionsBuilder/PositionsBuilder.cpp:15-47
+//   -1 / -2 mapping        IndexResultsPrinter/ContinuousIndexResultsPrinter.hpp:196-205
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "common.hpp"
+#include "formats.hpp"
+#include "index_internal.hpp"
+#include "rank_blocks.cuh"
+
+namespace sbwt {
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+
+// Presearch pyramid, level j from level j-1: entry(x) for the j-char string
+// x (first char in the top bits) = one step from entry(x >> 2) with char
+// x & 3; level 1 = [c_map[c], c_map[c+1] - 1].  Same table as d_presearch,
+// built in sum_j 4^j steps instead of p * 4^p.
+__global__ void presearch_level_kernel(SbwtView s, uint64_t *pyr, uint32_t j) {
+  const uint64_t n = 1ULL << (2 * j);
+  for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < n;
+       x += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = (uint32_t)(x & 3);
+    uint64_t l, r;
+    if (j == 1) {
+      l = s.c_map[c];
+      r = s.c_map[c + 1] - 1;
+    } else {
+      const uint64_t pe = presearch_level_offset(j - 1) + (x >> 2);
+      if (!s.wide) {
+        const uint64_t v = pyr[pe];
+        l = v >> 32;
+        r = v & 0xFFFFFFFFULL;
+      } else {
+        l = pyr[2 * pe];
+        r = pyr[2 * pe + 1];
+      }
+      if (l <= r) sbwt_step(s, c, l, r);  // empty stays empty
+    }
+    const uint64_t e = presearch_level_offset(j) + x;
+    if (!s.wide) {
+      pyr[e] = (l << 32) | (r & 0xFFFFFFFFULL);
+    } else {
+      pyr[2 * e] = l;
+      pyr[2 * e + 1] = r;
+    }
+  }
+}
+
+// ASCII -> 2-bit MSB-first words (A0 C1 G2 T3, either case) + invalid bits.
+// One warp per 32 consecutive chars: coalesced byte loads, the word is
+// assembled with warp reductions.  Chars at or past n pack as 0, valid.
+__global__ void pack_kernel(const char *__restrict__ chars, uint64_t n,
+                            uint64_t *__restrict__ packed,
+                            uint32_t *__restrict__ invalid, uint64_t n_words) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t warp0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t w = warp0; w < n_words; w += warps) {
+    const uint64_t i = w * 32 + lane;
+    uint32_t code = 0;
+    bool bad = false;
+    if (i < n) {
+      const uint32_t ch = (uint8_t)chars[i];
+      code = ((ch >> 1) ^ (ch >> 2)) & 3u;
+      const uint32_t lower = ch | 0x20u;
+      bad = !(lower == 'a' || lower == 'c' || lower == 'g' || lower == 't');
+      if (bad) code = 0;
+    }
+    const uint32_t hi = lane < 16 ? code << (30 - 2 * lane) : 0u;
+    const uint32_t lo = lane >= 16 ? code << (30 - 2 * (lane - 16)) : 0u;
+    const uint32_t whi = __reduce_or_sync(0xFFFFFFFFu, hi);
+    const uint32_t wlo = __reduce_or_sync(0xFFFFFFFFu, lo);
+    const uint32_t inv = __ballot_sync(0xFFFFFFFFu, bad);
+    if (lane == 0) {
+      packed[w] = ((uint64_t)whi << 32) | wlo;
+      invalid[w] = inv;
+    }
+  }
+}
+
+// --- exclusive scan of per-read k-mer counts -> kmer_off[0..n_reads] ---------
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr uint64_t kScanTile = (uint64_t)kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint64_t read_kmers(const uint64_t *ends, uint64_t r,
+                                               uint64_t base, uint32_t k) {
+  const uint64_t st = r ? ends[r - 1] : base;
+  const uint64_t len = ends[r] - st;
+  return len >= k ? len - k + 1 : 0;
+}
+
+template <class T>
+__device__ __forceinline__ T block_exclusive_scan(T v, T *total) {
+  __shared__ T warp_sums[kScanThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    T s = lane < kScanThreads / 32 ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      T y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < kScanThreads / 32) warp_sums[lane] = s;
+  }
+  __syncthreads();
+  const T warp_prefix = wid ? warp_sums[wid - 1] : 0;
+  *total = warp_sums[kScanThreads / 32 - 1];
+  __syncthreads();
+  return warp_prefix + x - v;
+}
+
+__global__ void scan_reduce_kernel(const uint64_t *ends, uint64_t n_reads,
+                                   uint64_t base, uint32_t k, uint64_t n_chars,
+                                   uint64_t *block_sums, uint32_t *err) {
+  const uint64_t t0 = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  uint64_t s = 0;
+  for (int i = 0; i < kScanItems; ++i)
+    if (t0 + i < n_reads) {
+      const uint64_t r = t0 + i;
+      const uint64_t st = r ? ends[r - 1] : base;
+      if (ends[r] < st || ends[r] - base > n_chars) atomicOr(err, 4u);
+      s += read_kmers(ends, r, base, k);
+    }
+  uint64_t total;
+  block_exclusive_scan<uint64_t>(s, &total);
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+__global__ void scan_sums_kernel(uint64_t *block_sums, uint64_t n_blocks,
+                                 uint64_t *grand_total) {
+  __shared__ uint64_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint64_t b0 = 0; b0 < n_blocks; b0 += kScanThreads) {
+    const uint64_t b = b0 + threadIdx.x;
+    uint64_t v = b < n_blocks ? block_sums[b] : 0;
+    uint64_t total;
+    uint64_t ex = block_exclusive_scan<uint64_t>(v, &total);
+    if (b < n_blocks) block_sums[b] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *grand_total = carry;
+}
+
+__global__ void scan_write_kernel(const uint64_t *ends, uint64_t n_reads,
+                                  uint64_t base, uint32_t k,
+                                  const uint64_t *block_sums, uint64_t *kmer_off) {
+  const uint64_t t0 = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  uint64_t v[kScanItems];
+  uint64_t s = 0;
+  for (int i = 0; i < kScanItems; ++i) {
+    v[i] = (t0 + i < n_reads) ? read_kmers(ends, t0 + i, base, k) : 0;
+    s += v[i];
+  }
+  uint64_t total;
+  uint64_t ex = block_exclusive_scan<uint64_t>(s, &total) + block_sums[blockIdx.x];
+  for (int i = 0; i < kScanItems; ++i) {
+    if (t0 + i < n_reads) kmer_off[t0 + i] = ex;
+    if (t0 + i == n_reads - 1) kmer_off[n_reads] = ex + v[i];
+    ex += v[i];
+  }
+}
+
+// --- search ------------------------------------------------------------------
+__device__ __forceinline__ uint32_t char_at(const uint64_t *packed, uint64_t i) {
+  return (uint32_t)((__ldg(packed + (i >> 5)) >> (62 - 2 * (i & 31))) & 3ULL);
+}
+
+// First `n` chars (n <= 32) from char i as an integer, first char on top.
+__device__ __forceinline__ uint64_t chars_prefix(const uint64_t *packed, uint64_t i,
+                                                 uint32_t n) {
+  const uint64_t w = i >> 5;
+  const uint32_t off = (uint32_t)(i & 31);
+  uint64_t win = __ldg(packed + w) << (2 * off);
+  if (off) win |= __ldg(packed + w + 1) >> (64 - 2 * off);
+  return win >> (64 - 2 * n);
+}
+
+// Full search of the k-mer starting at char `pos`: presearch lookup of the
+// first p chars, then one step per remaining char, stopping at the first
+// empty interval (emptiness is preserved by every later step, so the answer
+// is unchanged).  Returns the node or SBWT_NOT_FOUND.
+__device__ __forceinline__ uint64_t full_search(const SbwtView &s,
+                                                const uint64_t *packed,
+                                                uint64_t pos) {
+  uint64_t l, r;
+  presearch_get(s, s.p, chars_prefix(packed, pos, s.p), l, r);
+  if (l > r) return SBWT_NOT_FOUND;
+  for (uint64_t i = pos + s.p; i < pos + s.k; ++i) {
+    sbwt_step(s, char_at(packed, i), l, r);
+    if (l > r) return SBWT_NOT_FOUND;
+  }
+  return l;
+}
+
+// full_search that also counts the distinct rank-block sectors it reads
+// (one per step, two when l and r + 1 fall in different blocks).
+__device__ __forceinline__ uint64_t full_search_counted(const SbwtView &s,
+                                                        const uint64_t *packed,
+                                                        uint64_t pos, uint64_t &sectors) {
+  uint64_t l, r;
+  presearch_get(s, s.p, chars_prefix(packed, pos, s.p), l, r);
+  if (l > r) return SBWT_NOT_FOUND;
+  for (uint64_t i = pos + s.p; i < pos + s.k; ++i) {
+    sectors += (block_of(l) == block_of(r + 1)) ? 1 : 2;
+    sbwt_step(s, char_at(packed, i), l, r);
+    if (l > r) return SBWT_NOT_FOUND;
+  }
+  return l;
+}
+
+// Largest u <= v with suffix_group_starts[u] set (node 0, the root, always is).
+__device__ __forceinline__ uint64_t group_start(const uint64_t *sg, uint64_t v) {
+  uint64_t w = v >> 6;
+  uint64_t m = __ldg(sg + w) & low_mask((uint32_t)(v & 63) + 1);
+  while (m == 0 && w > 0) m = __ldg(sg + --w);
+  if (m == 0) return 0;
+  return w * 64 + 63 - __clzll(m);
+}
+
+// Successor of node v (a found k-mer x) by char c: the node of x[1..k) c, or
+// SBWT_NOT_FOUND.  The edge bit lives at the first node of v's suffix group.
+__device__ __forceinline__ uint64_t stream_step(const SbwtView &s, uint64_t v,
+                                                uint32_t c) {
+  uint64_t b = block_of(v);
+  Block B = load_block(s.blocks[c] + b);
+  uint32_t q = (uint32_t)(v - b * kBlockBits);
+  if (!block_bit(B, q)) {
+    const uint64_t u = group_start(s.suffix_group_starts, v);
+    if (u == v) return SBWT_NOT_FOUND;
+    const uint64_t bu = block_of(u);
+    if (bu != b) {
+      B = load_block(s.blocks[c] + bu);
+      b = bu;
+    }
+    q = (uint32_t)(u - b * kBlockBits);
+    if (!block_bit(B, q)) return SBWT_NOT_FOUND;
+  }
+  return s.c_map[c] + s.l0[c][b >> kSuperchunkShift] + block_rank(B, q);
+}
+
+// Forward walk of a found node to the next key k-mer
+// (src/IndexSearcher/IndexSearcher.cuh:60-70): while the node is not a key
+// k-mer, follow its first outgoing edge in A,C,G,T order.  Bounded: a node
+// without an outgoing edge sets *err and returns the node unchanged.
+constexpr uint32_t kMaxKeyWalk = 1u << 16;
+__device__ __forceinline__ uint64_t key_walk(const SbwtView &s, uint64_t v,
+                                             uint32_t *err) {
+  for (uint32_t it = 0; it < kMaxKeyWalk; ++it) {
+    if ((__ldg(s.key_marks + (v >> 6)) >> (v & 63)) & 1ULL) return v;
+    bool moved = false;
+    for (uint32_t c = 0; c < 4; ++c) {
+      const uint64_t b = block_of(v);
+      const Block B = load_block(s.blocks[c] + b);
+      const uint32_t q = (uint32_t)(v - b * kBlockBits);
+      if (block_bit(B, q)) {
+        v = s.c_map[c] + s.l0[c][b >> kSuperchunkShift] + block_rank(B, q);
+        moved = true;
+        break;
+      }
+    }
+    if (!moved) break;
+  }
+  atomicOr(err, 1u);
+  return v;
+}
+
+// The reference seam: one k-mer per position, independent walks.
+__global__ void __launch_bounds__(256) search_positions_kernel(
+    SbwtView s, const uint64_t *__restrict__ packed, uint64_t n_chars_cap,
+    const uint64_t *__restrict__ positions, uint64_t n, uint64_t *__restrict__ out,
+    uint32_t move_to_key, uint32_t *err) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t pos = __ldg(positions + t);
+    if (pos > n_chars_cap || n_chars_cap - pos < s.k) {  // k-mer past bit_seqs
+      atomicOr(err, 2u);
+      out[t] = SBWT_NOT_FOUND;
+      continue;
+    }
+    uint64_t v = full_search(s, packed, pos);
+    if (move_to_key && v != SBWT_NOT_FOUND) v = key_walk(s, v, err);
+    out[t] = v;
+  }
+}
+
+struct ReadsView {
+  const uint64_t *packed;   // chunk chars, 2-bit packed (+1 pad word)
+  const uint32_t *invalid;  // invalid-char bits, 32 per word
+  const uint64_t *ends;     // exclusive read ends (absolute)
+  const uint64_t *kmer_off; // n_reads + 1
+  uint64_t base;            // absolute char offset of chunk char 0
+  uint64_t n_reads;
+  uint64_t n_kmers;
+  uint64_t tile;            // k-mer slots per tile
+  uint64_t n_tiles;
+  uint64_t *out;
+  uint64_t out_capacity;
+};
+
+__device__ __forceinline__ bool invalid_at(const uint32_t *inv, uint64_t i) {
+  return (__ldg(inv + (i >> 5)) >> (i & 31)) & 1u;
+}
+
+// Highest invalid char position in [a, b) (chunk-relative), or -1.
+__device__ __forceinline__ int64_t last_invalid(const uint32_t *inv, uint64_t a,
+                                                uint64_t b) {
+  if (b <= a) return -1;
+  int64_t w = (int64_t)((b - 1) >> 5);
+  const int64_t wa = (int64_t)(a >> 5);
+  uint32_t m = __ldg(inv + w);
+  const uint32_t top = (uint32_t)((b - 1) & 31);
+  if (top < 31) m &= (2u << top) - 1u;
+  while (true) {
+    if (w == wa) m &= ~((1u << (a & 31)) - 1u);
+    if (m) return w * 32 + 31 - __clz(m);
+    if (w == wa) return -1;
+    m = __ldg(inv + --w);
+  }
+}
+
+// Fused index step over reads.  Work unit = a tile of consecutive k-mer
+// result slots; inside a read each k-mer after a found one is resolved with
+// one stream_step (the successor edge) instead of a full search.  Results are
+// identical to independent searches because a k-mer's node is unique.
+template <bool STREAM, bool COUNT>
+__global__ void __launch_bounds__(256) search_reads_kernel(SbwtView s, ReadsView rv,
+                                                           uint32_t move_to_key,
+                                                           uint32_t *err,
+                                                           unsigned long long *counters) {
+  const uint32_t k = s.k;
+  uint64_t n_full = 0, n_stream = 0, n_steps = 0;
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < rv.n_tiles;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t slot = t * rv.tile;
+    const uint64_t slot_end = min(slot + rv.tile, rv.n_kmers);
+    // read containing slot: kmer_off[r] <= slot < kmer_off[r + 1]
+    uint64_t lo = 0, hi = rv.n_reads;  // invariant kmer_off[lo] <= slot
+    while (hi - lo > 1) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if (__ldg(rv.kmer_off + mid) <= slot) lo = mid; else hi = mid;
+    }
+    uint64_t r = lo;
+    uint64_t r_next = __ldg(rv.kmer_off + r + 1);
+    while (r_next <= slot) {  // skip reads without k-mers
+      ++r;
+      r_next = __ldg(rv.kmer_off + r + 1);
+    }
+    uint64_t read_start = (r ? __ldg(rv.ends + r - 1) : rv.base) - rv.base;
+    uint64_t pos = read_start + (slot - __ldg(rv.kmer_off + r));
+    int64_t last_inv = last_invalid(rv.invalid, pos, pos + k - 1);
+    uint64_t v = SBWT_NOT_FOUND;  // node of the previous k-mer in this read
+    for (; slot < slot_end; ++slot, ++pos) {
+      if (slot == r_next) {  // next read
+        do {
+          ++r;
+          r_next = __ldg(rv.kmer_off + r + 1);
+        } while (r_next == slot);
+        read_start = __ldg(rv.ends + r - 1) - rv.base;
+        pos = read_start;
+        last_inv = last_invalid(rv.invalid, pos, pos + k - 1);
+        v = SBWT_NOT_FOUND;
+      }
+      const uint64_t newc = pos + k - 1;
+      if (invalid_at(rv.invalid, newc)) last_inv = (int64_t)newc;
+      uint64_t res;
+      if (last_inv >= (int64_t)pos) {
+        res = SBWT_INVALID;
+        v = SBWT_NOT_FOUND;
+      } else {
+        if (STREAM && v != SBWT_NOT_FOUND) {
+          v = stream_step(s, v, char_at(rv.packed, newc));
+          if (COUNT) ++n_stream;
+        } else {
+          if (COUNT) {
+            v = full_search_counted(s, rv.packed, pos, n_steps);
+            ++n_full;
+          } else {
+            v = full_search(s, rv.packed, pos);
+          }
+        }
+        res = v;
+        if (move_to_key && v != SBWT_NOT_FOUND) res = key_walk(s, v, err);
+      }
+      if (slot < rv.out_capacity) rv.out[slot] = res;
+    }
+  }
+  if (COUNT) {
+    atomicAdd(counters + 0, (unsigned long long)n_full);
+    atomicAdd(counters + 1, (unsigned long long)n_stream);
+    atomicAdd(counters + 2, (unsigned long long)n_steps);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+// Optional instrumentation (off by default): CUDA-event time of every search
+// kernel launch on its own stream, a count of this library's kernel
+// launches, and (count mode) the work counters of the read search kernel.
+struct Profile {
+  std::mutex mu;
+  bool enabled = false;
+  bool count = false;
+  double search_ms = 0;
+  uint64_t search_launches = 0;
+  uint64_t launches = 0;
+  uint64_t counters[4] = {0, 0, 0, 0};
+  DeviceBuffer d_counters;
+};
+static Profile &profile() {
+  static Profile p;
+  return p;
+}
+static void note_launches(uint64_t n) {
+  Profile &p = profile();
+  if (!p.enabled) return;
+  std::lock_guard<std::mutex> g(p.mu);
+  p.launches += n;
+}
+
+static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsView &rv,
+                                 uint32_t mtk, uint32_t *d_err, int grid, int threads,
+                                 cudaStream_t st) {
+  Profile &p = profile();
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (p.enabled) {
+    SBWT_CUDA(cudaEventCreate(&e0));
+    SBWT_CUDA(cudaEventCreate(&e1));
+    SBWT_CUDA(cudaEventRecord(e0, st));
+  }
+  unsigned long long *ctr = nullptr;
+  if (p.enabled && p.count) {
+    std::lock_guard<std::mutex> g(p.mu);
+    if (p.d_counters.size() == 0) {
+      p.d_counters.resize(64);
+      SBWT_CUDA(cudaMemset(p.d_counters.get(), 0, 64));
+    }
+    ctr = p.d_counters.get<unsigned long long>();
+  }
+  if (ctr) {
+    if (stream)
+      search_reads_kernel<true, true><<<grid, threads, 0, st>>>(sv, rv, mtk, d_err, ctr);
+    else
+      search_reads_kernel<false, true><<<grid, threads, 0, st>>>(sv, rv, mtk, d_err, ctr);
+  } else {
+    if (stream)
+      search_reads_kernel<true, false><<<grid, threads, 0, st>>>(sv, rv, mtk, d_err, ctr);
+    else
+      search_reads_kernel<false, false><<<grid, threads, 0, st>>>(sv, rv, mtk, d_err, ctr);
+  }
+  SBWT_CUDA(cudaGetLastError());
+  if (p.enabled) {
+    SBWT_CUDA(cudaEventRecord(e1, st));
+    SBWT_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    SBWT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> g(p.mu);
+    p.search_ms += ms;
+    p.search_launches += 1;
+    p.launches += 1;
+  }
+}
+static int sm_count(int dev) {
+  int n = 148;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n;
+}
+
+// Builds the rank blocks of one bitvector (host), see rank_blocks.cuh.
+static void build_rank_blocks(const u64 *words, u64 num_bits,
+                              std::vector<Block> &blocks, std::vector<u64> &l0,
+                              u64 &total) {
+  const u64 nb = num_bits / kBlockBits + 1;
+  const u64 nw = (num_bits + 63) / 64;
+  blocks.assign(nb, Block{0, 0, 0, 0});
+  l0.assign((nb >> kSuperchunkShift) + 1, 0);
+  auto get64 = [&](u64 bit) -> u64 {  // 64 bits from position `bit`, 0 past end
+    u64 w = bit / 64, o = bit % 64;
+    u64 a = w < nw ? words[w] : 0;
+    u64 v = a >> o;
+    if (o) {
+      u64 b = (w + 1) < nw ? words[w + 1] : 0;
+      v |= b << (64 - o);
+    }
+    return v;
+  };
+  auto clip = [&](u64 v, u64 bit0, u64 nbits) -> u64 {  // zero bits >= num_bits
+    if (bit0 >= num_bits) return 0;
+    u64 avail = num_bits - bit0;
+    if (avail >= nbits) return v;
+    return v & ((1ULL << avail) - 1);
+  };
+  u64 ones = 0, chunk_base = 0;
+  for (u64 b = 0; b < nb; ++b) {
+    if ((b & ((1ULL << kSuperchunkShift) - 1)) == 0) {
+      l0[b >> kSuperchunkShift] = ones;
+      chunk_base = ones;
+    }
+    const u64 s = b * kBlockBits;
+    u64 p0 = clip(get64(s) & 0xFFFFFFFFULL, s, 32);
+    u64 p1 = clip(get64(s + 32), s + 32, 64);
+    u64 p2 = clip(get64(s + 96), s + 96, 64);
+    u64 p3 = clip(get64(s + 160), s + 160, 64);
+    Block &B = blocks[b];
+    B.w0 = ((ones - chunk_base) & 0xFFFFFFFFULL) | (p0 << 32);
+    B.w1 = p1;
+    B.w2 = p2;
+    B.w3 = p3;
+    ones += __builtin_popcountll(p0) + __builtin_popcountll(p1) +
+            __builtin_popcountll(p2) + __builtin_popcountll(p3);
+  }
+  total = ones;
+}
+
+IndexImpl::IndexImpl(const u64 *const acgt[4], u64 num_bits_, u32 k_,
+                     const u64 *sg, const u64 *key_marks, int device_,
+                     unsigned presearch_letters) {
+  if (num_bits_ == 0) throw Error(SBWT_E_INVALID, "empty SBWT");
+  if (k_ == 0) throw Error(SBWT_E_INVALID, "k must be positive");
+  device = device_;
+  DeviceGuard g(device);
+  num_bits = num_bits_;
+  k = k_;
+  p_max = presearch_letters ? presearch_letters : 12;
+  if (p_max > 12) throw Error(SBWT_E_INVALID, "presearch_letters must be <= 12");
+  if (p_max > k) p_max = k;
+  wide = num_bits >= (1ULL << 32) ? 1 : 0;
+  // rank blocks, one host thread per vector
+  std::vector<Block> hb[4];
+  std::vector<u64> hl0[4];
+  u64 totals[4];
+  {
+    std::vector<std::thread> th;
+    for (int c = 0; c < 4; ++c)
+      th.emplace_back([&, c] { build_rank_blocks(acgt[c], num_bits, hb[c], hl0[c], totals[c]); });
+    for (auto &t : th) t.join();
+  }
+  view = SbwtView{};
+  c_map[0] = 1;
+  for (int c = 0; c < 4; ++c) c_map[c + 1] = c_map[c] + totals[c];
+  for (int c = 0; c < 5; ++c) view.c_map[c] = c_map[c];
+  for (int c = 0; c < 4; ++c) {
+    blocks[c].resize(hb[c].size() * sizeof(Block));
+    SBWT_CUDA(cudaMemcpy(blocks[c].get(), hb[c].data(), hb[c].size() * sizeof(Block),
+                         cudaMemcpyHostToDevice));
+    l0[c].resize(hl0[c].size() * 8);
+    SBWT_CUDA(cudaMemcpy(l0[c].get(), hl0[c].data(), hl0[c].size() * 8,
+                         cudaMemcpyHostToDevice));
+    view.blocks[c] = blocks[c].get<Block>();
+    view.l0[c] = l0[c].get<u64>();
+  }
+  const u64 nw = (num_bits + 63) / 64;
+  if (sg) {
+    sg_buf.resize((nw + 1) * 8);
+    SBWT_CUDA(cudaMemset(sg_buf.get(), 0, (nw + 1) * 8));
+    SBWT_CUDA(cudaMemcpy(sg_buf.get(), sg, nw * 8, cudaMemcpyHostToDevice));
+    view.suffix_group_starts = sg_buf.get<u64>();
+  }
+  if (key_marks) {
+    key_buf.resize((nw + 1) * 8);
+    SBWT_CUDA(cudaMemset(key_buf.get(), 0, (nw + 1) * 8));
+    SBWT_CUDA(cudaMemcpy(key_buf.get(), key_marks, nw * 8, cudaMemcpyHostToDevice));
+    view.key_marks = key_buf.get<u64>();
+  }
+  view.num_bits = num_bits;
+  view.k = k;
+  view.wide = wide;
+  // presearch pyramid, levels 1..p_max
+  const u64 entries = presearch_level_offset(p_max + 1);
+  presearch.resize(entries * 8 * (wide ? 2 : 1));
+  view.presearch = presearch.get<u64>();
+  view.p = p_max;
+  const int sms = sm_count(device);
+  for (u32 j = 1; j <= p_max; ++j) {
+    const u64 n = 1ULL << (2 * j);
+    const int grid = (int)std::min<u64>((n + 255) / 256, (u64)sms * 16);
+    presearch_level_kernel<<<grid, 256>>>(view, presearch.get<u64>(), j);
+    SBWT_CUDA(cudaGetLastError());
+  }
+  SBWT_CUDA(cudaDeviceSynchronize());
+  device_bytes = presearch.size() + sg_buf.size() + key_buf.size();
+  for (int c = 0; c < 4; ++c) device_bytes += blocks[c].size() + l0[c].size();
+}
+
+SbwtView IndexImpl::view_for(u32 p) const {
+  SbwtView v = view;
+  v.p = (p == 0 || p > p_max) ? p_max : p;
+  return v;
+}
+
+// Per-thread, per-device scratch (device buffers, streams, pinned error word).
+struct Workspace {
+  int device = -1;
+  cudaStream_t streams[2] = {nullptr, nullptr};
+  DeviceBuffer chars[2], ends[2], kmer_off[2], packed[2], invalid[2], results[2],
+      block_sums[2], total[2], positions, bits;
+  uint32_t *err_host = nullptr;  // pinned
+  DeviceBuffer err_dev;
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  ~Workspace() {
+    if (device < 0) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    for (auto &s : streams)
+      if (s) cudaStreamDestroy(s);
+    for (auto &e : done)
+      if (e) cudaEventDestroy(e);
+    if (err_host) cudaFreeHost(err_host);
+    cudaSetDevice(prev);
+  }
+};
+
+static Workspace &workspace(int device) {
+  thread_local std::map<int, std::unique_ptr<Workspace>> ws;
+  auto &p = ws[device];
+  if (!p) {
+    p = std::make_unique<Workspace>();
+    p->device = device;
+    for (auto &s : p->streams)
+      SBWT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    for (auto &e : p->done) SBWT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    SBWT_CUDA(cudaMallocHost(&p->err_host, sizeof(uint32_t)));
+    p->err_dev.resize(sizeof(uint32_t));
+    SBWT_CUDA(cudaMemset(p->err_dev.get(), 0, sizeof(uint32_t)));
+  }
+  return *p;
+}
+
+static void check_err_word(Workspace &ws, cudaStream_t st) {
+  SBWT_CUDA(cudaMemcpyAsync(ws.err_host, ws.err_dev.get(), 4, cudaMemcpyDeviceToHost, st));
+  SBWT_CUDA(cudaStreamSynchronize(st));
+  const uint32_t e = *ws.err_host;
+  if (e) {
+    *ws.err_host = 0;
+    SBWT_CUDA(cudaMemset(ws.err_dev.get(), 0, 4));
+    if (e & 4u)
+      throw Error(SBWT_E_INVALID, "read_ends are not non-decreasing within n_chars");
+    if (e & 2u)
+      throw Error(SBWT_E_INVALID, "a k-mer position lies past the end of bit_seqs");
+    throw Error(SBWT_E_TIMEOUT,
+                "key k-mer walk did not reach a key k-mer (node without an "
+                "outgoing edge); results of those k-mers are unspecified");
+  }
+}
+
+static int grid_for(int dev, u64 work, int threads, int per_sm) {
+  const u64 g = std::min<u64>((work + threads - 1) / threads, (u64)sm_count(dev) * per_sm);
+  return (int)std::max<u64>(g, 1);
+}
+
+// Launches scan + pack + search over one chunk that is resident on the device.
+void IndexImpl::launch_reads(const char *d_chars, u64 n_chars, const u64 *d_ends,
+                             u64 n_reads, u64 base, u64 *d_out, u64 out_capacity,
+                             u32 flags, const LaunchConfig &cfg, cudaStream_t st,
+                             DeviceBuffer &kmer_off, DeviceBuffer &packed,
+                             DeviceBuffer &invalid, DeviceBuffer &block_sums,
+                             DeviceBuffer &total, u32 *d_err, u64 n_kmers_hint) const {
+  if (n_reads == 0) return;
+  const u64 n_words = (n_chars + 31) / 32;
+  kmer_off.ensure((n_reads + 1) * 8);
+  packed.ensure((n_words + 2) * 8);
+  invalid.ensure((n_words + 2) * 4);
+  const u64 n_scan_blocks = (n_reads + kScanTile - 1) / kScanTile;
+  block_sums.ensure(n_scan_blocks * 8);
+  total.ensure(8);
+  scan_reduce_kernel<<<(unsigned)n_scan_blocks, kScanThreads, 0, st>>>(
+      d_ends, n_reads, base, k, n_chars, block_sums.get<u64>(), d_err);
+  scan_sums_kernel<<<1, kScanThreads, 0, st>>>(block_sums.get<u64>(), n_scan_blocks,
+                                              total.get<u64>());
+  scan_write_kernel<<<(unsigned)n_scan_blocks, kScanThreads, 0, st>>>(
+      d_ends, n_reads, base, k, block_sums.get<u64>(), kmer_off.get<u64>());
+  SBWT_CUDA(cudaMemsetAsync(packed.get<u64>() + n_words, 0, 16, st));
+  SBWT_CUDA(cudaMemsetAsync(invalid.get<u32>() + n_words, 0, 8, st));
+  if (n_words)
+    pack_kernel<<<grid_for(device, n_words * 32, 256, 32), 256, 0, st>>>(
+        d_chars, n_chars, packed.get<u64>(), invalid.get<u32>(), n_words);
+  SBWT_CUDA(cudaGetLastError());
+  note_launches(n_words ? 4 : 3);
+  if (n_kmers_hint == 0) return;
+  ReadsView rv{};
+  rv.packed = packed.get<u64>();
+  rv.invalid = invalid.get<u32>();
+  rv.ends = d_ends;
+  rv.kmer_off = kmer_off.get<u64>();
+  rv.base = base;
+  rv.n_reads = n_reads;
+  rv.n_kmers = n_kmers_hint;
+  const int threads = 256;
+  const u64 resident = (u64)sm_count(device) * cfg.blocks_per_sm * threads;
+  u64 tile = cfg.tile;
+  if (tile == 0) {
+    tile = n_kmers_hint / (resident * 8);
+    tile = std::min<u64>(std::max<u64>(tile, 16), 1024);
+  }
+  rv.tile = tile;
+  rv.n_tiles = (n_kmers_hint + tile - 1) / tile;
+  rv.out = d_out;
+  rv.out_capacity = out_capacity;
+  const int grid = grid_for(device, rv.n_tiles, threads, cfg.blocks_per_sm);
+  const SbwtView sv = view_for(cfg.presearch_letters);
+  const bool stream = !(flags & SBWT_PER_KMER_WALK) && view.suffix_group_starts;
+  const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
+  launch_search_kernel(stream, sv, rv, mtk, d_err, grid, threads, st);
+}
+
+u64 count_kmers_host(const u64 *ends, u64 n_reads, u32 k, u64 base) {
+  u64 n = 0, prev = base;
+  for (u64 r = 0; r < n_reads; ++r) {
+    if (ends[r] < prev) throw Error(SBWT_E_INVALID, "read_ends must be non-decreasing");
+    const u64 len = ends[r] - prev;
+    if (len >= k) n += len - k + 1;
+    prev = ends[r];
+  }
+  return n;
+}
+
+void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_ends,
+                             u64 n_reads, u64 *results, u64 capacity,
+                             u64 *n_results, u32 flags, cudaStream_t user_stream,
+                             const LaunchConfig &cfg) const {
+  DeviceGuard g(device);
+  Workspace &ws = workspace(device);
+  if (flags & SBWT_DEVICE_POINTERS) {
+    // everything resident: one pass, asynchronous unless n_results wanted
+    u64 n_k = 0;
+    // the k-mer count drives the tiling: take it from the device scan
+    launch_reads(chars, n_chars, read_ends, n_reads, 0, results, capacity, flags, cfg,
+                 user_stream, ws.kmer_off[0], ws.packed[0], ws.invalid[0],
+                 ws.block_sums[0], ws.total[0], ws.err_dev.get<u32>(), 0);
+    if (n_reads) {
+      SBWT_CUDA(cudaMemcpyAsync(&n_k, ws.total[0].get(), 8, cudaMemcpyDeviceToHost,
+                                user_stream));
+      SBWT_CUDA(cudaStreamSynchronize(user_stream));
+    }
+    check_err_word(ws, user_stream);
+    if (n_results) *n_results = n_k;
+    if (n_k > capacity)
+      throw Error(SBWT_E_CAPACITY, "results_capacity smaller than the k-mer count");
+    // search (the scan/pack results are reused)
+    launch_search_only(n_chars, read_ends, n_reads, 0, results, capacity, flags, cfg,
+                       user_stream, ws.kmer_off[0], ws.packed[0], ws.invalid[0],
+                       ws.err_dev.get<u32>(), n_k);
+    check_err_word(ws, user_stream);
+    return;
+  }
+  // host pointers: chunk the reads, double-buffer, overlap H2D/compute/D2H
+  const u64 total_k = count_kmers_host(read_ends, n_reads, k, 0);
+  if (n_results) *n_results = total_k;
+  if (total_k > capacity)
+    throw Error(SBWT_E_CAPACITY, "results_capacity smaller than the k-mer count");
+  const u64 chunk_chars = cfg.chunk_chars ? cfg.chunk_chars : (64ULL << 20);
+  const bool pinned = is_host_pinned(chars) && is_host_pinned(results) &&
+                      is_host_pinned(read_ends);
+  struct Chunk {
+    u64 r0, r1, c0, c1, k0, nk;
+  };
+  std::vector<Chunk> chunks;
+  {
+    u64 r = 0, kacc = 0;
+    while (r < n_reads) {
+      Chunk ch{};
+      ch.r0 = r;
+      ch.c0 = r ? read_ends[r - 1] : 0;
+      ch.k0 = kacc;
+      u64 prev = ch.c0;
+      u64 nk = 0;
+      while (r < n_reads && (r == ch.r0 || read_ends[r] - ch.c0 <= chunk_chars)) {
+        const u64 len = read_ends[r] - prev;
+        if (len >= k) nk += len - k + 1;
+        prev = read_ends[r];
+        ++r;
+      }
+      ch.r1 = r;
+      ch.c1 = prev;
+      ch.nk = nk;
+      kacc += nk;
+      chunks.push_back(ch);
+    }
+  }
+  for (size_t i = 0; i < chunks.size(); ++i) {
+    const Chunk &ch = chunks[i];
+    const int b = (int)(i & 1);
+    cudaStream_t st = ws.streams[b];
+    const u64 nc = ch.c1 - ch.c0, nr = ch.r1 - ch.r0;
+    ws.chars[b].ensure(nc + 16);
+    ws.ends[b].ensure(nr * 8);
+    ws.results[b].ensure(std::max<u64>(ch.nk, 1) * 8);
+    SBWT_CUDA(cudaMemcpyAsync(ws.chars[b].get(), chars + ch.c0, nc,
+                              cudaMemcpyHostToDevice, st));
+    SBWT_CUDA(cudaMemcpyAsync(ws.ends[b].get(), read_ends + ch.r0, nr * 8,
+                              cudaMemcpyHostToDevice, st));
+    launch_reads(ws.chars[b].get<char>(), nc, ws.ends[b].get<u64>(), nr, ch.c0,
+                 ws.results[b].get<u64>(), ch.nk, flags, cfg, st, ws.kmer_off[b],
+                 ws.packed[b], ws.invalid[b], ws.block_sums[b], ws.total[b],
+                 ws.err_dev.get<u32>(), ch.nk);
+    if (ch.nk)
+      SBWT_CUDA(cudaMemcpyAsync(results + ch.k0, ws.results[b].get(), ch.nk * 8,
+                                cudaMemcpyDeviceToHost, st));
+    if (!pinned) SBWT_CUDA(cudaStreamSynchronize(st));
+  }
+  for (auto &s : ws.streams) SBWT_CUDA(cudaStreamSynchronize(s));
+  check_err_word(ws, ws.streams[0]);
+}
+
+void IndexImpl::launch_search_only(u64 n_chars, const u64 *d_ends, u64 n_reads, u64 base,
+                                   u64 *d_out, u64 out_capacity, u32 flags,
+                                   const LaunchConfig &cfg, cudaStream_t st,
+                                   DeviceBuffer &kmer_off, DeviceBuffer &packed,
+                                   DeviceBuffer &invalid, u32 *d_err, u64 n_kmers) const {
+  if (n_reads == 0 || n_kmers == 0) return;
+  (void)n_chars;
+  ReadsView rv{};
+  rv.packed = packed.get<u64>();
+  rv.invalid = invalid.get<u32>();
+  rv.ends = d_ends;
+  rv.kmer_off = kmer_off.get<u64>();
+  rv.base = base;
+  rv.n_reads = n_reads;
+  rv.n_kmers = n_kmers;
+  const int threads = 256;
+  const u64 resident = (u64)sm_count(device) * cfg.blocks_per_sm * threads;
+  u64 tile = cfg.tile;
+  if (tile == 0) {
+    tile = n_kmers / (resident * 8);
+    tile = std::min<u64>(std::max<u64>(tile, 16), 1024);
+  }
+  rv.tile = tile;
+  rv.n_tiles = (n_kmers + tile - 1) / tile;
+  rv.out = d_out;
+  rv.out_capacity = out_capacity;
+  const int grid = grid_for(device, rv.n_tiles, threads, cfg.blocks_per_sm);
+  const SbwtView sv = view_for(cfg.presearch_letters);
+  const bool stream = !(flags & SBWT_PER_KMER_WALK) && view.suffix_group_starts;
+  const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
+  launch_search_kernel(stream, sv, rv, mtk, d_err, grid, threads, st);
+}
+
+void IndexImpl::search_positions(const u64 *bit_seqs, u64 n_words, const u64 *positions,
+                                 u64 n, u64 *results, u32 flags, cudaStream_t st,
+                                 const LaunchConfig &cfg) const {
+  DeviceGuard g(device);
+  Workspace &ws = workspace(device);
+  if (n == 0) return;
+  if ((flags & SBWT_MOVE_TO_KEY_KMER) && !view.key_marks)
+    throw Error(SBWT_E_INVALID, "SBWT_MOVE_TO_KEY_KMER needs key k-mer marks");
+  const SbwtView sv = view_for(cfg.presearch_letters);
+  const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
+  const int grid = grid_for(device, n, 256, cfg.blocks_per_sm);
+  if (flags & SBWT_DEVICE_POINTERS) {
+    search_positions_kernel<<<grid, 256, 0, st>>>(sv, bit_seqs, n_words * 32, positions,
+                                                   n, results, mtk, ws.err_dev.get<u32>());
+    note_launches(1);
+    SBWT_CUDA(cudaGetLastError());
+    check_err_word(ws, st);
+    return;
+  }
+  cudaStream_t s0 = ws.streams[0];
+  ws.bits.ensure((n_words + 2) * 8);
+  ws.positions.ensure(n * 8);
+  ws.results[0].ensure(n * 8);
+  SBWT_CUDA(cudaMemsetAsync(ws.bits.get<u64>() + n_words, 0, 16, s0));
+  SBWT_CUDA(cudaMemcpyAsync(ws.bits.get(), bit_seqs, n_words * 8, cudaMemcpyHostToDevice, s0));
+  SBWT_CUDA(cudaMemcpyAsync(ws.positions.get(), positions, n * 8, cudaMemcpyHostToDevice, s0));
+  search_positions_kernel<<<grid, 256, 0, s0>>>(sv, ws.bits.get<u64>(), n_words * 32,
+                                                 ws.positions.get<u64>(), n,
+                                                 ws.results[0].get<u64>(), mtk,
+                                                 ws.err_dev.get<u32>());
+  note_launches(1);
+  SBWT_CUDA(cudaGetLastError());
+  SBWT_CUDA(cudaMemcpyAsync(results, ws.results[0].get(), n * 8, cudaMemcpyDeviceToHost, s0));
+  check_err_word(ws, s0);
+}
+
+}  // namespace sbwt
+
+extern "C" {
+// Instrumentation hooks (not part of the reference-facing surface).
+int sbwt_profile_enable(int enabled, int count_work) {
+  sbwt::Profile &p = sbwt::profile();
+  std::lock_guard<std::mutex> g(p.mu);
+  p.enabled = enabled != 0;
+  p.count = count_work != 0;
+  return SBWT_OK;
+}
+// search_ms: summed CUDA-event time of the read/position search kernels;
+// counters: [0] full searches, [1] streaming steps, [2] rank-block sectors of
+// full searches (count mode only).  Resets the totals.
+int sbwt_profile_read(double *search_ms, uint64_t *search_launches,
+                      uint64_t *launches, uint64_t counters[4]) {
+  sbwt::Profile &p = sbwt::profile();
+  std::lock_guard<std::mutex> g(p.mu);
+  if (search_ms) *search_ms = p.search_ms;
+  if (search_launches) *search_launches = p.search_launches;
+  if (launches) *launches = p.launches;
+  if (counters) {
+    uint64_t dc[4] = {0, 0, 0, 0};
+    if (p.d_counters.size()) {
+      cudaMemcpy(dc, p.d_counters.get(), 32, cudaMemcpyDeviceToHost);
+      cudaMemset(p.d_counters.get(), 0, 64);
+    }
+    for (int i = 0; i < 4; ++i) counters[i] = dc[i];
+  }
+  p.search_ms = 0;
+  p.search_launches = 0;
+  p.launches = 0;
+  return SBWT_OK;
+}
+}

@@ -1,0 +1,60 @@
+// Internal C++ view of the index handle (behind the sbwt_index_t C type).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.hpp"
+#include "device_layout.hpp"
+
+namespace sbwt {
+
+// Launch parameters chosen by the autotuner (0 = built-in default).
+struct LaunchConfig {
+  uint32_t presearch_letters = 0;  // <= the handle's pyramid depth
+  uint32_t blocks_per_sm = 8;      // 256-thread blocks per SM in the grid
+  uint64_t tile = 0;               // k-mer slots per work tile
+  uint64_t chunk_chars = 0;        // host-pointer path: chars per chunk
+};
+
+struct IndexImpl {
+  IndexImpl(const u64 *const acgt[4], u64 num_bits, u32 k, const u64 *sg,
+            const u64 *key_marks, int device, unsigned presearch_letters);
+
+  SbwtView view_for(u32 p) const;
+
+  void search_positions(const u64 *bit_seqs, u64 n_words, const u64 *positions,
+                        u64 n, u64 *results, u32 flags, cudaStream_t st,
+                        const LaunchConfig &cfg) const;
+  void search_reads(const char *chars, u64 n_chars, const u64 *read_ends,
+                    u64 n_reads, u64 *results, u64 capacity, u64 *n_results,
+                    u32 flags, cudaStream_t st, const LaunchConfig &cfg) const;
+  void launch_reads(const char *d_chars, u64 n_chars, const u64 *d_ends,
+                    u64 n_reads, u64 base, u64 *d_out, u64 out_capacity,
+                    u32 flags, const LaunchConfig &cfg, cudaStream_t st,
+                    DeviceBuffer &kmer_off, DeviceBuffer &packed,
+                    DeviceBuffer &invalid, DeviceBuffer &block_sums,
+                    DeviceBuffer &total, u32 *d_err, u64 n_kmers_hint) const;
+  void launch_search_only(u64 n_chars, const u64 *d_ends, u64 n_reads, u64 base,
+                          u64 *d_out, u64 out_capacity, u32 flags,
+                          const LaunchConfig &cfg, cudaStream_t st,
+                          DeviceBuffer &kmer_off, DeviceBuffer &packed,
+                          DeviceBuffer &invalid, u32 *d_err, u64 n_kmers) const;
+
+  int device = 0;
+  u64 num_bits = 0;
+  u32 k = 0;
+  u32 p_max = 12;
+  u32 wide = 0;
+  u64 c_map[5] = {0, 0, 0, 0, 0};
+  u64 device_bytes = 0;
+  SbwtView view{};
+  DeviceBuffer blocks[4], l0[4], presearch, sg_buf, key_buf;
+};
+
+u64 count_kmers_host(const u64 *ends, u64 n_reads, u32 k, u64 base);
+
+}  // namespace sbwt
+
+struct sbwt_index {
+  sbwt::IndexImpl *impl;
+};

@@ -1,0 +1,95 @@
+// Device-side rank / search primitives over the layout in device_layout.hpp.
+#pragma once
+
+#include <cstdint>
+
+#include "device_layout.hpp"
+
+namespace sbwt {
+
+// One 256-bit read-only load (a single sector request on sm_100).
+__device__ __forceinline__ Block load_block(const Block *p) {
+  Block b;
+  asm("ld.global.nc.v4.u64 {%0,%1,%2,%3}, [%4];"
+               : "=l"(b.w0), "=l"(b.w1), "=l"(b.w2), "=l"(b.w3)
+               : "l"(p));
+  return b;
+}
+
+__device__ __forceinline__ unsigned long long low_mask(uint32_t t) {
+  // bits [0, t) set, t in [0, 64]
+  return t >= 64 ? ~0ULL : ((1ULL << t) - 1ULL);
+}
+
+__device__ __forceinline__ uint32_t clamp64(int t) {
+  return t <= 0 ? 0u : (t >= 64 ? 64u : (uint32_t)t);
+}
+
+// Ones of the block strictly before in-block offset q (q in [0, 224)),
+// including the block's own 32-bit relative count.
+__device__ __forceinline__ uint64_t block_rank(const Block &b, uint32_t q) {
+  const int Q = (int)q + 32;  // bit position inside the 256-bit block
+  uint32_t r = (uint32_t)(b.w0 & 0xFFFFFFFFULL);
+  r += __popcll(b.w0 & low_mask(clamp64(Q)) & 0xFFFFFFFF00000000ULL);
+  r += __popcll(b.w1 & low_mask(clamp64(Q - 64)));
+  r += __popcll(b.w2 & low_mask(clamp64(Q - 128)));
+  r += __popcll(b.w3 & low_mask(clamp64(Q - 192)));
+  return r;
+}
+
+__device__ __forceinline__ bool block_bit(const Block &b, uint32_t q) {
+  const uint32_t Q = q + 32;
+  unsigned long long w = Q < 64 ? b.w0 : (Q < 128 ? b.w1 : (Q < 192 ? b.w2 : b.w3));
+  return (w >> (Q & 63)) & 1ULL;
+}
+
+__device__ __forceinline__ uint64_t block_of(uint64_t i) {
+  return i / kBlockBits;
+}
+
+// rank_c(i): ones of vector c in [0, i), i in [0, N].
+__device__ __forceinline__ uint64_t rank_full(const SbwtView &s, uint32_t c,
+                                              uint64_t i) {
+  const uint64_t b = block_of(i);
+  const Block blk = load_block(s.blocks[c] + b);
+  return s.l0[c][b >> kSuperchunkShift] +
+         block_rank(blk, (uint32_t)(i - b * kBlockBits));
+}
+
+__device__ __forceinline__ void presearch_get(const SbwtView &s, uint32_t level,
+                                              uint64_t x, uint64_t &l,
+                                              uint64_t &r) {
+  const uint64_t e = presearch_level_offset(level) + x;
+  if (!s.wide) {
+    uint64_t v = __ldg(s.presearch + e);
+    l = v >> 32;
+    r = v & 0xFFFFFFFFULL;
+  } else {
+    ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2 *>(s.presearch) + e);
+    l = v.x;
+    r = v.y;
+  }
+}
+
+// One backward-search step on [l, r] with char c
+// (src/IndexSearcher/IndexSearcher.cuh:52-54 of the reference); both rank
+// blocks are loaded before either is used, and a shared block is loaded once.
+__device__ __forceinline__ void sbwt_step(const SbwtView &s, uint32_t c,
+                                          uint64_t &l, uint64_t &r) {
+  const uint64_t bl = block_of(l);
+  const uint64_t r1 = r + 1;
+  const uint64_t br = block_of(r1);
+  const Block *base = s.blocks[c];
+  const Block Bl = load_block(base + bl);
+  Block Br = Bl;
+  if (br != bl) Br = load_block(base + br);
+  const uint64_t cc = s.c_map[c];
+  const uint64_t nl = cc + s.l0[c][bl >> kSuperchunkShift] +
+                      block_rank(Bl, (uint32_t)(l - bl * kBlockBits));
+  const uint64_t nr = cc + s.l0[c][br >> kSuperchunkShift] +
+                      block_rank(Br, (uint32_t)(r1 - br * kBlockBits)) - 1;
+  l = nl;
+  r = nr;
+}
+
+}  // namespace sbwt

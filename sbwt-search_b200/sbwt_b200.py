@@ -1,0 +1,275 @@
+"""Python host binding of the C ABI in include/sbwt_b200.h (ctypes).
+
+Mirrors the reference's in-process seams so that tests read like the
+reference's own:
+
+  * SbwtIndex.search(bit_seqs, positions)  ~ IndexSearcher::search
+    (src/IndexSearcher/IndexSearcher.h:41-46);
+  * SbwtIndex.search_reads(chars, read_ends) ~ the index step over a batch
+    (SeqToBits + PositionsBuilder + search + -1/-2 mapping);
+  * ColorIndex.counts / ColorIndex.pseudoalign ~ ColorSearcher::search
+    (src/ColorSearcher/ColorSearcher.h:43-48) + the printer's threshold.
+
+Device arrays are torch tensors (only for memory and streams); host arrays
+are numpy.  Every call raises SbwtError carrying the library's status code
+and message.  There is no CPU fallback: a missing library raises at import
+of the handle classes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "libsbwt_b200.so"
+
+OK, E_IO, E_FORMAT, E_OOM, E_CUDA, E_TIMEOUT, E_INVALID, E_CAPACITY = range(8)
+DEVICE_POINTERS = 0x1
+MOVE_TO_KEY_KMER = 0x2
+PER_KMER_WALK = 0x4
+INCLUDE_NOT_FOUND = 0x8
+INCLUDE_INVALID = 0x10
+NOT_FOUND = (1 << 64) - 1
+INVALID = (1 << 64) - 2
+
+
+class SbwtError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class IndexInfo(C.Structure):
+    _fields_ = [("num_bits", C.c_uint64), ("k", C.c_uint32),
+                ("presearch_letters", C.c_uint32), ("c_map", C.c_uint64 * 5),
+                ("device_bytes", C.c_uint64), ("device", C.c_int),
+                ("has_key_kmer_marks", C.c_int)]
+
+
+_L = None
+
+
+def lib():
+    """Loads _build/libsbwt_b200.so (raises if it was not built)."""
+    global _L
+    if _L is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} missing: build with sbwt-search_b200/build.py")
+        L = C.CDLL(str(LIB_PATH))
+        vp, u64, u32 = C.c_void_p, C.c_uint64, C.c_uint32
+        L.sbwt_last_error.restype = C.c_char_p
+        L.sbwt_version.restype = C.c_char_p
+        L.sbwt_index_open.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_uint,
+                                      C.POINTER(vp)]
+        L.sbwt_index_from_arrays.argtypes = [vp, u64, u32, vp, vp, C.c_int, C.c_uint,
+                                             C.POINTER(vp)]
+        L.sbwt_index_free.argtypes = [vp]
+        L.sbwt_index_free.restype = None
+        L.sbwt_index_get_info.argtypes = [vp, C.POINTER(IndexInfo)]
+        L.sbwt_search_positions.argtypes = [vp, vp, u64, vp, u64, vp, u32, vp]
+        L.sbwt_count_kmers.argtypes = [vp, u64, u32]
+        L.sbwt_count_kmers.restype = u64
+        L.sbwt_search_reads.argtypes = [vp, vp, u64, vp, u64, vp, u64,
+                                        C.POINTER(u64), u32, vp]
+        L.sbwt_set_launch_config.argtypes = [u32, u32, u64, u64]
+        if hasattr(L, "sbwt_colors_open"):
+            L.sbwt_colors_open.argtypes = [C.c_char_p, C.c_int, C.POINTER(vp)]
+            L.sbwt_colors_free.argtypes = [vp]
+            L.sbwt_colors_free.restype = None
+            L.sbwt_colors_num_colors.argtypes = [vp]
+            L.sbwt_colors_num_colors.restype = u64
+            L.sbwt_color_counts.argtypes = [vp, vp, vp, u64, vp, u32, vp]
+            L.sbwt_pseudoalign.argtypes = [vp, vp, vp, vp, vp, u64, C.c_double, u32,
+                                           vp, u64, vp, vp]
+        _L = L
+    return _L
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        raise SbwtError(rc, lib().sbwt_last_error().decode(errors="replace"))
+
+
+def _ptr(a) -> int | None:
+    """Address of a numpy array or a torch tensor (None for empty/None)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags.c_contiguous
+        return a.ctypes.data
+    return a.data_ptr()  # torch tensor
+
+
+def _is_dev(a) -> bool:
+    return not isinstance(a, np.ndarray) and getattr(a, "is_cuda", False)
+
+
+def set_launch_config(presearch_letters: int = 0, blocks_per_sm: int = 0,
+                      tile: int = 0, chunk_chars: int = 0) -> None:
+    check(lib().sbwt_set_launch_config(presearch_letters, blocks_per_sm, tile,
+                                       chunk_chars))
+
+
+class SbwtIndex:
+    """A resident SBWT on one GPU (rank blocks + presearch pyramid)."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+        info = IndexInfo()
+        check(lib().sbwt_index_get_info(self._h, C.byref(info)))
+        self.k = info.k
+        self.num_bits = info.num_bits
+        self.presearch_letters = info.presearch_letters
+        self.c_map = list(info.c_map)
+        self.device_bytes = info.device_bytes
+        self.device = info.device
+        self.has_key_kmer_marks = bool(info.has_key_kmer_marks)
+
+    @classmethod
+    def open(cls, sbwt_path, colors_path=None, device: int = 0,
+             presearch_letters: int = 0) -> "SbwtIndex":
+        h = C.c_void_p()
+        check(lib().sbwt_index_open(str(sbwt_path).encode(),
+                                    None if colors_path is None else str(colors_path).encode(),
+                                    device, presearch_letters, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_arrays(cls, acgt, num_bits: int, k: int, suffix_group_starts=None,
+                    key_kmer_marks=None, device: int = 0,
+                    presearch_letters: int = 0) -> "SbwtIndex":
+        arrs = [np.ascontiguousarray(a, dtype=np.uint64) for a in acgt]
+        ptrs = (C.c_void_p * 4)(*[a.ctypes.data for a in arrs])
+        sg = None if suffix_group_starts is None else np.ascontiguousarray(
+            suffix_group_starts, dtype=np.uint64)
+        km = None if key_kmer_marks is None else np.ascontiguousarray(
+            key_kmer_marks, dtype=np.uint64)
+        h = C.c_void_p()
+        check(lib().sbwt_index_from_arrays(ptrs, num_bits, k, _ptr(sg), _ptr(km), device,
+                                           presearch_letters, C.byref(h)))
+        return cls(h.value)
+
+    def close(self) -> None:
+        if self._h:
+            lib().sbwt_index_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- IndexSearcher::search seam ------------------------------------------
+    def search(self, bit_seqs, positions, out=None, move_to_key_kmer: bool = False,
+               stream: int = 0):
+        """bit_seqs: u64 2-bit MSB-first packed chars; positions: u64 k-mer
+        starts.  Host numpy in -> numpy out (synchronous); CUDA tensors in ->
+        results written into `out` (a CUDA int64/uint64 tensor)."""
+        flags = MOVE_TO_KEY_KMER if move_to_key_kmer else 0
+        if _is_dev(positions):
+            flags |= DEVICE_POINTERS
+            assert out is not None
+            check(lib().sbwt_search_positions(self._h, _ptr(bit_seqs), bit_seqs.numel(),
+                                              _ptr(positions), positions.numel(),
+                                              _ptr(out), flags, stream or None))
+            return out
+        bit_seqs = np.ascontiguousarray(bit_seqs, dtype=np.uint64)
+        positions = np.ascontiguousarray(positions, dtype=np.uint64)
+        res = np.empty(max(len(positions), 1), dtype=np.uint64)
+        check(lib().sbwt_search_positions(self._h, _ptr(bit_seqs), len(bit_seqs),
+                                          _ptr(positions), len(positions), _ptr(res),
+                                          flags, None))
+        return res[:len(positions)]
+
+    # -- fused read path ------------------------------------------------------
+    def count_kmers(self, read_ends: np.ndarray) -> int:
+        read_ends = np.ascontiguousarray(read_ends, dtype=np.uint64)
+        return int(lib().sbwt_count_kmers(_ptr(read_ends), len(read_ends), self.k))
+
+    def search_reads(self, chars, read_ends, out=None, move_to_key_kmer: bool = False,
+                     per_kmer_walk: bool = False, stream: int = 0):
+        """chars: reads back to back (bytes / uint8); read_ends: cumulative
+        exclusive ends.  Host in -> numpy u64 per k-mer (NOT_FOUND / INVALID
+        markers).  CUDA tensors in -> fills `out`, returns the k-mer count."""
+        flags = (MOVE_TO_KEY_KMER if move_to_key_kmer else 0) | \
+            (PER_KMER_WALK if per_kmer_walk else 0)
+        n_res = C.c_uint64(0)
+        if _is_dev(read_ends):
+            flags |= DEVICE_POINTERS
+            check(lib().sbwt_search_reads(self._h, _ptr(chars), chars.numel(),
+                                          _ptr(read_ends), read_ends.numel(), _ptr(out),
+                                          out.numel(), C.byref(n_res), flags,
+                                          stream or None))
+            return int(n_res.value)
+        if isinstance(chars, (bytes, bytearray)):
+            chars = np.frombuffer(chars, dtype=np.uint8)
+        chars = np.ascontiguousarray(chars, dtype=np.uint8)
+        read_ends = np.ascontiguousarray(read_ends, dtype=np.uint64)
+        if out is None:
+            out = np.empty(max(self.count_kmers(read_ends), 1), dtype=np.uint64)
+        check(lib().sbwt_search_reads(self._h, _ptr(chars) if len(chars) else None,
+                                      len(chars), _ptr(read_ends), len(read_ends),
+                                      _ptr(out), len(out), C.byref(n_res), flags, None))
+        return out[:n_res.value]
+
+
+class ColorIndex:
+    """A resident .tcolors color index on one GPU."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+        self.num_colors = int(lib().sbwt_colors_num_colors(self._h))
+
+    @classmethod
+    def open(cls, tcolors_path, device: int = 0) -> "ColorIndex":
+        h = C.c_void_p()
+        check(lib().sbwt_colors_open(str(tcolors_path).encode(), device, C.byref(h)))
+        return cls(h.value)
+
+    def close(self) -> None:
+        if self._h:
+            lib().sbwt_colors_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def counts(self, sbwt_idxs: np.ndarray, idx_offsets: np.ndarray) -> np.ndarray:
+        sbwt_idxs = np.ascontiguousarray(sbwt_idxs, dtype=np.uint64)
+        idx_offsets = np.ascontiguousarray(idx_offsets, dtype=np.uint64)
+        n = len(idx_offsets) - 1
+        out = np.zeros((max(n, 1), self.num_colors), dtype=np.uint32)
+        check(lib().sbwt_color_counts(self._h, _ptr(sbwt_idxs) if len(sbwt_idxs) else None,
+                                      _ptr(idx_offsets), n, _ptr(out), 0, None))
+        return out[:n]
+
+    def pseudoalign(self, sbwt_idxs, idx_offsets, not_found=None, invalid=None,
+                    tau: float = 0.7, include_not_found: bool = False,
+                    include_invalid: bool = False):
+        """Per read, the ascending color ids whose count passes tau."""
+        sbwt_idxs = np.ascontiguousarray(sbwt_idxs, dtype=np.uint64)
+        idx_offsets = np.ascontiguousarray(idx_offsets, dtype=np.uint64)
+        n = len(idx_offsets) - 1
+        nf = None if not_found is None else np.ascontiguousarray(not_found, np.uint64)
+        inv = None if invalid is None else np.ascontiguousarray(invalid, np.uint64)
+        flags = (INCLUDE_NOT_FOUND if include_not_found else 0) | \
+            (INCLUDE_INVALID if include_invalid else 0)
+        offs = np.zeros(n + 1, dtype=np.uint64)
+        cap = max(1, len(sbwt_idxs))
+        while True:
+            ids = np.zeros(cap, dtype=np.uint32)
+            rc = lib().sbwt_pseudoalign(self._h, _ptr(sbwt_idxs) if len(sbwt_idxs) else None,
+                                        _ptr(idx_offsets), _ptr(nf), _ptr(inv), n, tau,
+                                        flags, _ptr(ids), cap, _ptr(offs), None)
+            if rc == E_CAPACITY:
+                cap = int(offs[n]) + 1
+                continue
+            check(rc)
+            break
+        return [ids[int(offs[r]):int(offs[r + 1])].tolist() for r in range(n)], offs, ids

@@ -1,0 +1,36 @@
+"""The C-ABI library loads without a GPU and exports every function that
+include/*.h declares (no compute calls are made here)."""
+import ctypes
+import re
+from pathlib import Path
+
+import sbwt_b200 as S
+
+REPO = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    names = set()
+    for h in (REPO / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        for m in re.finditer(r"\b(sbwt_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_api():
+    names = declared_functions()
+    assert "sbwt_search_reads" in names and "sbwt_index_open" in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(str(S.LIB_PATH))
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_version_and_error_without_gpu():
+    assert b"sm_100a" in S.lib().sbwt_version()
+    h = ctypes.c_void_p()
+    rc = S.lib().sbwt_index_open(None, None, 0, 0, ctypes.byref(h))
+    assert rc == S.E_INVALID and S.lib().sbwt_last_error()

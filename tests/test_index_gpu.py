@@ -1,0 +1,129 @@
+"""Index step on the GPU through the C ABI, bit-exact against the oracle,
+the reference's own kernels compiled for the host, and the reference's
+golden fixtures."""
+import numpy as np
+import pytest
+
+import oracle as O
+import sbwt_b200 as S
+import sbwt_tools as T
+from helpers import FIXTURE_FILES, GOLDEN, golden_sbwt_path, synthetic, oracle_index, \
+    mixed_reads, oracle_results
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def golden_index():
+    return S.SbwtIndex.open(golden_sbwt_path())
+
+
+@pytest.mark.parametrize("name", FIXTURE_FILES)
+@pytest.mark.parametrize("per_kmer", [False, True])
+def test_reads_reproduce_reference_fixture(golden_index, name, per_kmer):
+    reads = O.parse_fastx((GOLDEN / "index_search" / name).read_bytes())
+    chars = b"".join(reads)
+    ends = np.cumsum([len(r) for r in reads]).astype(np.uint64)
+    res = golden_index.search_reads(chars, ends, per_kmer_walk=per_kmer)
+    rows, t = [], 0
+    for r in reads:
+        m = max(0, len(r) - golden_index.k + 1)
+        rows.append(O.as_signed_tokens(res[t:t + m]))
+        t += m
+    exp = O.read_ascii_index_results(GOLDEN / "index_search" / "expected" /
+                                     (name.split(".")[0] + ".txt"))
+    assert rows == exp
+
+
+@pytest.mark.parametrize("p", [0, 1, 7, 12])
+def test_positions_seam_matches_oracle_and_reference(p):
+    g, path, sb = synthetic(4, 2, 4000, 31, 1, 0.02)
+    idx = S.SbwtIndex.open(path, presearch_letters=p)
+    chars, ends = mixed_reads(g, 5, 500)
+    bits, _ = O.seq_to_bits(chars.tobytes())
+    pos = O.positions_of(ends, 31)
+    got = idx.search(bits, pos)
+    exp = oracle_index(path, 8).search_positions(bits, pos)
+    assert np.array_equal(got, exp)
+    if O.ref_lib() is not None:
+        ref = O.OracleIndex(sb.acgt, sb.num_bits, sb.k, use_ref=True)
+        assert np.array_equal(got, ref.search_positions(bits, pos))
+
+
+@pytest.mark.parametrize("per_kmer", [False, True])
+@pytest.mark.parametrize("seed", [11, 12])
+def test_reads_match_oracle(per_kmer, seed):
+    g, path, sb = synthetic(7, 4, 6000, 31, 2, 0.02)
+    idx = S.SbwtIndex.open(path)
+    chars, ends = mixed_reads(g, seed, 2000, median=90, sigma=0.8, len_min=0,
+                              len_max=500, sub=0.01, n_rate=0.01)
+    got = idx.search_reads(chars, ends, per_kmer_walk=per_kmer)
+    exp = oracle_results(oracle_index(path, 8), chars, ends)
+    assert got.dtype == np.uint64 and np.array_equal(got, exp)
+    assert (got < O.INVALID).any() and (got == O.NOT_FOUND).any() and (got == O.INVALID).any()
+
+
+def test_reads_small_k_and_no_suffix_groups():
+    g, path, sb = synthetic(8, 1, 3000, 15)
+    chars, ends = mixed_reads(g, 3, 500, median=40, sigma=0.5, len_min=0, len_max=120)
+    exp = oracle_results(oracle_index(path, 8), chars, ends)
+    # from arrays without the suffix-group vector: per-k-mer walks only
+    idx = S.SbwtIndex.from_arrays(sb.acgt, sb.num_bits, sb.k)
+    assert np.array_equal(idx.search_reads(chars, ends), exp)
+    idx2 = S.SbwtIndex.from_arrays(sb.acgt, sb.num_bits, sb.k, sb.suffix_group_starts,
+                                   presearch_letters=6)
+    assert np.array_equal(idx2.search_reads(chars, ends), exp)
+
+
+def test_edge_cases_empty_short_invalid():
+    g, path, sb = synthetic(4, 2, 4000, 31, 1, 0.02)
+    idx = S.SbwtIndex.open(path)
+    gen = g.seq(0)
+    reads = [b"", b"ACGT", gen[:31], gen[100:130], b"N" * 40, gen[:31].lower(),
+             gen[500:700] + b"X" + gen[700:900], b"", gen[1000:1031]]
+    chars = b"".join(reads)
+    ends = np.cumsum([len(r) for r in reads]).astype(np.uint64)
+    got = idx.search_reads(chars, ends)
+    exp = oracle_results(oracle_index(path, 8), np.frombuffer(chars, np.uint8), ends)
+    assert np.array_equal(got, exp)
+    # no reads at all
+    assert len(idx.search_reads(b"", np.zeros(0, np.uint64))) == 0
+
+
+def test_device_pointer_path_matches_host_path():
+    import torch
+    g, path, sb = synthetic(7, 4, 6000, 31, 2, 0.02)
+    idx = S.SbwtIndex.open(path)
+    chars, ends = mixed_reads(g, 21, 3000)
+    host = idx.search_reads(chars, ends)
+    d_chars = torch.from_numpy(chars.copy()).cuda()
+    d_ends = torch.from_numpy(ends.view(np.int64).copy()).cuda()
+    d_out = torch.empty(len(host) + 5, dtype=torch.int64, device="cuda")
+    n = idx.search_reads(d_chars, d_ends, out=d_out)
+    torch.cuda.synchronize()
+    assert n == len(host)
+    assert np.array_equal(d_out[:n].cpu().numpy().view(np.uint64), host)
+
+
+def test_chunked_host_pipeline_matches_single_chunk():
+    g, path, sb = synthetic(7, 4, 6000, 31, 2, 0.02)
+    idx = S.SbwtIndex.open(path)
+    chars, ends = mixed_reads(g, 31, 4000)
+    one = idx.search_reads(chars, ends)
+    S.set_launch_config(chunk_chars=5000)
+    try:
+        many = idx.search_reads(chars, ends)
+    finally:
+        S.set_launch_config()
+    assert np.array_equal(one, many)
+
+
+def test_errors_are_status_codes():
+    with pytest.raises(S.SbwtError) as e:
+        S.SbwtIndex.open("/nonexistent/file.sbwt")
+    assert e.value.code == S.E_IO
+    g, path, sb = synthetic(4, 2, 4000, 31, 1, 0.02)
+    idx = S.SbwtIndex.open(path)
+    with pytest.raises(S.SbwtError) as e:
+        idx.search_reads(b"ACGT" * 20, np.array([80], np.uint64), move_to_key_kmer=True)
+    assert e.value.code == S.E_INVALID

@@ -237,7 +237,8 @@ def main():
     torch.cuda.synchronize()
     ctr = (C.c_uint64 * 4)()
     L.sbwt_profile_read(None, None, None, ctr)
-    n_full, n_stream, full_sectors = int(ctr[0]), int(ctr[1]), int(ctr[2])
+    n_full, n_stream, full_sectors, n_other = (int(ctr[0]), int(ctr[1]), int(ctr[2]),
+                                               int(ctr[3]))
     L.sbwt_profile_enable(0, 0)
 
     for _ in range(args.warmup):
@@ -299,11 +300,13 @@ def main():
     # roofline of the dominant kernel (the read search kernel)
     peak, peak_kind = load_peaks()
     kern_ms = search_ms.value / max(1, search_launches.value)
-    # algorithmic bytes per launch: rank-block sectors of full searches (32 B
-    # each) + one presearch entry (32 B sector) per full search + one rank
-    # block sector per streaming step + 8 B result per k-mer + 2 bits of
-    # packed input per char + invalid bits
-    alg_bytes = (full_sectors + n_full + n_stream) * 32 + n_kmers * 8 + n_chars / 4 + n_chars / 8
+    # algorithmic bytes per launch (what this kernel's algorithm must move):
+    # 32 B per rank-block sector of the full-search steps, per presearch entry
+    # (one per full search), two per stream step (rank block + suffix-group
+    # word), one per extra stream iteration; 8 B result per k-mer; 2 bits of
+    # packed input + 1 invalid bit per char.
+    alg_bytes = ((full_sectors + n_full + 2 * n_stream + n_other) * 32 + n_kmers * 8 +
+                 n_chars / 4 + n_chars / 8)
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9
 
     cpu = None
@@ -336,7 +339,9 @@ def main():
                      "peak_kind": peak_kind, "kernel": "search_reads_kernel",
                      "kernel_ms": kern_ms,
                      "work": {"full_searches": n_full, "stream_steps": n_stream,
-                              "full_search_block_sectors": full_sectors}},
+                              "full_search_block_sectors": full_sectors,
+                              "extra_stream_iterations": n_other,
+                              "bytes_per_kmer": alg_bytes / n_kmers}},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "clocks": clk.summary(),

@@ -174,6 +174,36 @@ int sbwt_pseudoalign(const sbwt_colors_t *colors, const uint64_t *sbwt_idxs,
                      uint64_t *ids_offsets, void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* Host I/O in the reference's file formats (no GPU involved)               */
+/* ------------------------------------------------------------------------ */
+/* Reads every record of a FASTA/FASTQ file (.gz ok) with the reference's
+ * record rules (kseq: src/SequenceFileParser/ContinuousSequenceFileParser.cpp
+ * :148-156): *chars / *read_ends are malloc'ed, release with sbwt_free. */
+int sbwt_fastx_read(const char *path, char **chars, uint64_t *n_chars,
+                    uint64_t **read_ends, uint64_t *n_reads);
+void sbwt_free(void *p);
+/* Writes index results as the reference's printers do
+ * (src/IndexResultsPrinter/ printers: format 0 ascii .txt, 1 binary .bin, 2 bool
+ * .bool; optional length-prefixed format/version header). */
+int sbwt_write_index_results(const char *out_prefix, int format,
+                             int write_headers, const uint64_t *results,
+                             const uint64_t *read_ends, uint64_t n_reads,
+                             uint32_t k);
+/* Reads an ascii or binary index-results file back (the colors step's input,
+ * src/IndexFileParser/AsciiIndexFileParser.cpp:33-98,
+ * BinaryIndexFileParser.cpp:33-69): found indexes per read + -1 / -2 counts.
+ * Arrays are malloc'ed (sbwt_free). */
+int sbwt_read_index_results(const char *path, uint64_t **found,
+                            uint64_t **offsets, uint64_t **not_found,
+                            uint64_t **invalid, uint64_t *n_reads);
+/* Writes color results as the reference's printers do
+ * (src/ColorResultsPrinter/ printers: format 0 ascii .txt, 1 binary .bin, 2 csv). */
+int sbwt_write_color_results(const char *out_prefix, int format,
+                             int write_headers, const uint32_t *ids,
+                             const uint64_t *ids_offsets, uint64_t n_reads,
+                             uint64_t num_colors);
+
+/* ------------------------------------------------------------------------ */
 /* Tuning and instrumentation (no counterpart in the reference)              */
 /* ------------------------------------------------------------------------ */
 /* Process-wide launch configuration used by the search calls (0 = default):

@@ -348,6 +348,68 @@ def as_signed_tokens(row: np.ndarray) -> list[int]:
 # --------------------------------------------------------------------------
 # Colors step
 # --------------------------------------------------------------------------
+class ColorsFile:
+    """Themisto "sdsl-hybrid-v4" .tcolors file, member order as read by the
+    reference (src/ColorIndexBuilder/ColorIndexBuilder.cpp:23-86): dense
+    arrays (bit_vector), dense intervals, sparse arrays, sparse intervals
+    (int_vector<>), is_dense marks + rank blob, key k-mer marks + rank blob,
+    color set indexes (int_vector<>), then three u64 (the second + 1 is the
+    number of colors).  sdsl layouts: bit_vector = u64 bits + words;
+    int_vector<> = u64 bits + u8 width + words."""
+
+    def __init__(self, data: bytes):
+        off = 0
+
+        def u64():
+            nonlocal off
+            v = struct.unpack_from("<Q", data, off)[0]
+            off += 8
+            return v
+
+        n = u64()
+        if data[off:off + n] != b"sdsl-hybrid-v4":
+            raise ValueError("The colors file has an incorrect format. "
+                             "Expected 'sdsl-hybrid-v4'")
+        off += n
+
+        def words(nbits):
+            nonlocal off
+            nw = (nbits + 63) // 64
+            a = np.frombuffer(data, dtype=np.uint64, count=nw, offset=off).copy()
+            off += nw * 8
+            return a
+
+        def bitvector():
+            nb = u64()
+            return nb, words(nb)
+
+        def intvector():
+            nonlocal off
+            nb = u64()
+            w = data[off]
+            off += 1
+            return nb, w, words(nb)
+
+        _, self.dense_arrays = bitvector()
+        nb, self.dense_intervals_width, self.dense_intervals = intvector()
+        self.n_dense_intervals = nb // max(1, self.dense_intervals_width)
+        nb, self.sparse_arrays_width, self.sparse_arrays = intvector()
+        self.n_sparse = nb // max(1, self.sparse_arrays_width)
+        nb, self.sparse_intervals_width, self.sparse_intervals = intvector()
+        self.is_dense_bits, self.is_dense_marks = bitvector()
+        bitvector()  # rank blob
+        self.key_kmer_bits, self.key_kmer_marks = bitvector()
+        bitvector()  # rank blob
+        nb, self.color_set_idxs_width, self.color_set_idxs = intvector()
+        self.n_keys = nb // max(1, self.color_set_idxs_width)
+        self.max_color_set_idx, largest, self.sum_sizes = u64(), u64(), u64()
+        self.num_colors = largest + 1
+
+    @classmethod
+    def read(cls, path) -> "ColorsFile":
+        with open(path, "rb") as f:
+            return cls(f.read())
+
 class _ColorsStruct(C.Structure):
     _fields_ = [
         ("dense_arrays", U64P), ("dense_intervals", U64P),

@@ -6,6 +6,7 @@
 
 #include "common.hpp"
 #include "formats.hpp"
+#include "colors_internal.hpp"
 #include "index_internal.hpp"
 
 namespace sbwt {
@@ -148,6 +149,70 @@ int sbwt_search_reads(const sbwt_index_t *index, const char *chars, uint64_t n_c
                               results_capacity, n_results, flags,
                               static_cast<cudaStream_t>(stream),
                               default_launch_config());
+  });
+}
+
+int sbwt_colors_open(const char *tcolors_path, int device, sbwt_colors_t **out) {
+  if (!tcolors_path || !out) {
+    set_last_error("null argument");
+    return SBWT_E_INVALID;
+  }
+  *out = nullptr;
+  return guarded([&] {
+    TColorsFile t;
+    try {
+      t = read_tcolors(tcolors_path);
+    } catch (const std::runtime_error &e) {
+      std::string m = e.what();
+      throw Error(m.rfind("Unable to open", 0) == 0 ? SBWT_E_IO : SBWT_E_FORMAT, m);
+    }
+    auto impl = std::make_unique<ColorsImpl>(t, device);
+    *out = new sbwt_colors{impl.release()};
+  });
+}
+
+void sbwt_colors_free(sbwt_colors_t *colors) {
+  if (!colors) return;
+  delete colors->impl;
+  delete colors;
+}
+
+uint64_t sbwt_colors_num_colors(const sbwt_colors_t *colors) {
+  return colors ? colors->impl->num_colors : 0;
+}
+
+int sbwt_color_counts(const sbwt_colors_t *colors, const uint64_t *sbwt_idxs,
+                      const uint64_t *idx_offsets, uint64_t n_reads, uint32_t *counts,
+                      uint32_t flags, void *stream) {
+  if (!colors || (n_reads && (!idx_offsets || !counts))) {
+    set_last_error("null argument");
+    return SBWT_E_INVALID;
+  }
+  return guarded([&] {
+    colors->impl->counts(sbwt_idxs, idx_offsets, n_reads, counts, flags,
+                         static_cast<cudaStream_t>(stream));
+  });
+}
+
+int sbwt_pseudoalign(const sbwt_colors_t *colors, const uint64_t *sbwt_idxs,
+                     const uint64_t *idx_offsets, const uint64_t *not_found,
+                     const uint64_t *invalid, uint64_t n_reads, double tau, uint32_t flags,
+                     uint32_t *ids, uint64_t ids_capacity, uint64_t *ids_offsets,
+                     void *stream) {
+  if (!colors || !ids_offsets || (n_reads && !idx_offsets) ||
+      ((flags & SBWT_INCLUDE_NOT_FOUND) && n_reads && !not_found) ||
+      ((flags & SBWT_INCLUDE_INVALID) && n_reads && !invalid)) {
+    set_last_error("null argument");
+    return SBWT_E_INVALID;
+  }
+  if (!(tau >= 0.0) || tau > 1.0e300) {
+    set_last_error("tau must be a finite non-negative number");
+    return SBWT_E_INVALID;
+  }
+  return guarded([&] {
+    colors->impl->pseudoalign(sbwt_idxs, idx_offsets, not_found, invalid, n_reads, tau,
+                              flags, ids, ids_capacity, ids_offsets,
+                              static_cast<cudaStream_t>(stream));
   });
 }
 

@@ -1,0 +1,236 @@
+// sbwt_search -- the reference's command line (src/main.cpp:24-34), on the
+// B200 library:
+//   sbwt_search index  -i <.sbwt|.tdbg> -q <query|.list> -o <prefix|.list>
+//                      [-p ascii|binary|bool] [-k <.tcolors>] [--no-headers]
+//   sbwt_search colors -k <.tcolors> -q <indexes|.list> -o <prefix|.list>
+//                      [-p ascii|binary|csv] [-t <tau>] [--include-not-found]
+//                      [--include-invalid] [--no-headers]
+// Flags and defaults follow src/ArgumentParser/IndexSearchArgumentParser.cpp
+// :29-241 and ColorSearchArgumentParser.cpp:29-177.  The memory / stream flags
+// (-u -m -c -g -r -s) are accepted; this build sizes its batches from free
+// device memory itself.  A missing required flag prints the help and exits 1
+// (src/ArgumentParser/ArgumentParser.cpp:20-22); an unreadable input file is
+// reported and skipped (src/SequenceFileParser/
+// ContinuousSequenceFileParser.cpp:114-133).
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sbwt_b200.h"
+#include "host_io.hpp"
+
+using namespace sbwt;
+
+namespace {
+
+struct Args {
+  std::map<std::string, std::string> kv;
+  std::map<std::string, bool> flags;
+  bool has(const std::string &k) const { return kv.count(k) != 0; }
+  std::string get(const std::string &k, const std::string &d = "") const {
+    auto it = kv.find(k);
+    return it == kv.end() ? d : it->second;
+  }
+};
+
+const char *kIndexHelp =
+    "Usage: sbwt_search index [OPTION...]\n"
+    "  -q, --query-file arg            query FASTA/FASTQ file (.gz ok) or .list of files\n"
+    "  -i, --index-file arg            .sbwt or .tdbg index\n"
+    "  -o, --output-prefix arg         output prefix or .list of prefixes\n"
+    "  -p, --print-mode arg            ascii | binary | bool (default: ascii)\n"
+    "  -k, --colors-file arg           .tcolors file: report the next key k-mer (d > 1)\n"
+    "      --no-headers                do not write the format/version header\n"
+    "  -u, -m, -c, -r, -g, -s          memory / stream sizing (accepted, unused)\n"
+    "  -h, --help                      print this help\n";
+const char *kColorsHelp =
+    "Usage: sbwt_search colors [OPTION...]\n"
+    "  -q, --query-file arg            index results (.txt/.bin) or .list of files\n"
+    "  -k, --colors-file arg           .tcolors file\n"
+    "  -o, --output-prefix arg         output prefix or .list of prefixes\n"
+    "  -p, --print-mode arg            ascii | binary | csv (default: ascii)\n"
+    "  -t, --threshold arg             fraction of k-mers a color needs (default: 1)\n"
+    "      --include-not-found         count not-found k-mers in the read size\n"
+    "      --include-invalid           count invalid k-mers in the read size\n"
+    "      --no-headers                do not write the format/version header\n"
+    "  -u, -m, -c, -r, -g, -s          memory / stream sizing (accepted, unused)\n"
+    "  -h, --help                      print this help\n";
+
+Args parse(int argc, char **argv, int first) {
+  static const std::map<std::string, std::string> shorts = {
+      {"q", "query-file"},    {"i", "index-file"},   {"o", "output-prefix"},
+      {"p", "print-mode"},    {"k", "colors-file"},  {"u", "unavailable-main-memory"},
+      {"m", "max-main-memory"}, {"c", "cpu-memory-percentage"},
+      {"r", "base-pairs-per-seq"}, {"g", "gpu-memory-percentage"}, {"s", "streams"},
+      {"t", "threshold"},     {"h", "help"}};
+  static const std::vector<std::string> bools = {"no-headers", "include-not-found",
+                                                 "include-invalid", "help"};
+  Args a;
+  for (int i = first; i < argc; ++i) {
+    std::string t = argv[i];
+    std::string name;
+    if (t.rfind("--", 0) == 0) {
+      name = t.substr(2);
+    } else if (t.size() >= 2 && t[0] == '-') {
+      auto it = shorts.find(t.substr(1));
+      name = it == shorts.end() ? t.substr(1) : it->second;
+    } else {
+      continue;
+    }
+    auto eq = name.find('=');
+    if (eq != std::string::npos) {
+      a.kv[name.substr(0, eq)] = name.substr(eq + 1);
+      continue;
+    }
+    bool is_bool = false;
+    for (auto &b : bools) is_bool |= (b == name);
+    if (is_bool) {
+      a.flags[name] = true;
+    } else if (i + 1 < argc) {
+      a.kv[name] = argv[++i];
+    }
+  }
+  return a;
+}
+
+int missing(const Args &a, const std::vector<std::string> &req, const char *help) {
+  for (auto &r : req)
+    if (!a.has(r)) {
+      std::printf("Missing option: %s\n%s", r.c_str(), help);
+      return 1;
+    }
+  return 0;
+}
+
+void check(int rc) {
+  if (rc != SBWT_OK) throw std::runtime_error(sbwt_last_error());
+}
+
+int run_index(const Args &a) {
+  if (a.flags.count("help")) {
+    std::printf("%s", kIndexHelp);
+    return 1;
+  }
+  if (missing(a, {"query-file", "index-file", "output-prefix"}, kIndexHelp)) return 1;
+  const std::string mode = a.get("print-mode", "ascii");
+  IndexFormat fmt = mode == "binary" ? IndexFormat::Binary
+                    : mode == "bool" ? IndexFormat::Bool
+                                     : IndexFormat::Ascii;
+  if (mode != "ascii" && mode != "binary" && mode != "bool")
+    throw std::runtime_error("invalid print mode " + mode);
+  const bool headers = !a.flags.count("no-headers");
+  const std::string colors = a.get("colors-file");
+  sbwt_index_t *ix = nullptr;
+  check(sbwt_index_open(a.get("index-file").c_str(), colors.empty() ? nullptr : colors.c_str(),
+                        0, 0, &ix));
+  sbwt_index_info_t info{};
+  check(sbwt_index_get_info(ix, &info));
+  const uint32_t flags = colors.empty() ? 0 : SBWT_MOVE_TO_KEY_KMER;
+  auto ins = expand_list(a.get("query-file"));
+  auto outs = expand_list(a.get("output-prefix"));
+  if (ins.size() != outs.size())
+    throw std::runtime_error("query and output lists differ in length");
+  const u64 batch_chars = 256ULL << 20;
+  std::vector<u64> results;
+  for (size_t f = 0; f < ins.size(); ++f) {
+    std::unique_ptr<FastxReader> rd;
+    try {
+      rd = std::make_unique<FastxReader>(ins[f]);
+    } catch (const std::exception &e) {
+      std::fprintf(stderr, "[error] %s\n", e.what());
+      continue;
+    }
+    IndexResultsWriter w(outs[f], fmt, headers);
+    ReadBatch b;
+    while (true) {
+      b.clear();
+      if (!rd->next_batch(b, batch_chars, ~0ULL)) break;
+      const u64 nk = sbwt_count_kmers(b.ends.data(), b.ends.size(), info.k);
+      results.resize(std::max<u64>(nk, 1));
+      u64 n = 0;
+      check(sbwt_search_reads(ix, b.chars.data(), b.chars.size(), b.ends.data(), b.ends.size(),
+                              results.data(), results.size(), &n, flags, nullptr));
+      w.write(results.data(), b.ends.data(), b.ends.size(), info.k);
+    }
+  }
+  sbwt_index_free(ix);
+  return 0;
+}
+
+int run_colors(const Args &a) {
+  if (a.flags.count("help")) {
+    std::printf("%s", kColorsHelp);
+    return 1;
+  }
+  if (missing(a, {"query-file", "colors-file", "output-prefix"}, kColorsHelp)) return 1;
+  const std::string mode = a.get("print-mode", "ascii");
+  if (mode != "ascii" && mode != "binary" && mode != "csv")
+    throw std::runtime_error("invalid print mode " + mode);
+  ColorFormat fmt = mode == "binary" ? ColorFormat::Binary
+                    : mode == "csv"  ? ColorFormat::Csv
+                                     : ColorFormat::Ascii;
+  const bool headers = !a.flags.count("no-headers");
+  const double tau = std::stod(a.get("threshold", "1"));
+  uint32_t flags = 0;
+  if (a.flags.count("include-not-found")) flags |= SBWT_INCLUDE_NOT_FOUND;
+  if (a.flags.count("include-invalid")) flags |= SBWT_INCLUDE_INVALID;
+  sbwt_colors_t *ci = nullptr;
+  check(sbwt_colors_open(a.get("colors-file").c_str(), 0, &ci));
+  const u64 C = sbwt_colors_num_colors(ci);
+  auto ins = expand_list(a.get("query-file"));
+  auto outs = expand_list(a.get("output-prefix"));
+  if (ins.size() != outs.size())
+    throw std::runtime_error("query and output lists differ in length");
+  for (size_t f = 0; f < ins.size(); ++f) {
+    IndexResults r;
+    try {
+      r = read_index_results(ins[f]);
+    } catch (const std::exception &e) {
+      std::fprintf(stderr, "[error] %s\n", e.what());
+      continue;
+    }
+    const u64 n = r.not_found.size();
+    std::vector<u64> offs(n + 1, 0);
+    std::vector<uint32_t> ids(std::max<u64>(r.found.size(), 1));
+    int rc = sbwt_pseudoalign(ci, r.found.data(), r.offsets.data(), r.not_found.data(),
+                              r.invalid.data(), n, tau, flags, ids.data(), ids.size(),
+                              offs.data(), nullptr);
+    if (rc == SBWT_E_CAPACITY) {
+      ids.resize(offs[n] + 1);
+      rc = sbwt_pseudoalign(ci, r.found.data(), r.offsets.data(), r.not_found.data(),
+                            r.invalid.data(), n, tau, flags, ids.data(), ids.size(),
+                            offs.data(), nullptr);
+    }
+    check(rc);
+    ColorResultsWriter w(outs[f], fmt, headers, C);
+    w.write(ids.data(), offs.data(), n);
+  }
+  sbwt_colors_free(ci);
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  const char *usage = "Usage: sbwt_search [index|colors] [OPTIONS]\n";
+  if (argc < 2) {
+    std::printf("%s", usage);
+    return 1;
+  }
+  const std::string cmd = argv[1];
+  try {
+    Args a = parse(argc, argv, 2);
+    if (cmd == "index") return run_index(a);
+    if (cmd == "colors") return run_colors(a);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "[error] %s\n", e.what());
+    return 2;
+  }
+  std::printf("%s", usage);
+  return 1;
+}

@@ -1,0 +1,53 @@
+// Internal C++ view of the color index handle (behind sbwt_colors_t).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.hpp"
+#include "device_layout.hpp"
+#include "formats.hpp"
+
+namespace sbwt {
+
+// Device view of the color index.
+struct ColorsView {
+  const Block *key_blocks;  // rank blocks of the key k-mer marks
+  const uint64_t *key_l0;
+  uint64_t key_bits;
+  const uint32_t *csi;      // color set id per key k-mer
+  uint64_t n_keys;
+  const ulonglong2 *desc;   // per set: x = start, y = (len << 1) | dense
+  uint64_t n_sets;
+  const uint64_t *dense;    // word-aligned dense rows
+  const uint32_t *sparse;   // sparse color ids
+  uint32_t num_colors;
+  uint32_t row_words;       // ceil(num_colors / 64)
+  uint32_t words_per_lane;  // ceil(row_words / 32)
+};
+
+struct ColorsImpl {
+  ColorsImpl(const TColorsFile &t, int device);
+  // Per-read counts (n_reads x num_colors u32).
+  void counts(const u64 *vals, const u64 *offs, u64 n_reads, uint32_t *out, u32 flags,
+              cudaStream_t st) const;
+  // Threshold + sorted ids.
+  void pseudoalign(const u64 *vals, const u64 *offs, const u64 *nf, const u64 *inv,
+                   u64 n_reads, double tau, u32 flags, uint32_t *ids, u64 capacity,
+                   u64 *ids_offsets, cudaStream_t st) const;
+  void launch(const u64 *d_vals, const u64 *d_offs, const u64 *d_nf, const u64 *d_inv,
+              u64 n_reads, u64 max_kmers, double tau, u32 flags, int mode,
+              u64 *d_pass_bits, uint32_t *d_pass_count, uint32_t *d_counts,
+              uint32_t *d_err, cudaStream_t st) const;
+
+  int device = 0;
+  u64 num_colors = 0;
+  u64 device_bytes = 0;
+  DeviceBuffer key_blocks, key_l0, csi_buf, desc_buf, dense_buf, sparse_buf;
+  ColorsView view{};
+};
+
+}  // namespace sbwt
+
+struct sbwt_colors {
+  sbwt::ColorsImpl *impl;
+};

@@ -348,76 +348,226 @@ __device__ __forceinline__ int64_t last_invalid(const uint32_t *inv, uint64_t a,
   }
 }
 
-// Fused index step over reads.  Work unit = a tile of consecutive k-mer
-// result slots; inside a read each k-mer after a found one is resolved with
-// one stream_step (the successor edge) instead of a full search.  Results are
-// identical to independent searches because a k-mer's node is unique.
+// 32-byte aligned chunk of a u64 array that holds word i, loaded as a block.
+__device__ __forceinline__ const Block *chunk_of(const uint64_t *base, uint64_t i) {
+  return reinterpret_cast<const Block *>(base + (i & ~3ULL));
+}
+__device__ __forceinline__ uint64_t chunk_word(const Block &b, uint64_t i) {
+  const uint32_t j = (uint32_t)(i & 3);
+  return j == 0 ? b.w0 : (j == 1 ? b.w1 : (j == 2 ? b.w2 : b.w3));
+}
+
+// First read of every work tile: tile_read[t] = the read holding k-mer slot
+// t * tile.  One thread per read; reads without k-mers own no tile.
+__global__ void tile_reads_kernel(const uint64_t *kmer_off, uint64_t n_reads, uint64_t tile,
+                                  uint64_t *tile_read) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n_reads;
+       r += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t a = kmer_off[r], b = kmer_off[r + 1];
+    for (uint64_t t = (a + tile - 1) / tile; t * tile < b; ++t) tile_read[t] = r;
+  }
+}
+
+// Fused index step over reads.
+//
+// Work unit = a tile of consecutive k-mer result slots.  Inside a read, a
+// k-mer that follows a found k-mer is resolved by ONE step along the
+// successor edge of the previous node (stream step) instead of a full search;
+// the answer is the same because a k-mer's node is unique.
+//
+// Every lane runs its own state machine and each loop iteration performs one
+// memory round trip for every active lane: addresses are computed in divergent
+// code, then the warp reconverges (the warp-uniform exit test) and issues the
+// loads together, then consumes them in divergent code.  A lane in the middle
+// of a 19-step full search therefore never makes the other 31 lanes wait for
+// 19 round trips, and no lane's round trip is serialized behind another's.
+//   mode 0: the k-mer at `slot` needs its first load (stream step if the
+//           previous k-mer was found, else the presearch entry);
+//   mode 1: full search, next char wi (both rank blocks of [l, r]);
+//   mode 2: stream step, suffix-group-start word u (bits <= ubit) to find the
+//           first node g of v's suffix group;
+//   mode 3: stream step, rank block of char c at the group start u.
 template <bool STREAM, bool COUNT>
 __global__ void __launch_bounds__(256) search_reads_kernel(SbwtView s, ReadsView rv,
+                                                           const uint64_t *__restrict__ tile_read,
                                                            uint32_t move_to_key,
                                                            uint32_t *err,
                                                            unsigned long long *counters) {
   const uint32_t k = s.k;
-  uint64_t n_full = 0, n_stream = 0, n_steps = 0;
-  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < rv.n_tiles;
-       t += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t slot = t * rv.tile;
-    const uint64_t slot_end = min(slot + rv.tile, rv.n_kmers);
-    // read containing slot: kmer_off[r] <= slot < kmer_off[r + 1]
-    uint64_t lo = 0, hi = rv.n_reads;  // invariant kmer_off[lo] <= slot
-    while (hi - lo > 1) {
-      const uint64_t mid = (lo + hi) >> 1;
-      if (__ldg(rv.kmer_off + mid) <= slot) lo = mid; else hi = mid;
-    }
-    uint64_t r = lo;
-    uint64_t r_next = __ldg(rv.kmer_off + r + 1);
-    while (r_next <= slot) {  // skip reads without k-mers
-      ++r;
-      r_next = __ldg(rv.kmer_off + r + 1);
-    }
-    uint64_t read_start = (r ? __ldg(rv.ends + r - 1) : rv.base) - rv.base;
-    uint64_t pos = read_start + (slot - __ldg(rv.kmer_off + r));
-    int64_t last_inv = last_invalid(rv.invalid, pos, pos + k - 1);
-    uint64_t v = SBWT_NOT_FOUND;  // node of the previous k-mer in this read
-    for (; slot < slot_end; ++slot, ++pos) {
-      if (slot == r_next) {  // next read
-        do {
-          ++r;
-          r_next = __ldg(rv.kmer_off + r + 1);
-        } while (r_next == slot);
-        read_start = __ldg(rv.ends + r - 1) - rv.base;
-        pos = read_start;
-        last_inv = last_invalid(rv.invalid, pos, pos + k - 1);
-        v = SBWT_NOT_FOUND;
-      }
-      const uint64_t newc = pos + k - 1;
-      if (invalid_at(rv.invalid, newc)) last_inv = (int64_t)newc;
-      uint64_t res;
-      if (last_inv >= (int64_t)pos) {
-        res = SBWT_INVALID;
-        v = SBWT_NOT_FOUND;
-      } else {
-        if (STREAM && v != SBWT_NOT_FOUND) {
-          v = stream_step(s, v, char_at(rv.packed, newc));
-          if (COUNT) ++n_stream;
-        } else {
-          if (COUNT) {
-            v = full_search_counted(s, rv.packed, pos, n_steps);
-            ++n_full;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t n_pre = 0, n_stream = 0, n_walk_sectors = 0, n_other = 0;
+  uint64_t tile = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  uint64_t slot = 0, slot_end = 0, r = 0, r_next = 0, pos = 0;
+  int64_t last_inv = -1;
+  uint64_t v = SBWT_NOT_FOUND;  // node of the previous k-mer of this read
+  uint64_t l = 0, rr = 0, wi = 0, u = 0;
+  uint32_t mode = 0, c = 0, ubit = 63;
+  bool done = false;
+  const uint64_t pre_base = presearch_level_offset(s.p);
+  while (true) {
+    // ---- phase 1 (divergent): decide this lane's loads --------------------
+    const Block *addrA = nullptr, *addrB = nullptr;
+    uint64_t pre_e = 0;
+    if (!done) {
+      if (mode == 0) {
+        while (true) {
+          if (slot >= slot_end) {  // next tile
+            if (tile >= rv.n_tiles) {
+              done = true;
+              break;
+            }
+            slot = tile * rv.tile;
+            slot_end = min(slot + rv.tile, rv.n_kmers);
+            r = __ldg(tile_read + tile);
+            tile += stride;
+            r_next = __ldg(rv.kmer_off + r + 1);
+            pos = (r ? __ldg(rv.ends + r - 1) : rv.base) - rv.base +
+                  (slot - __ldg(rv.kmer_off + r));
+            last_inv = last_invalid(rv.invalid, pos, pos + k - 1);
+            v = SBWT_NOT_FOUND;
+          } else if (slot == r_next) {  // next read
+            do {
+              r_next = __ldg(rv.kmer_off + (++r) + 1);
+            } while (r_next == slot);
+            pos = __ldg(rv.ends + r - 1) - rv.base;
+            last_inv = last_invalid(rv.invalid, pos, pos + k - 1);
+            v = SBWT_NOT_FOUND;
+          }
+          const uint64_t newc = pos + k - 1;
+          if (invalid_at(rv.invalid, newc)) last_inv = (int64_t)newc;
+          if (last_inv < (int64_t)pos) break;  // a k-mer to search
+          if (slot < rv.out_capacity) __stcs(rv.out + slot, (unsigned long long)SBWT_INVALID);
+          v = SBWT_NOT_FOUND;
+          ++slot;
+          ++pos;
+        }
+        if (!done) {
+          if (STREAM && v != SBWT_NOT_FOUND) {
+            c = char_at(rv.packed, pos + k - 1);
+            addrA = s.blocks[c] + block_of(v);
+            if (COUNT) ++n_stream;
           } else {
-            v = full_search(s, rv.packed, pos);
+            pre_e = pre_base + chars_prefix(rv.packed, pos, s.p);
+            addrA = s.wide ? chunk_of(s.presearch, 2 * pre_e) : chunk_of(s.presearch, pre_e);
+            if (COUNT) ++n_pre;
           }
         }
-        res = v;
-        if (move_to_key && v != SBWT_NOT_FOUND) res = key_walk(s, v, err);
+      } else if (mode == 1) {
+        c = char_at(rv.packed, wi);
+        const uint64_t bl = block_of(l), br = block_of(rr + 1);
+        addrA = s.blocks[c] + bl;
+        if (br != bl) addrB = s.blocks[c] + br;
+        if (COUNT) n_walk_sectors += (br != bl) ? 2 : 1;
+      } else if (mode == 2) {
+        addrA = chunk_of(s.suffix_group_starts, u);
+        if (COUNT) ++n_other;
+      } else {
+        addrA = s.blocks[c] + block_of(u);
+        if (COUNT) ++n_other;
       }
-      if (slot < rv.out_capacity) rv.out[slot] = res;
+    }
+    if (__all_sync(0xFFFFFFFFu, done)) break;
+    // ---- phase 2 (converged): the loads ------------------------------------
+    Block A = Block{0, 0, 0, 0}, B;
+    if (addrA) A = load_block(addrA);
+    B = A;
+    if (addrB) B = load_block(addrB);
+    if (done) continue;
+    // ---- phase 3 (divergent): consume ----------------------------------------
+    uint64_t emit = 0;
+    bool emitted = false;
+    if (mode == 0) {
+      if (STREAM && v != SBWT_NOT_FOUND) {
+        const uint64_t b = block_of(v);
+        const uint32_t q = (uint32_t)(v - b * kBlockBits);
+        if (block_bit(A, q)) {  // v starts its suffix group and has edge c
+          emit = s.c_map[c] + s.l0[c][b >> kSuperchunkShift] + block_rank(A, q);
+          emitted = true;
+        } else {  // find the first node of v's suffix group
+          u = v >> 6;
+          ubit = (uint32_t)(v & 63);
+          mode = 2;
+        }
+      } else {
+        uint64_t pl, pr;
+        if (!s.wide) {
+          const uint64_t e = chunk_word(A, pre_e);
+          pl = e >> 32;
+          pr = e & 0xFFFFFFFFULL;
+        } else {
+          pl = chunk_word(A, 2 * pre_e);
+          pr = chunk_word(A, 2 * pre_e + 1);
+        }
+        if (pl > pr) {
+          emit = SBWT_NOT_FOUND;
+          emitted = true;
+        } else if (s.p >= k) {
+          emit = pl;
+          emitted = true;
+        } else {
+          l = pl;
+          rr = pr;
+          wi = pos + s.p;
+          mode = 1;
+        }
+      }
+    } else if (mode == 1) {
+      const uint64_t bl = block_of(l), r1 = rr + 1, br = block_of(r1);
+      const uint64_t cc = s.c_map[c];
+      const uint64_t nl = cc + s.l0[c][bl >> kSuperchunkShift] +
+                          block_rank(A, (uint32_t)(l - bl * kBlockBits));
+      const uint64_t nr = cc + s.l0[c][br >> kSuperchunkShift] +
+                          block_rank(B, (uint32_t)(r1 - br * kBlockBits)) - 1;
+      l = nl;
+      rr = nr;
+      ++wi;
+      if (l > rr) {
+        emit = SBWT_NOT_FOUND;
+        emitted = true;
+      } else if (wi == pos + k) {
+        emit = l;
+        emitted = true;
+      }
+    } else if (mode == 2) {
+      const uint64_t w = chunk_word(A, u) & low_mask(ubit + 1);
+      if (w) {
+        const uint64_t g = u * 64 + 63 - __clzll(w);
+        if (g == v) {  // v starts its group and has no edge c
+          emit = SBWT_NOT_FOUND;
+          emitted = true;
+        } else {
+          u = g;
+          mode = 3;
+        }
+      } else if (u == 0) {
+        emit = SBWT_NOT_FOUND;  // no group start below v: malformed SBWT
+        emitted = true;
+      } else {
+        --u;
+        ubit = 63;
+      }
+    } else {
+      const uint64_t b = block_of(u);
+      const uint32_t q = (uint32_t)(u - b * kBlockBits);
+      emit = block_bit(A, q) ? s.c_map[c] + s.l0[c][b >> kSuperchunkShift] + block_rank(A, q)
+                             : SBWT_NOT_FOUND;
+      emitted = true;
+    }
+    if (emitted) {
+      v = emit;
+      uint64_t res = emit;
+      if (move_to_key && emit != SBWT_NOT_FOUND) res = key_walk(s, emit, err);
+      if (slot < rv.out_capacity) __stcs(rv.out + slot, (unsigned long long)res);
+      ++slot;
+      ++pos;
+      mode = 0;
     }
   }
   if (COUNT) {
-    atomicAdd(counters + 0, (unsigned long long)n_full);
+    atomicAdd(counters + 0, (unsigned long long)n_pre);
     atomicAdd(counters + 1, (unsigned long long)n_stream);
-    atomicAdd(counters + 2, (unsigned long long)n_steps);
+    atomicAdd(counters + 2, (unsigned long long)n_walk_sectors);
+    atomicAdd(counters + 3, (unsigned long long)n_other);
   }
 }
 
@@ -449,8 +599,8 @@ static void note_launches(uint64_t n) {
 }
 
 static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsView &rv,
-                                 uint32_t mtk, uint32_t *d_err, int grid, int threads,
-                                 cudaStream_t st) {
+                                 const uint64_t *tile_read, uint32_t mtk, uint32_t *d_err,
+                                 int grid, int threads, cudaStream_t st) {
   Profile &p = profile();
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (p.enabled) {
@@ -469,14 +619,14 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
   }
   if (ctr) {
     if (stream)
-      search_reads_kernel<true, true><<<grid, threads, 0, st>>>(sv, rv, mtk, d_err, ctr);
+      search_reads_kernel<true, true><<<grid, threads, 0, st>>>(sv, rv, tile_read, mtk, d_err, ctr);
     else
-      search_reads_kernel<false, true><<<grid, threads, 0, st>>>(sv, rv, mtk, d_err, ctr);
+      search_reads_kernel<false, true><<<grid, threads, 0, st>>>(sv, rv, tile_read, mtk, d_err, ctr);
   } else {
     if (stream)
-      search_reads_kernel<true, false><<<grid, threads, 0, st>>>(sv, rv, mtk, d_err, ctr);
+      search_reads_kernel<true, false><<<grid, threads, 0, st>>>(sv, rv, tile_read, mtk, d_err, ctr);
     else
-      search_reads_kernel<false, false><<<grid, threads, 0, st>>>(sv, rv, mtk, d_err, ctr);
+      search_reads_kernel<false, false><<<grid, threads, 0, st>>>(sv, rv, tile_read, mtk, d_err, ctr);
   }
   SBWT_CUDA(cudaGetLastError());
   if (p.enabled) {
@@ -498,8 +648,8 @@ static int sm_count(int dev) {
   return n;
 }
 
-// Builds the rank blocks of one bitvector (host), see rank_blocks.cuh.
-static void build_rank_blocks(const u64 *words, u64 num_bits,
+// Builds the rank blocks of one bitvector (host), see device_layout.hpp.
+void build_rank_blocks_host(const u64 *words, u64 num_bits,
                               std::vector<Block> &blocks, std::vector<u64> &l0,
                               u64 &total) {
   const u64 nb = num_bits / kBlockBits + 1;
@@ -564,7 +714,7 @@ IndexImpl::IndexImpl(const u64 *const acgt[4], u64 num_bits_, u32 k_,
   {
     std::vector<std::thread> th;
     for (int c = 0; c < 4; ++c)
-      th.emplace_back([&, c] { build_rank_blocks(acgt[c], num_bits, hb[c], hl0[c], totals[c]); });
+      th.emplace_back([&, c] { build_rank_blocks_host(acgt[c], num_bits, hb[c], hl0[c], totals[c]); });
     for (auto &t : th) t.join();
   }
   view = SbwtView{};
@@ -583,8 +733,8 @@ IndexImpl::IndexImpl(const u64 *const acgt[4], u64 num_bits_, u32 k_,
   }
   const u64 nw = (num_bits + 63) / 64;
   if (sg) {
-    sg_buf.resize((nw + 1) * 8);
-    SBWT_CUDA(cudaMemset(sg_buf.get(), 0, (nw + 1) * 8));
+    sg_buf.resize((nw + 8) * 8);
+    SBWT_CUDA(cudaMemset(sg_buf.get(), 0, (nw + 8) * 8));
     SBWT_CUDA(cudaMemcpy(sg_buf.get(), sg, nw * 8, cudaMemcpyHostToDevice));
     view.suffix_group_starts = sg_buf.get<u64>();
   }
@@ -599,7 +749,7 @@ IndexImpl::IndexImpl(const u64 *const acgt[4], u64 num_bits_, u32 k_,
   view.wide = wide;
   // presearch pyramid, levels 1..p_max
   const u64 entries = presearch_level_offset(p_max + 1);
-  presearch.resize(entries * 8 * (wide ? 2 : 1));
+  presearch.resize(entries * 8 * (wide ? 2 : 1) + 64);
   view.presearch = presearch.get<u64>();
   view.p = p_max;
   const int sms = sm_count(device);
@@ -625,7 +775,7 @@ struct Workspace {
   int device = -1;
   cudaStream_t streams[2] = {nullptr, nullptr};
   DeviceBuffer chars[2], ends[2], kmer_off[2], packed[2], invalid[2], results[2],
-      block_sums[2], total[2], positions, bits;
+      block_sums[2], total[2], tile_read[2], positions, bits;
   uint32_t *err_host = nullptr;  // pinned
   DeviceBuffer err_dev;
   cudaEvent_t done[2] = {nullptr, nullptr};
@@ -681,59 +831,90 @@ static int grid_for(int dev, u64 work, int threads, int per_sm) {
   return (int)std::max<u64>(g, 1);
 }
 
-// Launches scan + pack + search over one chunk that is resident on the device.
-void IndexImpl::launch_reads(const char *d_chars, u64 n_chars, const u64 *d_ends,
-                             u64 n_reads, u64 base, u64 *d_out, u64 out_capacity,
-                             u32 flags, const LaunchConfig &cfg, cudaStream_t st,
-                             DeviceBuffer &kmer_off, DeviceBuffer &packed,
-                             DeviceBuffer &invalid, DeviceBuffer &block_sums,
-                             DeviceBuffer &total, u32 *d_err, u64 n_kmers_hint) const {
-  if (n_reads == 0) return;
+// Device scratch of one read batch: scan outputs, packed chars, invalid
+// bits, the tile table and the error word.
+struct ReadsScratch {
+  u64 *kmer_off;    // n_reads + 1
+  u64 *packed;      // n_words + 2
+  uint32_t *invalid;  // n_words + 2
+  u64 *block_sums;  // ceil(n_reads / kScanTile)
+  u64 *total;       // 1
+  u64 *tile_read;   // n_tiles
+  uint32_t *err;    // 1
+};
+
+static u64 tile_size(int device, u64 n_kmers, const LaunchConfig &cfg) {
+  if (cfg.tile) return cfg.tile;
+  const u64 resident = (u64)sm_count(device) * cfg.blocks_per_sm * 256;
+  u64 tile = n_kmers / (resident * 8);
+  return std::min<u64>(std::max<u64>(tile, 16), 1024);
+}
+
+// Scan of per-read k-mer counts and the packing of the chars (device-resident
+// inputs).  The k-mer total lands in *sc.total.
+static void launch_prepare(int device, u32 k, const char *d_chars, u64 n_chars,
+                           const u64 *d_ends, u64 n_reads, u64 base,
+                           const ReadsScratch &sc, cudaStream_t st) {
   const u64 n_words = (n_chars + 31) / 32;
-  kmer_off.ensure((n_reads + 1) * 8);
-  packed.ensure((n_words + 2) * 8);
-  invalid.ensure((n_words + 2) * 4);
   const u64 n_scan_blocks = (n_reads + kScanTile - 1) / kScanTile;
-  block_sums.ensure(n_scan_blocks * 8);
-  total.ensure(8);
   scan_reduce_kernel<<<(unsigned)n_scan_blocks, kScanThreads, 0, st>>>(
-      d_ends, n_reads, base, k, n_chars, block_sums.get<u64>(), d_err);
-  scan_sums_kernel<<<1, kScanThreads, 0, st>>>(block_sums.get<u64>(), n_scan_blocks,
-                                              total.get<u64>());
+      d_ends, n_reads, base, k, n_chars, sc.block_sums, sc.err);
+  scan_sums_kernel<<<1, kScanThreads, 0, st>>>(sc.block_sums, n_scan_blocks, sc.total);
   scan_write_kernel<<<(unsigned)n_scan_blocks, kScanThreads, 0, st>>>(
-      d_ends, n_reads, base, k, block_sums.get<u64>(), kmer_off.get<u64>());
-  SBWT_CUDA(cudaMemsetAsync(packed.get<u64>() + n_words, 0, 16, st));
-  SBWT_CUDA(cudaMemsetAsync(invalid.get<u32>() + n_words, 0, 8, st));
+      d_ends, n_reads, base, k, sc.block_sums, sc.kmer_off);
+  SBWT_CUDA(cudaMemsetAsync(sc.packed + n_words, 0, 16, st));
+  SBWT_CUDA(cudaMemsetAsync(sc.invalid + n_words, 0, 8, st));
   if (n_words)
     pack_kernel<<<grid_for(device, n_words * 32, 256, 32), 256, 0, st>>>(
-        d_chars, n_chars, packed.get<u64>(), invalid.get<u32>(), n_words);
+        d_chars, n_chars, sc.packed, sc.invalid, n_words);
   SBWT_CUDA(cudaGetLastError());
   note_launches(n_words ? 4 : 3);
-  if (n_kmers_hint == 0) return;
+}
+
+// Tile table + the read search kernel over a prepared batch of n_kmers.
+static void launch_search(const IndexImpl &ix, const u64 *d_ends, u64 n_reads, u64 base,
+                          u64 n_kmers, u64 *d_out, u64 out_capacity, u32 flags,
+                          const LaunchConfig &cfg, const ReadsScratch &sc,
+                          cudaStream_t st) {
+  if (n_reads == 0 || n_kmers == 0) return;
   ReadsView rv{};
-  rv.packed = packed.get<u64>();
-  rv.invalid = invalid.get<u32>();
+  rv.packed = sc.packed;
+  rv.invalid = sc.invalid;
   rv.ends = d_ends;
-  rv.kmer_off = kmer_off.get<u64>();
+  rv.kmer_off = sc.kmer_off;
   rv.base = base;
   rv.n_reads = n_reads;
-  rv.n_kmers = n_kmers_hint;
-  const int threads = 256;
-  const u64 resident = (u64)sm_count(device) * cfg.blocks_per_sm * threads;
-  u64 tile = cfg.tile;
-  if (tile == 0) {
-    tile = n_kmers_hint / (resident * 8);
-    tile = std::min<u64>(std::max<u64>(tile, 16), 1024);
-  }
-  rv.tile = tile;
-  rv.n_tiles = (n_kmers_hint + tile - 1) / tile;
+  rv.n_kmers = n_kmers;
+  rv.tile = tile_size(ix.device, n_kmers, cfg);
+  rv.n_tiles = (n_kmers + rv.tile - 1) / rv.tile;
   rv.out = d_out;
   rv.out_capacity = out_capacity;
-  const int grid = grid_for(device, rv.n_tiles, threads, cfg.blocks_per_sm);
-  const SbwtView sv = view_for(cfg.presearch_letters);
-  const bool stream = !(flags & SBWT_PER_KMER_WALK) && view.suffix_group_starts;
+  tile_reads_kernel<<<grid_for(ix.device, n_reads, 256, 16), 256, 0, st>>>(
+      sc.kmer_off, n_reads, rv.tile, sc.tile_read);
+  SBWT_CUDA(cudaGetLastError());
+  note_launches(1);
+  const int threads = 256;
+  const int grid = grid_for(ix.device, rv.n_tiles, threads, cfg.blocks_per_sm);
+  const SbwtView sv = ix.view_for(cfg.presearch_letters);
+  const bool stream = !(flags & SBWT_PER_KMER_WALK) && ix.view.suffix_group_starts;
   const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
-  launch_search_kernel(stream, sv, rv, mtk, d_err, grid, threads, st);
+  launch_search_kernel(stream, sv, rv, sc.tile_read, mtk, sc.err, grid, threads, st);
+}
+
+// Grows the workspace buffers of slot b for a batch and returns raw pointers.
+static ReadsScratch scratch_for(Workspace &ws, int b, u64 n_chars, u64 n_reads,
+                                u64 n_kmers_max, u64 tile_min) {
+  const u64 n_words = (n_chars + 31) / 32;
+  ws.kmer_off[b].ensure((n_reads + 1) * 8);
+  ws.packed[b].ensure((n_words + 2) * 8);
+  ws.invalid[b].ensure((n_words + 2) * 4);
+  ws.block_sums[b].ensure(((n_reads + kScanTile - 1) / kScanTile + 1) * 8);
+  ws.total[b].ensure(8);
+  ws.tile_read[b].ensure((n_kmers_max / tile_min + 2) * 8);
+  return ReadsScratch{ws.kmer_off[b].get<u64>(), ws.packed[b].get<u64>(),
+                      ws.invalid[b].get<uint32_t>(), ws.block_sums[b].get<u64>(),
+                      ws.total[b].get<u64>(), ws.tile_read[b].get<u64>(),
+                      ws.err_dev.get<uint32_t>()};
 }
 
 u64 count_kmers_host(const u64 *ends, u64 n_reads, u32 k, u64 base) {
@@ -754,26 +935,25 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
   DeviceGuard g(device);
   Workspace &ws = workspace(device);
   if (flags & SBWT_DEVICE_POINTERS) {
-    // everything resident: one pass, asynchronous unless n_results wanted
+    // everything resident; the k-mer count (needed for the tiling and the
+    // capacity check) comes from the device scan
     u64 n_k = 0;
-    // the k-mer count drives the tiling: take it from the device scan
-    launch_reads(chars, n_chars, read_ends, n_reads, 0, results, capacity, flags, cfg,
-                 user_stream, ws.kmer_off[0], ws.packed[0], ws.invalid[0],
-                 ws.block_sums[0], ws.total[0], ws.err_dev.get<u32>(), 0);
     if (n_reads) {
-      SBWT_CUDA(cudaMemcpyAsync(&n_k, ws.total[0].get(), 8, cudaMemcpyDeviceToHost,
-                                user_stream));
+      // k-mers <= chars, so a tile table sized for n_chars is always enough
+      const ReadsScratch sc = scratch_for(ws, 0, n_chars, n_reads, n_chars, 16);
+      launch_prepare(device, k, chars, n_chars, read_ends, n_reads, 0, sc, user_stream);
+      SBWT_CUDA(cudaMemcpyAsync(&n_k, sc.total, 8, cudaMemcpyDeviceToHost, user_stream));
       SBWT_CUDA(cudaStreamSynchronize(user_stream));
+      check_err_word(ws, user_stream);
+      if (n_results) *n_results = n_k;
+      if (n_k > capacity)
+        throw Error(SBWT_E_CAPACITY, "results_capacity smaller than the k-mer count");
+      launch_search(*this, read_ends, n_reads, 0, n_k, results, capacity, flags, cfg, sc,
+                    user_stream);
+      check_err_word(ws, user_stream);
+    } else if (n_results) {
+      *n_results = 0;
     }
-    check_err_word(ws, user_stream);
-    if (n_results) *n_results = n_k;
-    if (n_k > capacity)
-      throw Error(SBWT_E_CAPACITY, "results_capacity smaller than the k-mer count");
-    // search (the scan/pack results are reused)
-    launch_search_only(n_chars, read_ends, n_reads, 0, results, capacity, flags, cfg,
-                       user_stream, ws.kmer_off[0], ws.packed[0], ws.invalid[0],
-                       ws.err_dev.get<u32>(), n_k);
-    check_err_word(ws, user_stream);
     return;
   }
   // host pointers: chunk the reads, double-buffer, overlap H2D/compute/D2H
@@ -818,14 +998,15 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
     ws.chars[b].ensure(nc + 16);
     ws.ends[b].ensure(nr * 8);
     ws.results[b].ensure(std::max<u64>(ch.nk, 1) * 8);
+    const ReadsScratch sc = scratch_for(ws, b, nc, nr, ch.nk, tile_size(device, ch.nk, cfg));
     SBWT_CUDA(cudaMemcpyAsync(ws.chars[b].get(), chars + ch.c0, nc,
                               cudaMemcpyHostToDevice, st));
     SBWT_CUDA(cudaMemcpyAsync(ws.ends[b].get(), read_ends + ch.r0, nr * 8,
                               cudaMemcpyHostToDevice, st));
-    launch_reads(ws.chars[b].get<char>(), nc, ws.ends[b].get<u64>(), nr, ch.c0,
-                 ws.results[b].get<u64>(), ch.nk, flags, cfg, st, ws.kmer_off[b],
-                 ws.packed[b], ws.invalid[b], ws.block_sums[b], ws.total[b],
-                 ws.err_dev.get<u32>(), ch.nk);
+    launch_prepare(device, k, ws.chars[b].get<char>(), nc, ws.ends[b].get<u64>(), nr, ch.c0,
+                   sc, st);
+    launch_search(*this, ws.ends[b].get<u64>(), nr, ch.c0, ch.nk, ws.results[b].get<u64>(),
+                  ch.nk, flags, cfg, sc, st);
     if (ch.nk)
       SBWT_CUDA(cudaMemcpyAsync(results + ch.k0, ws.results[b].get(), ch.nk * 8,
                                 cudaMemcpyDeviceToHost, st));
@@ -833,39 +1014,6 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
   }
   for (auto &s : ws.streams) SBWT_CUDA(cudaStreamSynchronize(s));
   check_err_word(ws, ws.streams[0]);
-}
-
-void IndexImpl::launch_search_only(u64 n_chars, const u64 *d_ends, u64 n_reads, u64 base,
-                                   u64 *d_out, u64 out_capacity, u32 flags,
-                                   const LaunchConfig &cfg, cudaStream_t st,
-                                   DeviceBuffer &kmer_off, DeviceBuffer &packed,
-                                   DeviceBuffer &invalid, u32 *d_err, u64 n_kmers) const {
-  if (n_reads == 0 || n_kmers == 0) return;
-  (void)n_chars;
-  ReadsView rv{};
-  rv.packed = packed.get<u64>();
-  rv.invalid = invalid.get<u32>();
-  rv.ends = d_ends;
-  rv.kmer_off = kmer_off.get<u64>();
-  rv.base = base;
-  rv.n_reads = n_reads;
-  rv.n_kmers = n_kmers;
-  const int threads = 256;
-  const u64 resident = (u64)sm_count(device) * cfg.blocks_per_sm * threads;
-  u64 tile = cfg.tile;
-  if (tile == 0) {
-    tile = n_kmers / (resident * 8);
-    tile = std::min<u64>(std::max<u64>(tile, 16), 1024);
-  }
-  rv.tile = tile;
-  rv.n_tiles = (n_kmers + tile - 1) / tile;
-  rv.out = d_out;
-  rv.out_capacity = out_capacity;
-  const int grid = grid_for(device, rv.n_tiles, threads, cfg.blocks_per_sm);
-  const SbwtView sv = view_for(cfg.presearch_letters);
-  const bool stream = !(flags & SBWT_PER_KMER_WALK) && view.suffix_group_starts;
-  const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
-  launch_search_kernel(stream, sv, rv, mtk, d_err, grid, threads, st);
 }
 
 void IndexImpl::search_positions(const u64 *bit_seqs, u64 n_words, const u64 *positions,

@@ -28,17 +28,6 @@ struct IndexImpl {
   void search_reads(const char *chars, u64 n_chars, const u64 *read_ends,
                     u64 n_reads, u64 *results, u64 capacity, u64 *n_results,
                     u32 flags, cudaStream_t st, const LaunchConfig &cfg) const;
-  void launch_reads(const char *d_chars, u64 n_chars, const u64 *d_ends,
-                    u64 n_reads, u64 base, u64 *d_out, u64 out_capacity,
-                    u32 flags, const LaunchConfig &cfg, cudaStream_t st,
-                    DeviceBuffer &kmer_off, DeviceBuffer &packed,
-                    DeviceBuffer &invalid, DeviceBuffer &block_sums,
-                    DeviceBuffer &total, u32 *d_err, u64 n_kmers_hint) const;
-  void launch_search_only(u64 n_chars, const u64 *d_ends, u64 n_reads, u64 base,
-                          u64 *d_out, u64 out_capacity, u32 flags,
-                          const LaunchConfig &cfg, cudaStream_t st,
-                          DeviceBuffer &kmer_off, DeviceBuffer &packed,
-                          DeviceBuffer &invalid, u32 *d_err, u64 n_kmers) const;
 
   int device = 0;
   u64 num_bits = 0;

@@ -1,0 +1,320 @@
+#include <algorithm>
+#include <charconv>
+#include <cstring>
+#include <fstream>
+#include <stdexcept>
+
+#include "../../include/sbwt_b200.h"
+#include "host_io.hpp"
+
+namespace sbwt {
+
+namespace {
+
+FILE *open_out(const std::string &path) {
+  FILE *f = std::fopen(path.c_str(), "wb");
+  if (!f) throw std::runtime_error("Unable to open file for writing " + path);
+  std::setvbuf(f, nullptr, _IOFBF, 1 << 22);
+  return f;
+}
+
+void put_string(FILE *f, const std::string &s) {  // length-prefixed
+  const u64 n = s.size();
+  std::fwrite(&n, 8, 1, f);
+  std::fwrite(s.data(), 1, n, f);
+}
+
+void flush_buf(FILE *f, std::vector<char> &b) {
+  if (!b.empty() && std::fwrite(b.data(), 1, b.size(), f) != b.size())
+    throw std::runtime_error("write failed");
+  b.clear();
+}
+
+inline void put_u64(std::vector<char> &b, u64 v) {
+  char tmp[8];
+  std::memcpy(tmp, &v, 8);
+  b.insert(b.end(), tmp, tmp + 8);
+}
+
+inline void put_dec(std::vector<char> &b, u64 v) {
+  char tmp[24];
+  auto r = std::to_chars(tmp, tmp + sizeof(tmp), v);
+  b.insert(b.end(), tmp, r.ptr);
+}
+
+}  // namespace
+
+IndexResultsWriter::IndexResultsWriter(const std::string &prefix, IndexFormat fmt,
+                                       bool headers)
+    : fmt_(fmt) {
+  const char *ext = fmt == IndexFormat::Ascii ? ".txt" : fmt == IndexFormat::Binary ? ".bin" : ".bool";
+  f_ = open_out(prefix + ext);
+  if (headers) {
+    put_string(f_, fmt == IndexFormat::Ascii ? "ascii" : fmt == IndexFormat::Binary ? "binary" : "bool");
+    put_string(f_, fmt == IndexFormat::Bool ? "v2.0" : "v1.0");
+  }
+}
+
+IndexResultsWriter::~IndexResultsWriter() {
+  if (f_) {
+    flush_buf(f_, buf_);
+    std::fclose(f_);
+  }
+}
+
+void IndexResultsWriter::write(const u64 *res, const u64 *ends, u64 n_reads, u32 k) {
+  u64 prev = 0, t = 0;
+  for (u64 r = 0; r < n_reads; ++r) {
+    const u64 len = ends[r] - prev;
+    prev = ends[r];
+    const u64 m = len >= k ? len - k + 1 : 0;
+    for (u64 j = 0; j < m; ++j, ++t) {
+      const u64 v = res[t];
+      switch (fmt_) {
+        case IndexFormat::Ascii:
+          if (j) buf_.push_back(' ');
+          if (v == SBWT_NOT_FOUND) {
+            buf_.push_back('-');
+            buf_.push_back('1');
+          } else if (v == SBWT_INVALID) {
+            buf_.push_back('-');
+            buf_.push_back('2');
+          } else {
+            put_dec(buf_, v);
+          }
+          break;
+        case IndexFormat::Binary:
+          put_u64(buf_, v);  // -1 and -2 are the same bit patterns
+          break;
+        case IndexFormat::Bool:
+          buf_.push_back(v == SBWT_NOT_FOUND ? '1' : (v == SBWT_INVALID ? '2' : '0'));
+          break;
+      }
+    }
+    if (fmt_ == IndexFormat::Binary)
+      put_u64(buf_, (u64)-3);
+    else
+      buf_.push_back('\n');
+    if (buf_.size() > (1u << 22)) flush_buf(f_, buf_);
+  }
+  flush_buf(f_, buf_);
+}
+
+ColorResultsWriter::ColorResultsWriter(const std::string &prefix, ColorFormat fmt,
+                                       bool headers, u64 num_colors)
+    : fmt_(fmt), num_colors_(num_colors) {
+  const char *ext = fmt == ColorFormat::Ascii ? ".txt" : fmt == ColorFormat::Binary ? ".bin" : ".csv";
+  f_ = open_out(prefix + ext);
+  if (fmt == ColorFormat::Csv) {  // the csv header row is always written
+    for (u64 i = 1; i <= num_colors; ++i) {
+      put_dec(buf_, i);
+      buf_.push_back(i == num_colors ? '\n' : ',');
+    }
+    flush_buf(f_, buf_);
+  } else if (headers) {
+    put_string(f_, fmt == ColorFormat::Ascii ? "ascii" : "binary");
+    put_string(f_, "v1.0");
+  }
+}
+
+ColorResultsWriter::~ColorResultsWriter() {
+  if (f_) {
+    flush_buf(f_, buf_);
+    std::fclose(f_);
+  }
+}
+
+void ColorResultsWriter::write(const uint32_t *ids, const u64 *offs, u64 n_reads) {
+  std::vector<char> row;
+  if (fmt_ == ColorFormat::Csv) {
+    row.resize(num_colors_ * 2);
+    for (u64 i = 0; i < num_colors_; ++i) {
+      row[2 * i] = '0';
+      row[2 * i + 1] = (i + 1 == num_colors_) ? '\n' : ',';
+    }
+  }
+  for (u64 r = 0; r < n_reads; ++r) {
+    switch (fmt_) {
+      case ColorFormat::Ascii:
+        for (u64 t = offs[r]; t < offs[r + 1]; ++t) {
+          if (t != offs[r]) buf_.push_back(' ');
+          put_dec(buf_, ids[t]);
+        }
+        buf_.push_back('\n');
+        break;
+      case ColorFormat::Binary:
+        for (u64 t = offs[r]; t < offs[r + 1]; ++t) put_u64(buf_, ids[t]);
+        put_u64(buf_, (u64)-1);
+        break;
+      case ColorFormat::Csv: {
+        const size_t at = buf_.size();
+        buf_.insert(buf_.end(), row.begin(), row.end());
+        for (u64 t = offs[r]; t < offs[r + 1]; ++t) buf_[at + 2 * (u64)ids[t]] = '1';
+        break;
+      }
+    }
+    if (buf_.size() > (1u << 22)) flush_buf(f_, buf_);
+  }
+  flush_buf(f_, buf_);
+}
+
+IndexResults read_index_results(const std::string &path) {
+  std::ifstream in(path, std::ios::binary);
+  if (!in) throw std::runtime_error("Unable to open file " + path);
+  auto get_str = [&]() {
+    u64 n = 0;
+    in.read(reinterpret_cast<char *>(&n), 8);
+    if (!in || n > 64) throw std::runtime_error("The file has an incompatible format");
+    std::string s(n, '\0');
+    in.read(s.data(), (std::streamsize)n);
+    return s;
+  };
+  const std::string fmt = get_str();
+  if (fmt != "ascii" && fmt != "binary")
+    throw std::runtime_error("Unknown index file format '" + fmt + "'");
+  if (get_str() != "v1.0") throw std::runtime_error("The file has an incompatible version number");
+  std::vector<char> data((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+  IndexResults out;
+  out.offsets.push_back(0);
+  u64 nf = 0, inv = 0;
+  auto end_read = [&]() {
+    out.offsets.push_back(out.found.size());
+    out.not_found.push_back(nf);
+    out.invalid.push_back(inv);
+    nf = inv = 0;
+  };
+  bool open_read = false;
+  if (fmt == "ascii") {
+    size_t i = 0;
+    const size_t n = data.size();
+    while (i < n) {
+      const char c = data[i];
+      if (c == '\n') {
+        end_read();
+        open_read = false;
+        ++i;
+      } else if (c == '-') {  // -1 / -2 (other negatives are skipped)
+        if (i + 1 < n && data[i + 1] == '1') ++nf;
+        else if (i + 1 < n && data[i + 1] == '2') ++inv;
+        ++i;
+        while (i < n && data[i] >= '0') ++i;
+        open_read = true;
+      } else if (c >= '0' && c <= '9') {
+        u64 v = 0;
+        while (i < n && data[i] >= '0' && data[i] <= '9') v = v * 10 + (u64)(data[i++] - '0');
+        out.found.push_back(v);
+        open_read = true;
+      } else {
+        ++i;
+      }
+    }
+  } else {
+    const size_t nw = data.size() / 8;
+    for (size_t w = 0; w < nw; ++w) {
+      u64 v;
+      std::memcpy(&v, data.data() + 8 * w, 8);
+      if (v == (u64)-1) {
+        ++nf;
+        open_read = true;
+      } else if (v == (u64)-2) {
+        ++inv;
+        open_read = true;
+      } else if (v == (u64)-3) {
+        end_read();
+        open_read = false;
+      } else {
+        out.found.push_back(v);
+        open_read = true;
+      }
+    }
+  }
+  if (open_read) end_read();  // unterminated last read
+  return out;
+}
+
+}  // namespace sbwt
+
+// ---------------------------------------------------------------------------
+// C ABI of the host I/O (no GPU involved)
+// ---------------------------------------------------------------------------
+#include <cstdlib>
+
+#include "common.hpp"
+
+using namespace sbwt;
+
+extern "C" {
+
+void sbwt_free(void *p) { std::free(p); }
+
+int sbwt_fastx_read(const char *path, char **chars, uint64_t *n_chars, uint64_t **read_ends,
+                    uint64_t *n_reads) {
+  if (!path || !chars || !n_chars || !read_ends || !n_reads) {
+    set_last_error("null argument");
+    return SBWT_E_INVALID;
+  }
+  return guarded([&] {
+    ReadBatch b;
+    FastxReader r(path);
+    while (r.next_batch(b, ~0ULL, ~0ULL)) {
+    }
+    *chars = static_cast<char *>(std::malloc(std::max<size_t>(b.chars.size(), 1)));
+    *read_ends = static_cast<uint64_t *>(std::malloc(std::max<size_t>(b.ends.size(), 1) * 8));
+    if (!*chars || !*read_ends) throw std::bad_alloc();
+    std::memcpy(*chars, b.chars.data(), b.chars.size());
+    std::memcpy(*read_ends, b.ends.data(), b.ends.size() * 8);
+    *n_chars = b.chars.size();
+    *n_reads = b.ends.size();
+  });
+}
+
+int sbwt_write_index_results(const char *out_prefix, int format, int write_headers,
+                             const uint64_t *results, const uint64_t *read_ends,
+                             uint64_t n_reads, uint32_t k) {
+  if (!out_prefix || (n_reads && !read_ends) || format < 0 || format > 2) {
+    set_last_error("bad argument");
+    return SBWT_E_INVALID;
+  }
+  return guarded([&] {
+    IndexResultsWriter w(out_prefix, static_cast<IndexFormat>(format), write_headers != 0);
+    w.write(results, read_ends, n_reads, k);
+  });
+}
+
+int sbwt_write_color_results(const char *out_prefix, int format, int write_headers,
+                             const uint32_t *ids, const uint64_t *ids_offsets,
+                             uint64_t n_reads, uint64_t num_colors) {
+  if (!out_prefix || !ids_offsets || format < 0 || format > 2) {
+    set_last_error("bad argument");
+    return SBWT_E_INVALID;
+  }
+  return guarded([&] {
+    ColorResultsWriter w(out_prefix, static_cast<ColorFormat>(format), write_headers != 0,
+                         num_colors);
+    w.write(ids, ids_offsets, n_reads);
+  });
+}
+
+int sbwt_read_index_results(const char *path, uint64_t **found, uint64_t **offsets,
+                            uint64_t **not_found, uint64_t **invalid, uint64_t *n_reads) {
+  if (!path || !found || !offsets || !not_found || !invalid || !n_reads) {
+    set_last_error("null argument");
+    return SBWT_E_INVALID;
+  }
+  return guarded([&] {
+    IndexResults r = read_index_results(path);
+    auto dup = [](const std::vector<u64> &v) {
+      auto *p = static_cast<uint64_t *>(std::malloc(std::max<size_t>(v.size(), 1) * 8));
+      if (!p) throw std::bad_alloc();
+      std::memcpy(p, v.data(), v.size() * 8);
+      return p;
+    };
+    *found = dup(r.found);
+    *offsets = dup(r.offsets);
+    *not_found = dup(r.not_found);
+    *invalid = dup(r.invalid);
+    *n_reads = r.not_found.size();
+  });
+}
+
+}  // extern "C"

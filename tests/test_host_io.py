@@ -1,0 +1,133 @@
+"""Host I/O of the drop-in boundary (no GPU): the FASTA/FASTQ reader, the
+index-result writers and the index-file reader reproduce the reference's
+formats byte for byte on its own fixtures."""
+import ctypes as C
+import struct
+
+import numpy as np
+import pytest
+
+import oracle as O
+import sbwt_b200 as S
+from helpers import FIXTURE_FILES, GOLDEN, TMP, golden_sbwt_path, oracle_index
+
+U64P = C.POINTER(C.c_uint64)
+
+
+def lib():
+    L = S.lib()
+    L.sbwt_fastx_read.argtypes = [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]
+    L.sbwt_free.argtypes = [C.c_void_p]
+    L.sbwt_write_index_results.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p,
+                                           C.c_void_p, C.c_uint64, C.c_uint32]
+    L.sbwt_read_index_results.argtypes = [C.c_char_p] + [C.POINTER(C.c_void_p)] * 4 + \
+        [C.POINTER(C.c_uint64)]
+    L.sbwt_write_color_results.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p,
+                                           C.c_void_p, C.c_uint64, C.c_uint64]
+    return L
+
+
+def fastx_read(path):
+    L = lib()
+    ch, en = C.c_void_p(), C.c_void_p()
+    nc, nr = C.c_uint64(), C.c_uint64()
+    S.check(L.sbwt_fastx_read(str(path).encode(), C.byref(ch), C.byref(nc), C.byref(en),
+                              C.byref(nr)))
+    chars = C.string_at(ch, nc.value) if nc.value else b""
+    ends = np.ctypeslib.as_array(C.cast(en, U64P), (max(nr.value, 1),))[:nr.value].copy()
+    L.sbwt_free(ch)
+    L.sbwt_free(en)
+    return chars, ends
+
+
+@pytest.mark.parametrize("name", FIXTURE_FILES)
+def test_fastx_reader_matches_kseq_rules(name):
+    chars, ends = fastx_read(GOLDEN / "index_search" / name)
+    reads = O.parse_fastx((GOLDEN / "index_search" / name).read_bytes())
+    assert chars == b"".join(reads)
+    assert ends.tolist() == np.cumsum([len(r) for r in reads]).tolist()
+
+
+def test_fastx_reader_gzip_and_edge_cases(tmp_path):
+    import gzip
+    data = b">a\r\nAC\r\nGT\n>b\n>c\nTT\n\n@q x\nACG\nT\n+\nII\nII\n@r\n\n+\n\n"
+    p = tmp_path / "x.fq.gz"
+    with gzip.open(p, "wb") as f:
+        f.write(data)
+    chars, ends = fastx_read(p)
+    assert chars == b"ACGTTTACGT"
+    assert ends.tolist() == [4, 4, 6, 10, 10]
+
+
+@pytest.mark.parametrize("name", FIXTURE_FILES)
+def test_ascii_writer_reproduces_reference_bytes(name):
+    idx = oracle_index(golden_sbwt_path(), 10)
+    chars, ends = fastx_read(GOLDEN / "index_search" / name)
+    reads = O.parse_fastx((GOLDEN / "index_search" / name).read_bytes())
+    res = np.concatenate(O.index_search_reads(idx, reads) + [np.zeros(0, np.uint64)])
+    res = np.ascontiguousarray(res.astype(np.uint64))
+    out = TMP / ("w_" + name.split(".")[0])
+    S.check(lib().sbwt_write_index_results(str(out).encode(), 0, 1,
+                                           res.ctypes.data if len(res) else None,
+                                           ends.ctypes.data if len(ends) else None,
+                                           len(ends), 30))
+    exp = (GOLDEN / "index_search" / "expected" / (name.split(".")[0] + ".txt")).read_bytes()
+    assert (TMP / ("w_" + name.split(".")[0] + ".txt")).read_bytes() == exp
+
+
+def test_binary_and_bool_writers():
+    res = np.array([5, O.NOT_FOUND, O.INVALID, 7], np.uint64)
+    ends = np.array([33, 33, 64], np.uint64)  # 3 + 0 + 1 k-mers at k=31
+    for fmt, ext in ((1, ".bin"), (2, ".bool")):
+        out = TMP / f"wb_{fmt}"
+        S.check(lib().sbwt_write_index_results(str(out).encode(), fmt, 1, res.ctypes.data,
+                                               ends.ctypes.data, 3, 31))
+        b = (TMP / f"wb_{fmt}{ext}").read_bytes()
+        if fmt == 1:
+            assert b[:8 + 6 + 8 + 4] == struct.pack("<Q", 6) + b"binary" + struct.pack("<Q", 4) + b"v1.0"
+            vals = np.frombuffer(b[26:], np.uint64).tolist()
+            m3 = (1 << 64) - 3
+            assert vals == [5, O.NOT_FOUND, O.INVALID, m3, m3, 7, m3]
+        else:
+            assert b[8 + 4 + 8 + 4:] == b"012\n\n0\n"
+
+
+def test_index_file_reader_on_reference_fixtures():
+    L = lib()
+    for name in ("fasta1", "fasta2", "fasta3", "fasta4"):
+        path = GOLDEN / "color_search" / f"{name}.indexes.txt"
+        ptrs = [C.c_void_p() for _ in range(4)]
+        n = C.c_uint64()
+        S.check(L.sbwt_read_index_results(str(path).encode(), *[C.byref(p) for p in ptrs],
+                                          C.byref(n)))
+        nr = n.value
+        offs = np.ctypeslib.as_array(C.cast(ptrs[1], U64P), (nr + 1,)).copy()
+        found = np.ctypeslib.as_array(C.cast(ptrs[0], U64P), (max(int(offs[-1]), 1),))
+        nf = np.ctypeslib.as_array(C.cast(ptrs[2], U64P), (max(nr, 1),))
+        inv = np.ctypeslib.as_array(C.cast(ptrs[3], U64P), (max(nr, 1),))
+        rows = O.read_ascii_index_results(path)
+        assert nr == len(rows)
+        for r, toks in enumerate(rows):
+            assert found[offs[r]:offs[r + 1]].tolist() == [t for t in toks if t >= 0]
+            assert nf[r] == toks.count(-1) and inv[r] == toks.count(-2)
+        for p in ptrs:
+            L.sbwt_free(p)
+
+
+def test_color_writers():
+    ids = np.array([0, 2, 1], np.uint32)
+    offs = np.array([0, 2, 2, 3], np.uint64)
+    L = lib()
+    for fmt, ext in ((0, ".txt"), (1, ".bin"), (2, ".csv")):
+        out = TMP / f"cw_{fmt}"
+        S.check(L.sbwt_write_color_results(str(out).encode(), fmt, 1, ids.ctypes.data,
+                                           offs.ctypes.data, 3, 3))
+        b = (TMP / f"cw_{fmt}{ext}").read_bytes()
+        if fmt == 0:
+            assert b == struct.pack("<Q", 5) + b"ascii" + struct.pack("<Q", 4) + b"v1.0" + b"0 2\n\n1\n"
+        elif fmt == 1:
+            vals = np.frombuffer(b[26:], np.uint64).tolist()
+            assert vals == [0, 2, O.NOT_FOUND, O.NOT_FOUND, 1, O.NOT_FOUND]
+        else:
+            assert b == b"1,2,3\n1,0,1\n0,0,0\n0,1,0\n"

@@ -133,6 +133,30 @@ int sbwt_search_reads(const sbwt_index_t *index, const char *chars,
                       uint64_t results_capacity, uint64_t *n_results,
                       uint32_t flags, void *stream);
 
+/* The fused read search with NO device allocation, for callers that may not
+ * allocate device memory: code running while another framework owns the
+ * device allocator, serving loops where a cudaMalloc / cudaFree would stall
+ * or implicitly synchronize the device, hosts with a fixed memory budget.
+ * This entry point has no counterpart in the reference.
+ *   - All arrays are device pointers on the index's device (SBWT_DEVICE_POINTERS
+ *     is implied); the caller allocates inputs and outputs.  n_results (host,
+ *     may be NULL) receives the k-mer count; the call returns when the results
+ *     are written (it synchronizes `stream`).
+ *   - Scratch is one fixed array of about 9 MiB in the library's device
+ *     memory, present on every GPU that loads the library until the process
+ *     exits.  At most 8 Mi chars (8388608) and 256 Ki reads (262144) per call;
+ *     larger calls fail with SBWT_E_INVALID.
+ *   - The first call on a device looks up the array's device address; make
+ *     that first call before any stream capture on that device.
+ *   - Every call shares the array: calls that overlap on the GPU (several host
+ *     threads or streams at once) race and must be serialized by the caller.
+ * Results are identical to sbwt_search_reads. */
+int sbwt_search_reads_noalloc(const sbwt_index_t *index, const char *d_chars,
+                              uint64_t n_chars, const uint64_t *d_read_ends,
+                              uint64_t n_reads, uint64_t *d_results,
+                              uint64_t results_capacity, uint64_t *n_results,
+                              uint32_t flags, void *stream);
+
 /* ------------------------------------------------------------------------ */
 /* Colors step                                                               */
 /* ------------------------------------------------------------------------ */

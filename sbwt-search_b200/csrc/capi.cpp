@@ -216,6 +216,25 @@ int sbwt_pseudoalign(const sbwt_colors_t *colors, const uint64_t *sbwt_idxs,
   });
 }
 
+int sbwt_search_reads_noalloc(const sbwt_index_t *index, const char *d_chars,
+                              uint64_t n_chars, const uint64_t *d_read_ends,
+                              uint64_t n_reads, uint64_t *d_results,
+                              uint64_t results_capacity, uint64_t *n_results,
+                              uint32_t flags, void *stream) {
+  if (!index || (n_reads && (!d_read_ends || !d_results)) || (n_chars && !d_chars)) {
+    set_last_error("null argument");
+    return SBWT_E_INVALID;
+  }
+  return guarded([&] {
+    if ((flags & SBWT_MOVE_TO_KEY_KMER) && !index->impl->view.key_marks)
+      throw Error(SBWT_E_INVALID, "SBWT_MOVE_TO_KEY_KMER needs key k-mer marks");
+    index->impl->search_reads_noalloc(d_chars, n_chars, d_read_ends, n_reads, d_results,
+                                      results_capacity, n_results, flags,
+                                      static_cast<cudaStream_t>(stream),
+                                      default_launch_config());
+  });
+}
+
 // Tuning hook used by the autotuner and the benchmark (not part of the
 // reference-facing surface): sets the process-wide launch configuration.
 int sbwt_set_launch_config(uint32_t presearch_letters, uint32_t blocks_per_sm,

@@ -1052,6 +1052,126 @@ void IndexImpl::search_positions(const u64 *bit_seqs, u64 n_words, const u64 *po
   check_err_word(ws, s0);
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the fused read search
+// ---------------------------------------------------------------------------
+// Some callers may not allocate device memory themselves or through us: code
+// that runs while another framework owns the device allocator (a caching
+// allocator that must see every byte), latency-critical serving loops where a
+// cudaMalloc / cudaFree would stall or implicitly synchronize the device, and
+// hosts that have already sized their memory budget to the last byte.  For
+// them sbwt_search_reads_noalloc runs the same pipeline (scan, pack, tile
+// table, search kernel) with all its scratch in this fixed device array.
+//
+// Limits: at most kNoAllocMaxChars chars and kNoAllocMaxReads reads per call.
+// The array (about 9 MiB) lives on every GPU that loads this library until
+// the process exits.  All calls share it, so calls that overlap on the GPU
+// (from several host threads or streams) race: serialize them.
+constexpr u64 kNoAllocMaxChars = 8ULL << 20;
+constexpr u64 kNoAllocMaxReads = 1ULL << 18;
+constexpr u64 kNoAllocWords = kNoAllocMaxChars / 32;
+constexpr u64 kNoAllocOffKmerOff = 0;
+constexpr u64 kNoAllocOffPacked = kNoAllocOffKmerOff + (kNoAllocMaxReads + 1) * 8;
+constexpr u64 kNoAllocOffInvalid = kNoAllocOffPacked + (kNoAllocWords + 2) * 8;
+constexpr u64 kNoAllocOffBlockSums =
+    ((kNoAllocOffInvalid + (kNoAllocWords + 2) * 4 + 255) / 256) * 256;
+constexpr u64 kNoAllocOffTotal =
+    kNoAllocOffBlockSums + ((kNoAllocMaxReads + kScanTile - 1) / kScanTile + 1) * 8;
+constexpr u64 kNoAllocOffErr = kNoAllocOffTotal + 8;
+constexpr u64 kNoAllocOffTileRead = kNoAllocOffErr + 248;  // keeps 8-byte alignment
+constexpr u64 kNoAllocTileMin = 16;
+constexpr u64 kNoAllocBytes =
+    kNoAllocOffTileRead + (kNoAllocMaxChars / kNoAllocTileMin + 2) * 8;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch on `device`, looked up once per device
+// (with that device current) on the first call there.
+static unsigned char *noalloc_scratch_address(int device) {
+  static std::mutex mu;
+  static unsigned char *addr[64] = {};
+  if (device < 0 || device >= 64) throw Error(SBWT_E_INVALID, "device id out of range");
+  std::lock_guard<std::mutex> g(mu);
+  if (!addr[device]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      throw Error(SBWT_E_CUDA, std::string("cudaGetSymbolAddress(no-alloc scratch): ") +
+                                   cudaGetErrorString(e));
+    addr[device] = static_cast<unsigned char *>(p);
+  }
+  return addr[device];
+}
+
+void IndexImpl::search_reads_noalloc(const char *d_chars, u64 n_chars, const u64 *d_ends,
+                                     u64 n_reads, u64 *d_results, u64 capacity,
+                                     u64 *n_results, u32 flags, cudaStream_t st,
+                                     const LaunchConfig &cfg_in) const {
+  if (n_chars > kNoAllocMaxChars || n_reads > kNoAllocMaxReads)
+    throw Error(SBWT_E_INVALID,
+                "sbwt_search_reads_noalloc takes at most " +
+                    std::to_string(kNoAllocMaxChars) + " chars and " +
+                    std::to_string(kNoAllocMaxReads) + " reads per call (got " +
+                    std::to_string(n_chars) + " chars, " + std::to_string(n_reads) +
+                    " reads); split the batch or use sbwt_search_reads");
+  DeviceGuard g(device);
+  unsigned char *base = noalloc_scratch_address(device);
+  ReadsScratch sc{reinterpret_cast<u64 *>(base + kNoAllocOffKmerOff),
+                  reinterpret_cast<u64 *>(base + kNoAllocOffPacked),
+                  reinterpret_cast<uint32_t *>(base + kNoAllocOffInvalid),
+                  reinterpret_cast<u64 *>(base + kNoAllocOffBlockSums),
+                  reinterpret_cast<u64 *>(base + kNoAllocOffTotal),
+                  reinterpret_cast<u64 *>(base + kNoAllocOffTileRead),
+                  reinterpret_cast<uint32_t *>(base + kNoAllocOffErr)};
+  // the error word keeps the last call's value: clear it first
+  SBWT_CUDA(cudaMemsetAsync(sc.err, 0, 4, st));
+  u64 n_k = 0;
+  uint32_t err = 0;
+  if (n_reads) {
+    launch_prepare(device, k, d_chars, n_chars, d_ends, n_reads, 0, sc, st);
+    SBWT_CUDA(cudaMemcpyAsync(&n_k, sc.total, 8, cudaMemcpyDeviceToHost, st));
+    SBWT_CUDA(cudaMemcpyAsync(&err, sc.err, 4, cudaMemcpyDeviceToHost, st));
+    SBWT_CUDA(cudaStreamSynchronize(st));
+    if (err) throw Error(SBWT_E_INVALID, "read_ends are not non-decreasing within n_chars");
+  }
+  if (n_results) *n_results = n_k;
+  if (n_k > capacity)
+    throw Error(SBWT_E_CAPACITY, "results_capacity smaller than the k-mer count");
+  if (n_k == 0) return;
+  LaunchConfig cfg = cfg_in;  // the tile table is sized for tiles of >= 16
+  if (cfg.tile && cfg.tile < kNoAllocTileMin) cfg.tile = kNoAllocTileMin;
+  ReadsView rv{};
+  rv.packed = sc.packed;
+  rv.invalid = sc.invalid;
+  rv.ends = d_ends;
+  rv.kmer_off = sc.kmer_off;
+  rv.base = 0;
+  rv.n_reads = n_reads;
+  rv.n_kmers = n_k;
+  rv.tile = tile_size(device, n_k, cfg);
+  rv.n_tiles = (n_k + rv.tile - 1) / rv.tile;
+  rv.out = d_results;
+  rv.out_capacity = capacity;
+  tile_reads_kernel<<<grid_for(device, n_reads, 256, 16), 256, 0, st>>>(sc.kmer_off, n_reads,
+                                                                        rv.tile, sc.tile_read);
+  const int grid = grid_for(device, rv.n_tiles, 256, cfg.blocks_per_sm);
+  const SbwtView sv = view_for(cfg.presearch_letters);
+  const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
+  if (!(flags & SBWT_PER_KMER_WALK) && view.suffix_group_starts)
+    search_reads_kernel<true, false><<<grid, 256, 0, st>>>(sv, rv, sc.tile_read, mtk, sc.err,
+                                                            nullptr);
+  else
+    search_reads_kernel<false, false><<<grid, 256, 0, st>>>(sv, rv, sc.tile_read, mtk, sc.err,
+                                                             nullptr);
+  SBWT_CUDA(cudaGetLastError());
+  SBWT_CUDA(cudaMemcpyAsync(&err, sc.err, 4, cudaMemcpyDeviceToHost, st));
+  SBWT_CUDA(cudaStreamSynchronize(st));
+  if (err)
+    throw Error(SBWT_E_TIMEOUT,
+                "key k-mer walk did not reach a key k-mer (node without an outgoing "
+                "edge); results of those k-mers are unspecified");
+}
+
 }  // namespace sbwt
 
 extern "C" {

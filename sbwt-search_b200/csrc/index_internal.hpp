@@ -29,6 +29,10 @@ struct IndexImpl {
                     u64 n_reads, u64 *results, u64 capacity, u64 *n_results,
                     u32 flags, cudaStream_t st, const LaunchConfig &cfg) const;
 
+  void search_reads_noalloc(const char *d_chars, u64 n_chars, const u64 *d_ends,
+                            u64 n_reads, u64 *d_results, u64 capacity, u64 *n_results,
+                            u32 flags, cudaStream_t st, const LaunchConfig &cfg) const;
+
   int device = 0;
   u64 num_bits = 0;
   u32 k = 0;

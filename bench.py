@@ -237,8 +237,7 @@ def main():
     torch.cuda.synchronize()
     ctr = (C.c_uint64 * 4)()
     L.sbwt_profile_read(None, None, None, ctr)
-    n_full, n_stream, full_sectors, n_other = (int(ctr[0]), int(ctr[1]), int(ctr[2]),
-                                               int(ctr[3]))
+    n_pre, n_block, n_sg, n_probe = (int(ctr[0]), int(ctr[1]), int(ctr[2]), int(ctr[3]))
     L.sbwt_profile_enable(0, 0)
 
     for _ in range(args.warmup):
@@ -301,12 +300,10 @@ def main():
     peak, peak_kind = load_peaks()
     kern_ms = search_ms.value / max(1, search_launches.value)
     # algorithmic bytes per launch (what this kernel's algorithm must move):
-    # 32 B per rank-block sector of the full-search steps, per presearch entry
-    # (one per full search), two per stream step (rank block + suffix-group
-    # word), one per extra stream iteration; 8 B result per k-mer; 2 bits of
+    # one 32-byte sector per presearch entry, per rank block and per
+    # suffix-group word the search reads; 8 B result per k-mer; 2 bits of
     # packed input + 1 invalid bit per char.
-    alg_bytes = ((full_sectors + n_full + 2 * n_stream + n_other) * 32 + n_kmers * 8 +
-                 n_chars / 4 + n_chars / 8)
+    alg_bytes = ((n_pre + n_block + n_sg) * 32 + n_kmers * 8 + n_chars / 4 + n_chars / 8)
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9
 
     cpu = None
@@ -338,9 +335,8 @@ def main():
                      "frac": achieved / peak, "traffic": None,
                      "peak_kind": peak_kind, "kernel": "search_reads_kernel",
                      "kernel_ms": kern_ms,
-                     "work": {"full_searches": n_full, "stream_steps": n_stream,
-                              "full_search_block_sectors": full_sectors,
-                              "extra_stream_iterations": n_other,
+                     "work": {"presearch_lookups": n_pre, "rank_block_sectors": n_block,
+                              "suffix_group_words": n_sg, "probe_iterations": n_probe,
                               "bytes_per_kmer": alg_bytes / n_kmers}},
         "cpu_baseline": cpu,
         "e2e": e2e,

@@ -235,11 +235,23 @@ int sbwt_write_color_results(const char *out_prefix, int format,
  * per work tile, chars per chunk of the host-pointer pipeline. */
 int sbwt_set_launch_config(uint32_t presearch_letters, uint32_t blocks_per_sm,
                            uint64_t tile, uint64_t chunk_chars);
+/* Length of the read search's absent-prefix probe (0 = automatic,
+ * 0xFFFFFFFF = off).  Results never depend on it. */
+int sbwt_set_probe_length(uint32_t probe_len);
+/* Persisting-L2 access-policy window over the index's rank blocks on the
+ * search launches (0 = off, the default; 1 = on: sets this context's
+ * persisting-L2 size). */
+int sbwt_set_l2_window(int enabled);
 /* Off by default.  When enabled, every search-kernel launch is timed with
  * CUDA events on its own stream and this library's kernel launches are
  * counted; count_work also counts full searches / streaming steps / rank
  * block sectors of the read search kernel. */
 int sbwt_profile_enable(int enabled, int count_work);
+/* Random 32-byte-sector gather throughput of `device` over a `bytes` buffer
+ * (allocated inside the call), `chains` independent dependent-load chains
+ * per thread (1, 2, 4 or 8): the roofline denominator of the search kernels. */
+int sbwt_measure_random_sectors(int device, uint64_t bytes, int chains,
+                                double *gbs, double *sectors_per_s);
 /* Reads and resets the totals (any pointer may be NULL). */
 int sbwt_profile_read(double *search_ms, uint64_t *search_launches,
                       uint64_t *launches, uint64_t counters[4]);

@@ -325,6 +325,7 @@ struct ReadsView {
   uint64_t n_tiles;
   uint64_t *out;
   uint64_t out_capacity;
+  uint32_t probe_len;       // L of the absent-prefix probe (0 = off)
 };
 
 __device__ __forceinline__ bool invalid_at(const uint32_t *inv, uint64_t i) {
@@ -370,46 +371,142 @@ __global__ void tile_reads_kernel(const uint64_t *kmer_off, uint64_t n_reads, ui
 
 // Fused index step over reads.
 //
-// Work unit = a tile of consecutive k-mer result slots.  Inside a read, a
-// k-mer that follows a found k-mer is resolved by ONE step along the
-// successor edge of the previous node (stream step) instead of a full search;
-// the answer is the same because a k-mer's node is unique.
+// Work unit = a tile of consecutive k-mer result slots.  Inside a read:
+//  * a k-mer that follows a found k-mer is resolved by ONE step along the
+//    successor edge of the previous node (stream step); the answer is the
+//    same as a full search because a k-mer's node is unique;
+//  * when a search fails at char f (the string x[pos..f] is not a suffix of
+//    any node), the kernel probes the L-mer x[f-L+1..f].  If it is absent,
+//    every k-mer starting in (pos, f-L+1] holds it as a prefix of its own
+//    prefix x[j..f], and every prefix of a k-mer in the SBWT is a suffix of
+//    some node, so all those k-mers are reported not found without a search.
+//    This removes most of the full searches around sequencing errors.
 //
-// Every lane runs its own state machine and each loop iteration performs one
-// memory round trip for every active lane: addresses are computed in divergent
-// code, then the warp reconverges (the warp-uniform exit test) and issues the
-// loads together, then consumes them in divergent code.  A lane in the middle
-// of a 19-step full search therefore never makes the other 31 lanes wait for
-// 19 round trips, and no lane's round trip is serialized behind another's.
-//   mode 0: the k-mer at `slot` needs its first load (stream step if the
-//           previous k-mer was found, else the presearch entry);
-//   mode 1: full search, next char wi (both rank blocks of [l, r]);
-//   mode 2: stream step, suffix-group-start word u (bits <= ubit) to find the
-//           first node g of v's suffix group;
-//   mode 3: stream step, rank block of char c at the group start u.
-template <bool STREAM, bool COUNT>
-__global__ void __launch_bounds__(256) search_reads_kernel(SbwtView s, ReadsView rv,
-                                                           const uint64_t *__restrict__ tile_read,
-                                                           uint32_t move_to_key,
-                                                           uint32_t *err,
-                                                           unsigned long long *counters) {
+// Every lane runs its own state machine; each loop iteration is one memory
+// round trip per active lane: addresses are computed per lane, the warp
+// reconverges (warp-uniform exit test) and issues the loads together, then
+// ONE shared rank computation serves every mode, followed by small per-mode
+// updates.
+//   M_NEW   : the k-mer at `slot` needs its first load (stream step if the
+//             previous k-mer was found, else the presearch entry);
+//   M_WALK  : full search, next char wi (rank blocks of l and r + 1);
+//   M_SG    : stream step, suffix-group-start word u (bits <= ubit);
+//   M_GS    : stream step, rank block of char c at the group start u;
+//   M_PPRE  : probe, presearch entry of x[m..m+lvl);
+//   M_PROBE : probe, next char wi up to probe_end.
+// Per-lane register window over the packed chars and invalid bits of a read:
+// words wbase and wbase + 1, i.e. chunk positions [32 wbase, 32 wbase + 64).
+// With k <= 33 every char the lane needs for the k-mer at pos (and for a probe
+// started when that k-mer failed) lies in the window of wbase = pos / 32, so
+// after the window moves the search reads no char from memory.
+struct CharWindow {
+  uint64_t w0, w1;   // packed words wbase, wbase + 1
+  uint64_t inv;      // invalid bits of both words (word wbase in the low half)
+  uint64_t wbase;
+  __device__ __forceinline__ void init(const uint64_t *packed, const uint32_t *invalid) {
+    wbase = ~1ULL;  // neither equal to nor one below any real word index
+    w0 = w1 = inv = 0;
+    (void)packed;
+    (void)invalid;
+  }
+  __device__ __forceinline__ void move_to(const uint64_t *packed, const uint32_t *invalid,
+                                          uint64_t pos) {
+    const uint64_t wb = pos >> 5;
+    if (wb == wbase) return;
+    if (wb == wbase + 1) {
+      w0 = w1;
+      w1 = __ldg(packed + wb + 1);
+      inv = (inv >> 32) | ((uint64_t)__ldg(invalid + wb + 1) << 32);
+    } else {
+      w0 = __ldg(packed + wb);
+      w1 = __ldg(packed + wb + 1);
+      inv = (uint64_t)__ldg(invalid + wb) | ((uint64_t)__ldg(invalid + wb + 1) << 32);
+    }
+    wbase = wb;
+  }
+  __device__ __forceinline__ uint32_t char_at(uint64_t i) const {
+    const uint32_t off = (uint32_t)(i - 32 * wbase);
+    const uint64_t w = off < 32 ? w0 : w1;
+    return (uint32_t)((w >> (62 - 2 * (off & 31))) & 3ULL);
+  }
+  // first n chars (1 <= n <= 32) from position i, first char on top
+  __device__ __forceinline__ uint64_t prefix(uint64_t i, uint32_t n) const {
+    const uint32_t off = (uint32_t)(i - 32 * wbase);
+    uint64_t v;
+    if (off < 32) {
+      v = w0 << (2 * off);
+      if (off) v |= w1 >> (64 - 2 * off);
+    } else {
+      v = w1 << (2 * (off - 32));
+    }
+    return v >> (64 - 2 * n);
+  }
+  __device__ __forceinline__ bool invalid_at(uint64_t i) const {
+    return (inv >> (uint32_t)(i - 32 * wbase)) & 1ULL;
+  }
+  // highest invalid position in [a, b) (b - a <= 63), or -1
+  __device__ __forceinline__ int64_t last_invalid(uint64_t a, uint64_t b) const {
+    if (b <= a) return -1;
+    const uint32_t oa = (uint32_t)(a - 32 * wbase), ob = (uint32_t)(b - 32 * wbase);
+    uint64_t m = inv & (ob >= 64 ? ~0ULL : ((1ULL << ob) - 1));
+    m &= ~((1ULL << oa) - 1);
+    return m ? (int64_t)(32 * wbase + 63 - __clzll(m)) : -1;
+  }
+};
+
+enum : uint32_t { M_NEW = 0, M_WALK = 1, M_SG = 2, M_GS = 3, M_PPRE = 4, M_PROBE = 5 };
+enum : uint32_t { K_NONE = 0, K_BLOCK = 1, K_PRE = 2, K_SGW = 3 };
+// SBWTs with fewer nodes than this use 32-bit node arithmetic in the search.
+constexpr uint64_t kNarrowLimit = (uint64_t)kBlockBits << kSuperchunkShift;
+
+#ifndef SBWT_SEARCH_MIN_BLOCKS
+#define SBWT_SEARCH_MIN_BLOCKS 4  // 256-thread blocks per SM the register budget targets
+#endif
+
+// Node-index arithmetic of the search kernel: 32-bit when the SBWT has fewer
+// than 224 * 2^24 nodes (one superchunk: no l0 table, all ranks fit in 32
+// bits), else 64-bit.
+template <class I>
+struct NodeMath {
+  static constexpr I kNone = ~I(0);
+  __device__ __forceinline__ static I block(I i) {
+    return (I)((uint32_t)((uint64_t)i >> 5) / 7u);
+  }
+  __device__ __forceinline__ static I rank(const SbwtView &s, uint32_t c, I b,
+                                           const Block &B, uint32_t q) {
+    if (sizeof(I) == 4) return (I)s.c_map[c] + (I)block_rank(B, q);
+    return (I)(s.c_map[c] + s.l0[c][(uint64_t)b >> kSuperchunkShift] + block_rank(B, q));
+  }
+};
+
+template <bool STREAM, bool COUNT, bool SMALLK, class I>
+__global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
+    search_reads_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
+                        uint32_t move_to_key, uint32_t *err,
+                        unsigned long long *counters) {
+  using NM = NodeMath<I>;
+  constexpr I NONE = NM::kNone;
   const uint32_t k = s.k;
+  const uint32_t L = rv.probe_len;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  uint64_t n_pre = 0, n_stream = 0, n_walk_sectors = 0, n_other = 0;
+  uint64_t n_pre = 0, n_block = 0, n_sg = 0, n_probe = 0;
   uint64_t tile = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  uint64_t slot = 0, slot_end = 0, r = 0, r_next = 0, pos = 0;
+  uint64_t slot = 0, slot_end = 0, r = 0, r_next = 0, pos = 0, skip_until = 0;
   int64_t last_inv = -1;
-  uint64_t v = SBWT_NOT_FOUND;  // node of the previous k-mer of this read
-  uint64_t l = 0, rr = 0, wi = 0, u = 0;
-  uint32_t mode = 0, c = 0, ubit = 63;
+  I v = NONE;  // node of the previous k-mer of this read
+  I l = 0, rr = 0, u = 0;
+  uint64_t wi = 0, probe_end = 0, probe_skip = 0, pu = 0;
+  uint32_t mode = M_NEW, c = 0, ubit = 63;
   bool done = false;
-  const uint64_t pre_base = presearch_level_offset(s.p);
+  CharWindow cw;
+  cw.init(rv.packed, rv.invalid);
   while (true) {
-    // ---- phase 1 (divergent): decide this lane's loads --------------------
-    const Block *addrA = nullptr, *addrB = nullptr;
+    // ---- phase 1 (per lane): what to load --------------------------------
+    uint32_t kind = K_NONE;
+    I pa = 0, pb = 0;
     uint64_t pre_e = 0;
     if (!done) {
-      if (mode == 0) {
+      if (mode == M_NEW) {
         while (true) {
           if (slot >= slot_end) {  // next tile
             if (tile >= rv.n_tiles) {
@@ -423,83 +520,127 @@ __global__ void __launch_bounds__(256) search_reads_kernel(SbwtView s, ReadsView
             r_next = __ldg(rv.kmer_off + r + 1);
             pos = (r ? __ldg(rv.ends + r - 1) : rv.base) - rv.base +
                   (slot - __ldg(rv.kmer_off + r));
-            last_inv = last_invalid(rv.invalid, pos, pos + k - 1);
-            v = SBWT_NOT_FOUND;
+            if (SMALLK) {
+              cw.move_to(rv.packed, rv.invalid, pos);
+              last_inv = cw.last_invalid(pos, pos + k - 1);
+            } else {
+              last_inv = last_invalid(rv.invalid, pos, pos + k - 1);
+            }
+            v = NONE;
+            skip_until = 0;
           } else if (slot == r_next) {  // next read
             do {
               r_next = __ldg(rv.kmer_off + (++r) + 1);
             } while (r_next == slot);
             pos = __ldg(rv.ends + r - 1) - rv.base;
-            last_inv = last_invalid(rv.invalid, pos, pos + k - 1);
-            v = SBWT_NOT_FOUND;
+            if (SMALLK) {
+              cw.move_to(rv.packed, rv.invalid, pos);
+              last_inv = cw.last_invalid(pos, pos + k - 1);
+            } else {
+              last_inv = last_invalid(rv.invalid, pos, pos + k - 1);
+            }
+            v = NONE;
+            skip_until = 0;
           }
           const uint64_t newc = pos + k - 1;
-          if (invalid_at(rv.invalid, newc)) last_inv = (int64_t)newc;
-          if (last_inv < (int64_t)pos) break;  // a k-mer to search
-          if (slot < rv.out_capacity) __stcs(rv.out + slot, (unsigned long long)SBWT_INVALID);
-          v = SBWT_NOT_FOUND;
+          if (SMALLK) cw.move_to(rv.packed, rv.invalid, pos);
+          if (SMALLK ? cw.invalid_at(newc) : invalid_at(rv.invalid, newc))
+            last_inv = (int64_t)newc;
+          uint64_t known = 0;
+          if (last_inv >= (int64_t)pos) {
+            known = SBWT_INVALID;
+          } else if (slot < skip_until) {
+            known = SBWT_NOT_FOUND;
+          } else {
+            break;  // a k-mer to search
+          }
+          if (slot < rv.out_capacity) __stcs(rv.out + slot, (unsigned long long)known);
+          v = NONE;
           ++slot;
           ++pos;
         }
         if (!done) {
-          if (STREAM && v != SBWT_NOT_FOUND) {
-            c = char_at(rv.packed, pos + k - 1);
-            addrA = s.blocks[c] + block_of(v);
-            if (COUNT) ++n_stream;
+          if (STREAM && v != NONE) {
+            kind = K_BLOCK;
+            c = SMALLK ? cw.char_at(pos + k - 1) : char_at(rv.packed, pos + k - 1);
+            pa = pb = v;
           } else {
-            pre_e = pre_base + chars_prefix(rv.packed, pos, s.p);
-            addrA = s.wide ? chunk_of(s.presearch, 2 * pre_e) : chunk_of(s.presearch, pre_e);
-            if (COUNT) ++n_pre;
+            kind = K_PRE;
+            pre_e = presearch_level_offset(s.p) +
+                    (SMALLK ? cw.prefix(pos, s.p) : chars_prefix(rv.packed, pos, s.p));
           }
         }
-      } else if (mode == 1) {
-        c = char_at(rv.packed, wi);
-        const uint64_t bl = block_of(l), br = block_of(rr + 1);
-        addrA = s.blocks[c] + bl;
-        if (br != bl) addrB = s.blocks[c] + br;
-        if (COUNT) n_walk_sectors += (br != bl) ? 2 : 1;
-      } else if (mode == 2) {
-        addrA = chunk_of(s.suffix_group_starts, u);
-        if (COUNT) ++n_other;
-      } else {
-        addrA = s.blocks[c] + block_of(u);
-        if (COUNT) ++n_other;
+      } else if (mode == M_WALK || mode == M_PROBE) {
+        kind = K_BLOCK;
+        c = SMALLK ? cw.char_at(wi) : char_at(rv.packed, wi);
+        pa = l;
+        pb = rr + 1;
+      } else if (mode == M_SG) {
+        kind = K_SGW;
+      } else if (mode == M_GS) {
+        kind = K_BLOCK;
+        pa = pb = u;
+      } else {  // M_PPRE: pu = probe start m, ubit = level
+        kind = K_PRE;
+        pre_e = presearch_level_offset(ubit) +
+                (SMALLK ? cw.prefix(pu, ubit) : chars_prefix(rv.packed, pu, ubit));
       }
     }
     if (__all_sync(0xFFFFFFFFu, done)) break;
     // ---- phase 2 (converged): the loads ------------------------------------
+    const I ba = NM::block(pa), bb = NM::block(pb);
+    const Block *addrA = nullptr, *addrB = nullptr;
+    if (kind == K_BLOCK) {
+      addrA = s.blocks[c] + ba;
+      if (bb != ba) addrB = s.blocks[c] + bb;
+    } else if (kind == K_PRE) {
+      addrA = s.wide ? chunk_of(s.presearch, 2 * pre_e) : chunk_of(s.presearch, pre_e);
+    } else if (kind == K_SGW) {
+      addrA = chunk_of(s.suffix_group_starts, (uint64_t)u);
+    }
     Block A = Block{0, 0, 0, 0}, B;
     if (addrA) A = load_block(addrA);
     B = A;
     if (addrB) B = load_block(addrB);
+    if (COUNT) {
+      n_pre += kind == K_PRE;
+      n_block += (kind == K_BLOCK) + (addrB != nullptr);
+      n_sg += kind == K_SGW;
+      n_probe += (mode == M_PPRE || mode == M_PROBE);
+    }
     if (done) continue;
-    // ---- phase 3 (divergent): consume ----------------------------------------
-    uint64_t emit = 0;
-    bool emitted = false;
-    if (mode == 0) {
-      if (STREAM && v != SBWT_NOT_FOUND) {
-        const uint64_t b = block_of(v);
-        const uint32_t q = (uint32_t)(v - b * kBlockBits);
-        if (block_bit(A, q)) {  // v starts its suffix group and has edge c
-          emit = s.c_map[c] + s.l0[c][b >> kSuperchunkShift] + block_rank(A, q);
-          emitted = true;
-        } else {  // find the first node of v's suffix group
-          u = v >> 6;
-          ubit = (uint32_t)(v & 63);
-          mode = 2;
-        }
+    // ---- phase 3: one shared rank computation, then per-mode updates ------
+    const uint32_t qa = (uint32_t)(pa - ba * kBlockBits), qb = (uint32_t)(pb - bb * kBlockBits);
+    const I ra = NM::rank(s, c, ba, A, qa);
+    const I rb = NM::rank(s, c, bb, B, qb);
+    const bool bita = block_bit(A, qa);
+    I pl = 0, pr = 0;
+    if (kind == K_PRE) {
+      if (!s.wide) {
+        const uint64_t e = chunk_word(A, pre_e);
+        pl = (I)(e >> 32);
+        pr = (I)(e & 0xFFFFFFFFULL);
       } else {
-        uint64_t pl, pr;
-        if (!s.wide) {
-          const uint64_t e = chunk_word(A, pre_e);
-          pl = e >> 32;
-          pr = e & 0xFFFFFFFFULL;
-        } else {
-          pl = chunk_word(A, 2 * pre_e);
-          pr = chunk_word(A, 2 * pre_e + 1);
-        }
-        if (pl > pr) {
-          emit = SBWT_NOT_FOUND;
+        pl = (I)chunk_word(A, 2 * pre_e);
+        pr = (I)chunk_word(A, 2 * pre_e + 1);
+      }
+    }
+    I emit = 0;
+    bool emitted = false;
+    int64_t fail_at = -1;  // char where a search of this k-mer failed
+    switch (mode) {
+      case M_NEW:
+        if (kind == K_BLOCK) {  // stream step from v
+          if (bita) {
+            emit = ra;
+            emitted = true;
+          } else {
+            u = v >> 6;
+            ubit = (uint32_t)(v & 63);
+            mode = M_SG;
+          }
+        } else if (pl > pr) {
+          emit = NONE;
           emitted = true;
         } else if (s.p >= k) {
           emit = pl;
@@ -508,66 +649,103 @@ __global__ void __launch_bounds__(256) search_reads_kernel(SbwtView s, ReadsView
           l = pl;
           rr = pr;
           wi = pos + s.p;
-          mode = 1;
+          mode = M_WALK;
         }
-      }
-    } else if (mode == 1) {
-      const uint64_t bl = block_of(l), r1 = rr + 1, br = block_of(r1);
-      const uint64_t cc = s.c_map[c];
-      const uint64_t nl = cc + s.l0[c][bl >> kSuperchunkShift] +
-                          block_rank(A, (uint32_t)(l - bl * kBlockBits));
-      const uint64_t nr = cc + s.l0[c][br >> kSuperchunkShift] +
-                          block_rank(B, (uint32_t)(r1 - br * kBlockBits)) - 1;
-      l = nl;
-      rr = nr;
-      ++wi;
-      if (l > rr) {
-        emit = SBWT_NOT_FOUND;
-        emitted = true;
-      } else if (wi == pos + k) {
-        emit = l;
-        emitted = true;
-      }
-    } else if (mode == 2) {
-      const uint64_t w = chunk_word(A, u) & low_mask(ubit + 1);
-      if (w) {
-        const uint64_t g = u * 64 + 63 - __clzll(w);
-        if (g == v) {  // v starts its group and has no edge c
-          emit = SBWT_NOT_FOUND;
+        break;
+      case M_WALK:
+        l = ra;
+        rr = rb - 1;
+        ++wi;
+        if (l > rr) {
+          emit = NONE;
+          emitted = true;
+          fail_at = (int64_t)wi - 1;
+        } else if (wi == pos + k) {
+          emit = l;
+          emitted = true;
+        }
+        break;
+      case M_SG: {
+        const uint64_t w = chunk_word(A, (uint64_t)u) & low_mask(ubit + 1);
+        if (w) {
+          const I g = (I)((uint64_t)u * 64 + 63 - __clzll(w));
+          if (g == v) {  // v starts its group and has no edge c
+            emit = NONE;
+            emitted = true;
+            fail_at = (int64_t)(pos + k - 1);
+          } else {
+            u = g;
+            mode = M_GS;
+          }
+        } else if (u == 0) {
+          emit = NONE;  // no group start below v: malformed SBWT
           emitted = true;
         } else {
-          u = g;
-          mode = 3;
+          --u;
+          ubit = 63;
         }
-      } else if (u == 0) {
-        emit = SBWT_NOT_FOUND;  // no group start below v: malformed SBWT
-        emitted = true;
-      } else {
-        --u;
-        ubit = 63;
+        break;
       }
-    } else {
-      const uint64_t b = block_of(u);
-      const uint32_t q = (uint32_t)(u - b * kBlockBits);
-      emit = block_bit(A, q) ? s.c_map[c] + s.l0[c][b >> kSuperchunkShift] + block_rank(A, q)
-                             : SBWT_NOT_FOUND;
-      emitted = true;
+      case M_GS:
+        emitted = true;
+        if (bita) {
+          emit = ra;
+        } else {
+          emit = NONE;
+          fail_at = (int64_t)(pos + k - 1);
+        }
+        break;
+      case M_PPRE:
+        if (pl > pr) {
+          skip_until = probe_skip;  // x[m..probe_end] is absent
+          mode = M_NEW;
+        } else if (pu + ubit > probe_end) {
+          mode = M_NEW;  // present: nothing to skip
+        } else {
+          l = pl;
+          rr = pr;
+          wi = pu + ubit;
+          mode = M_PROBE;
+        }
+        break;
+      default:  // M_PROBE
+        l = ra;
+        rr = rb - 1;
+        ++wi;
+        if (l > rr) {
+          skip_until = probe_skip;
+          mode = M_NEW;
+        } else if (wi > probe_end) {
+          mode = M_NEW;
+        }
+        break;
     }
     if (emitted) {
       v = emit;
-      uint64_t res = emit;
-      if (move_to_key && emit != SBWT_NOT_FOUND) res = key_walk(s, emit, err);
+      uint64_t res = emit == NONE ? SBWT_NOT_FOUND : (uint64_t)emit;
+      if (move_to_key && res != SBWT_NOT_FOUND) res = key_walk(s, res, err);
       if (slot < rv.out_capacity) __stcs(rv.out + slot, (unsigned long long)res);
+      // a failed search may prove the next k-mers absent: probe x[m..f]
+      if (L && fail_at >= 0 && (uint64_t)fail_at >= pos + L + 1) {
+        const uint64_t m = (uint64_t)fail_at - L + 1;  // > pos + 1
+        probe_end = (uint64_t)fail_at;
+        probe_skip = slot + (m - pos) + 1;  // slots of k-mers starting at pos+1..m
+        pu = m;
+        ubit = min(L, s.p);
+        mode = M_PPRE;
+      } else {
+        mode = M_NEW;
+      }
       ++slot;
       ++pos;
-      mode = 0;
+      if (SMALLK && mode == M_PPRE) cw.move_to(rv.packed, rv.invalid, pos);
     }
   }
   if (COUNT) {
     atomicAdd(counters + 0, (unsigned long long)n_pre);
-    atomicAdd(counters + 1, (unsigned long long)n_stream);
-    atomicAdd(counters + 2, (unsigned long long)n_walk_sectors);
-    atomicAdd(counters + 3, (unsigned long long)n_other);
+    atomicAdd(counters + 1, (unsigned long long)n_block);
+    atomicAdd(counters + 2, (unsigned long long)n_sg);
+    atomicAdd(counters + 3, (unsigned long long)n_probe);
   }
 }
 
@@ -598,9 +776,44 @@ static void note_launches(uint64_t n) {
   p.launches += n;
 }
 
+// Launch attributes of a search kernel: the persisting L2 window over the
+// index's hot data when the device supports one.
+struct LaunchAttrs {
+  cudaLaunchAttribute attr[1];
+  unsigned n = 0;
+};
+static LaunchAttrs search_attrs(const void *hot, u64 window_bytes, u64 persist_bytes) {
+  LaunchAttrs a;
+  if (hot && window_bytes && persist_bytes) {
+    a.attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+    a.attr[0].val.accessPolicyWindow.base_ptr = const_cast<void *>(hot);
+    a.attr[0].val.accessPolicyWindow.num_bytes = window_bytes;
+    a.attr[0].val.accessPolicyWindow.hitRatio =
+        (float)std::min(1.0, (double)persist_bytes / (double)window_bytes);
+    a.attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    a.attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    a.n = 1;
+  }
+  return a;
+}
+
+template <class... KArgs, class... Args>
+static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStream_t st,
+                      const LaunchAttrs &la, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)threads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cfg.attrs = const_cast<cudaLaunchAttribute *>(la.attr);
+  cfg.numAttrs = la.n;
+  SBWT_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
+}
+
 static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsView &rv,
                                  const uint64_t *tile_read, uint32_t mtk, uint32_t *d_err,
-                                 int grid, int threads, cudaStream_t st) {
+                                 int grid, int threads, cudaStream_t st,
+                                 const LaunchAttrs &la) {
   Profile &p = profile();
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (p.enabled) {
@@ -617,17 +830,31 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
     }
     ctr = p.d_counters.get<unsigned long long>();
   }
+  const bool small = sv.k <= 33;
+  const bool narrow = sv.num_bits < kNarrowLimit;
+#define SBWT_LAUNCH(S_, C_, K_)                                                          \
+  do {                                                                                   \
+    if (narrow)                                                                          \
+      launch_ex(search_reads_kernel<S_, C_, K_, uint32_t>, grid, threads, st, la, sv, rv, \
+                tile_read, mtk, d_err, ctr);                                             \
+    else                                                                                 \
+      launch_ex(search_reads_kernel<S_, C_, K_, uint64_t>, grid, threads, st, la, sv, rv, \
+                tile_read, mtk, d_err, ctr);                                             \
+  } while (0)
   if (ctr) {
-    if (stream)
-      search_reads_kernel<true, true><<<grid, threads, 0, st>>>(sv, rv, tile_read, mtk, d_err, ctr);
-    else
-      search_reads_kernel<false, true><<<grid, threads, 0, st>>>(sv, rv, tile_read, mtk, d_err, ctr);
+    if (stream) {
+      if (small) SBWT_LAUNCH(true, true, true); else SBWT_LAUNCH(true, true, false);
+    } else {
+      if (small) SBWT_LAUNCH(false, true, true); else SBWT_LAUNCH(false, true, false);
+    }
   } else {
-    if (stream)
-      search_reads_kernel<true, false><<<grid, threads, 0, st>>>(sv, rv, tile_read, mtk, d_err, ctr);
-    else
-      search_reads_kernel<false, false><<<grid, threads, 0, st>>>(sv, rv, tile_read, mtk, d_err, ctr);
+    if (stream) {
+      if (small) SBWT_LAUNCH(true, false, true); else SBWT_LAUNCH(true, false, false);
+    } else {
+      if (small) SBWT_LAUNCH(false, false, true); else SBWT_LAUNCH(false, false, false);
+    }
   }
+#undef SBWT_LAUNCH
   SBWT_CUDA(cudaGetLastError());
   if (p.enabled) {
     SBWT_CUDA(cudaEventRecord(e1, st));
@@ -698,6 +925,8 @@ IndexImpl::IndexImpl(const u64 *const acgt[4], u64 num_bits_, u32 k_,
                      const u64 *sg, const u64 *key_marks, int device_,
                      unsigned presearch_letters) {
   if (num_bits_ == 0) throw Error(SBWT_E_INVALID, "empty SBWT");
+  if (num_bits_ >= (1ULL << 37))
+    throw Error(SBWT_E_INVALID, "SBWTs of 2^37 or more nodes are not supported");
   if (k_ == 0) throw Error(SBWT_E_INVALID, "k must be positive");
   device = device_;
   DeviceGuard g(device);
@@ -721,22 +950,42 @@ IndexImpl::IndexImpl(const u64 *const acgt[4], u64 num_bits_, u32 k_,
   c_map[0] = 1;
   for (int c = 0; c < 4; ++c) c_map[c + 1] = c_map[c] + totals[c];
   for (int c = 0; c < 5; ++c) view.c_map[c] = c_map[c];
+  // The rank blocks of A/C/G/T and the suffix-group-start words share one
+  // allocation ("hot" data of every search step), so one L2 access-policy
+  // window can keep them resident.
+  const u64 nw = (num_bits + 63) / 64;
+  u64 off[5];
+  u64 hot_bytes = 0;
   for (int c = 0; c < 4; ++c) {
-    blocks[c].resize(hb[c].size() * sizeof(Block));
-    SBWT_CUDA(cudaMemcpy(blocks[c].get(), hb[c].data(), hb[c].size() * sizeof(Block),
+    off[c] = hot_bytes;
+    hot_bytes += ((hb[c].size() * sizeof(Block) + 255) / 256) * 256;
+  }
+  off[4] = hot_bytes;
+  if (sg) hot_bytes += (((nw + 8) * 8 + 255) / 256) * 256;
+  hot.resize(hot_bytes);
+  SBWT_CUDA(cudaMemset(hot.get(), 0, hot_bytes));
+  unsigned char *hp = hot.get<unsigned char>();
+  for (int c = 0; c < 4; ++c) {
+    SBWT_CUDA(cudaMemcpy(hp + off[c], hb[c].data(), hb[c].size() * sizeof(Block),
                          cudaMemcpyHostToDevice));
     l0[c].resize(hl0[c].size() * 8);
     SBWT_CUDA(cudaMemcpy(l0[c].get(), hl0[c].data(), hl0[c].size() * 8,
                          cudaMemcpyHostToDevice));
-    view.blocks[c] = blocks[c].get<Block>();
+    view.blocks[c] = reinterpret_cast<const Block *>(hp + off[c]);
     view.l0[c] = l0[c].get<u64>();
   }
-  const u64 nw = (num_bits + 63) / 64;
   if (sg) {
-    sg_buf.resize((nw + 8) * 8);
-    SBWT_CUDA(cudaMemset(sg_buf.get(), 0, (nw + 8) * 8));
-    SBWT_CUDA(cudaMemcpy(sg_buf.get(), sg, nw * 8, cudaMemcpyHostToDevice));
-    view.suffix_group_starts = sg_buf.get<u64>();
+    SBWT_CUDA(cudaMemcpy(hp + off[4], sg, nw * 8, cudaMemcpyHostToDevice));
+    view.suffix_group_starts = reinterpret_cast<const u64 *>(hp + off[4]);
+  }
+  // An optional persisting-L2 window over the hot data (off by default: the
+  // carve-out takes L2 away from the presearch table and the streams, and
+  // measured slower on the 100 Mbp workload).
+  {
+    int max_window = 0;
+    cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, device);
+    window_bytes = std::min<u64>(hot_bytes, (u64)std::max(max_window, 0));
+    cudaGetLastError();
   }
   if (key_marks) {
     key_buf.resize((nw + 1) * 8);
@@ -760,8 +1009,8 @@ IndexImpl::IndexImpl(const u64 *const acgt[4], u64 num_bits_, u32 k_,
     SBWT_CUDA(cudaGetLastError());
   }
   SBWT_CUDA(cudaDeviceSynchronize());
-  device_bytes = presearch.size() + sg_buf.size() + key_buf.size();
-  for (int c = 0; c < 4; ++c) device_bytes += blocks[c].size() + l0[c].size();
+  device_bytes = presearch.size() + hot.size() + key_buf.size();
+  for (int c = 0; c < 4; ++c) device_bytes += l0[c].size();
 }
 
 SbwtView IndexImpl::view_for(u32 p) const {
@@ -843,6 +1092,20 @@ struct ReadsScratch {
   uint32_t *err;    // 1
 };
 
+// Length L of the absent-prefix probe: a random L-mer is a suffix of some
+// node with probability about N / 4^L, so L = ceil(log4 N) + 3 makes a probe
+// of an erroneous stretch come back absent most of the time.
+static uint32_t probe_length(u64 num_bits, u32 k, const LaunchConfig &cfg) {
+  if (cfg.probe_len == ~0u) return 0;
+  uint32_t L = cfg.probe_len;
+  if (L == 0) {
+    uint32_t lg = 0;
+    while (lg < 32 && (1ULL << (2 * lg)) < num_bits) ++lg;
+    L = lg + 3;
+  }
+  return L < k ? L : 0;
+}
+
 static u64 tile_size(int device, u64 n_kmers, const LaunchConfig &cfg) {
   if (cfg.tile) return cfg.tile;
   const u64 resident = (u64)sm_count(device) * cfg.blocks_per_sm * 256;
@@ -889,6 +1152,7 @@ static void launch_search(const IndexImpl &ix, const u64 *d_ends, u64 n_reads, u
   rv.n_tiles = (n_kmers + rv.tile - 1) / rv.tile;
   rv.out = d_out;
   rv.out_capacity = out_capacity;
+  rv.probe_len = probe_length(ix.num_bits, ix.k, cfg);
   tile_reads_kernel<<<grid_for(ix.device, n_reads, 256, 16), 256, 0, st>>>(
       sc.kmer_off, n_reads, rv.tile, sc.tile_read);
   SBWT_CUDA(cudaGetLastError());
@@ -898,7 +1162,21 @@ static void launch_search(const IndexImpl &ix, const u64 *d_ends, u64 n_reads, u
   const SbwtView sv = ix.view_for(cfg.presearch_letters);
   const bool stream = !(flags & SBWT_PER_KMER_WALK) && ix.view.suffix_group_starts;
   const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
-  launch_search_kernel(stream, sv, rv, sc.tile_read, mtk, sc.err, grid, threads, st);
+  u64 persist = 0;
+  if (cfg.l2_window && ix.window_bytes) {  // sets the context's persisting L2 size
+    int max_persist = 0;
+    cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, ix.device);
+    size_t cur = 0;
+    cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
+    const size_t want = std::min<size_t>((size_t)std::max(max_persist, 0), ix.window_bytes);
+    if (want > cur) cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want);
+    cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
+    cudaGetLastError();
+    persist = cur;
+  }
+  launch_search_kernel(stream, sv, rv, sc.tile_read, mtk, sc.err, grid, threads, st,
+                       persist ? search_attrs(ix.hot.get(), ix.window_bytes, persist)
+                               : LaunchAttrs{});
 }
 
 // Grows the workspace buffers of slot b for a batch and returns raw pointers.
@@ -1152,17 +1430,29 @@ void IndexImpl::search_reads_noalloc(const char *d_chars, u64 n_chars, const u64
   rv.n_tiles = (n_k + rv.tile - 1) / rv.tile;
   rv.out = d_results;
   rv.out_capacity = capacity;
+  rv.probe_len = probe_length(num_bits, k, cfg);
   tile_reads_kernel<<<grid_for(device, n_reads, 256, 16), 256, 0, st>>>(sc.kmer_off, n_reads,
                                                                         rv.tile, sc.tile_read);
   const int grid = grid_for(device, rv.n_tiles, 256, cfg.blocks_per_sm);
   const SbwtView sv = view_for(cfg.presearch_letters);
   const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
-  if (!(flags & SBWT_PER_KMER_WALK) && view.suffix_group_starts)
-    search_reads_kernel<true, false><<<grid, 256, 0, st>>>(sv, rv, sc.tile_read, mtk, sc.err,
-                                                            nullptr);
-  else
-    search_reads_kernel<false, false><<<grid, 256, 0, st>>>(sv, rv, sc.tile_read, mtk, sc.err,
-                                                             nullptr);
+  const bool stream = !(flags & SBWT_PER_KMER_WALK) && view.suffix_group_starts;
+  const bool narrow = sv.num_bits < kNarrowLimit;
+#define SBWT_NA_LAUNCH(S_, K_)                                                          \
+  do {                                                                                  \
+    if (narrow)                                                                         \
+      search_reads_kernel<S_, false, K_, uint32_t>                                      \
+          <<<grid, 256, 0, st>>>(sv, rv, sc.tile_read, mtk, sc.err, nullptr);           \
+    else                                                                                \
+      search_reads_kernel<S_, false, K_, uint64_t>                                      \
+          <<<grid, 256, 0, st>>>(sv, rv, sc.tile_read, mtk, sc.err, nullptr);           \
+  } while (0)
+  if (sv.k <= 33) {
+    if (stream) SBWT_NA_LAUNCH(true, true); else SBWT_NA_LAUNCH(false, true);
+  } else {
+    if (stream) SBWT_NA_LAUNCH(true, false); else SBWT_NA_LAUNCH(false, false);
+  }
+#undef SBWT_NA_LAUNCH
   SBWT_CUDA(cudaGetLastError());
   SBWT_CUDA(cudaMemcpyAsync(&err, sc.err, 4, cudaMemcpyDeviceToHost, st));
   SBWT_CUDA(cudaStreamSynchronize(st));

@@ -14,6 +14,8 @@ struct LaunchConfig {
   uint32_t blocks_per_sm = 8;      // 256-thread blocks per SM in the grid
   uint64_t tile = 0;               // k-mer slots per work tile
   uint64_t chunk_chars = 0;        // host-pointer path: chars per chunk
+  uint32_t probe_len = 0;          // absent-prefix probe length (0 = auto, ~0u = off)
+  uint32_t l2_window = 0;          // persisting L2 window over the index's hot data
 };
 
 struct IndexImpl {
@@ -41,7 +43,9 @@ struct IndexImpl {
   u64 c_map[5] = {0, 0, 0, 0, 0};
   u64 device_bytes = 0;
   SbwtView view{};
-  DeviceBuffer blocks[4], l0[4], presearch, sg_buf, key_buf;
+  DeviceBuffer hot;  // rank blocks of A/C/G/T + suffix-group words, contiguous
+  DeviceBuffer l0[4], presearch, key_buf;
+  u64 window_bytes = 0;   // L2 access-policy window over `hot`
 };
 
 u64 count_kmers_host(const u64 *ends, u64 n_reads, u32 k, u64 base);

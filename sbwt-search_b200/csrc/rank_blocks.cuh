@@ -43,8 +43,10 @@ __device__ __forceinline__ bool block_bit(const Block &b, uint32_t q) {
   return (w >> (Q & 63)) & 1ULL;
 }
 
+// Block of position i.  Indexes are < 2^37 (checked when an index is built),
+// so i / 224 = (i >> 5) / 7 is a 32-bit division by a constant.
 __device__ __forceinline__ uint64_t block_of(uint64_t i) {
-  return i / kBlockBits;
+  return (uint64_t)((uint32_t)(i >> 5) / 7u);
 }
 
 // rank_c(i): ones of vector c in [0, i), i in [0, N].

@@ -74,6 +74,8 @@ def lib():
         L.sbwt_search_reads.argtypes = [vp, vp, u64, vp, u64, vp, u64,
                                         C.POINTER(u64), u32, vp]
         L.sbwt_set_launch_config.argtypes = [u32, u32, u64, u64]
+        L.sbwt_set_probe_length.argtypes = [u32]
+        L.sbwt_set_l2_window.argtypes = [C.c_int]
         if hasattr(L, "sbwt_colors_open"):
             L.sbwt_colors_open.argtypes = [C.c_char_p, C.c_int, C.POINTER(vp)]
             L.sbwt_colors_free.argtypes = [vp]
@@ -110,6 +112,15 @@ def set_launch_config(presearch_letters: int = 0, blocks_per_sm: int = 0,
                       tile: int = 0, chunk_chars: int = 0) -> None:
     check(lib().sbwt_set_launch_config(presearch_letters, blocks_per_sm, tile,
                                        chunk_chars))
+
+
+def set_probe_length(probe_len: int = 0) -> None:
+    """0 = automatic, 0xFFFFFFFF = off (results never depend on it)."""
+    check(lib().sbwt_set_probe_length(probe_len))
+
+
+def set_l2_window(enabled: bool = True) -> None:
+    check(lib().sbwt_set_l2_window(int(enabled)))
 
 
 class SbwtIndex:

@@ -127,3 +127,21 @@ def test_errors_are_status_codes():
     with pytest.raises(S.SbwtError) as e:
         idx.search_reads(b"ACGT" * 20, np.array([80], np.uint64), move_to_key_kmer=True)
     assert e.value.code == S.E_INVALID
+
+
+@pytest.mark.parametrize("probe", [0, 0xFFFFFFFF, 5, 13, 20, 30])
+def test_absent_prefix_probe_is_exact(probe):
+    """The probe only skips k-mers it proves absent: results are identical
+    for every probe length (0 = automatic, 0xFFFFFFFF = off)."""
+    g, path, sb = synthetic(7, 4, 6000, 31, 2, 0.02)
+    idx = S.SbwtIndex.open(path)
+    chars, ends = mixed_reads(g, 77, 3000, median=150, sigma=0.5, len_min=20,
+                              len_max=600, sub=0.03, n_rate=0.005)
+    exp = oracle_results(oracle_index(path, 8), chars, ends)
+    S.set_probe_length(probe)
+    try:
+        got = idx.search_reads(chars, ends)
+        got2 = idx.search_reads(chars, ends, per_kmer_walk=True)
+    finally:
+        S.set_probe_length(0)
+    assert np.array_equal(got, exp) and np.array_equal(got2, exp)

@@ -198,6 +198,61 @@ int sbwt_pseudoalign(const sbwt_colors_t *colors, const uint64_t *sbwt_idxs,
                      uint64_t *ids_offsets, void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* Batched pipelines and the serving loop (no counterpart in the reference:  */
+/* the reference runs one synchronous copy-kernel-copy per batch per stream,  */
+/* src/IndexSearcher/IndexSearcher.cpp:26-51)                                */
+/* ------------------------------------------------------------------------ */
+typedef struct sbwt_pipeline sbwt_pipeline_t;
+typedef struct sbwt_server sbwt_server_t;
+
+/* A reusable device pipeline for batches of up to max_chars chars and
+ * max_reads reads: its own device buffers, pinned staging and stream.  Each
+ * batch (H2D -> index step -> colors step when `colors` is not NULL -> D2H)
+ * runs as one CUDA graph with no host synchronisation inside, captured per
+ * batch and applied to the instantiated graph with cudaGraphExecUpdate.  The
+ * search kernel is a persistent launch fed by a device work queue. */
+int sbwt_pipeline_create(const sbwt_index_t *index, const sbwt_colors_t *colors,
+                         uint64_t max_chars, uint64_t max_reads, uint32_t flags,
+                         double tau, sbwt_pipeline_t **out);
+void sbwt_pipeline_free(sbwt_pipeline_t *p);
+/* Runs one batch (host pointers; synchronous).  Without colors: results per
+ * k-mer as sbwt_search_reads.  With colors: ids / ids_offsets as
+ * sbwt_pseudoalign (tau and flags from sbwt_pipeline_create). */
+int sbwt_pipeline_run(sbwt_pipeline_t *p, const char *chars, uint64_t n_chars,
+                      const uint64_t *read_ends, uint64_t n_reads,
+                      uint64_t *results, uint64_t results_capacity,
+                      uint64_t *n_results, uint32_t *ids, uint64_t ids_capacity,
+                      uint64_t *ids_offsets);
+
+/* A serving loop over resident indexes: `slots` pipelines of batch_chars /
+ * batch_reads (shrunk at creation until they fit in half of the free device
+ * memory).  Requests of any size are accepted from any thread; a background
+ * thread keeps every free slot busy with the pending requests in arrival
+ * order (continuous batching: a request arriving while batches run joins the
+ * next free slot and runs concurrently with them; a large request is split
+ * over several batches).  Results are identical to the single calls. */
+int sbwt_server_create(const sbwt_index_t *index, const sbwt_colors_t *colors,
+                       uint64_t batch_chars, uint64_t batch_reads, int slots,
+                       uint32_t flags, double tau, sbwt_server_t **out);
+void sbwt_server_free(sbwt_server_t *s);
+int sbwt_server_submit(sbwt_server_t *s, const char *chars, uint64_t n_chars,
+                       const uint64_t *read_ends, uint64_t n_reads,
+                       uint64_t *request_id);
+/* Waits up to timeout_ms (< 0: forever; SBWT_E_TIMEOUT if not done) for a
+ * request and hands its results over (malloc'ed; sbwt_free):
+ *   index mode:  *values (n_values k-mer results), *offsets per read;
+ *   colors mode: *ids (n_ids color ids), *offsets per read. */
+int sbwt_server_wait(sbwt_server_t *s, uint64_t request_id, double timeout_ms,
+                     uint64_t **values, uint64_t *n_values, uint32_t **ids,
+                     uint64_t *n_ids, uint64_t **offsets, uint64_t *n_reads);
+/* Latency percentiles (seconds, submit -> results ready) of the requests
+ * finished since the last reset, their count, reads and batches done and the
+ * elapsed time; reset != 0 starts a new window. */
+int sbwt_server_stats(sbwt_server_t *s, double *p50_s, double *p99_s,
+                      uint64_t *requests_done, uint64_t *reads_done,
+                      uint64_t *batches, double *elapsed_s, int reset);
+
+/* ------------------------------------------------------------------------ */
 /* Host I/O in the reference's file formats (no GPU involved)               */
 /* ------------------------------------------------------------------------ */
 /* Reads every record of a FASTA/FASTQ file (.gz ok) with the reference's

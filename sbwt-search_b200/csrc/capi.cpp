@@ -17,6 +17,8 @@ LaunchConfig &default_launch_config() {
   return cfg;
 }
 }  // namespace sbwt
+namespace sbwt {
+}  // namespace sbwt
 
 using namespace sbwt;
 

@@ -416,6 +416,40 @@ void ColorsImpl::launch(const u64 *d_vals, const u64 *d_offs, const u64 *d_nf,
   SBWT_CUDA(cudaGetLastError());
 }
 
+// The colors step of one device-resident batch without host synchronisation
+// (capturable): per-read counting over `vals` (index-step results, -1/-2
+// markers counted, not looked up) + threshold, scan of the per-read pass
+// counts into d_ids_off (n_reads + 1), ids into d_ids (capacity bound checked
+// on the device; d_ids_off[n_reads] is the required size).
+void ColorsImpl::enqueue_pseudoalign(const u64 *d_vals, const u64 *d_offs, u64 n_reads,
+                                     u64 max_kmers, double tau, u32 flags, u64 *d_pass_bits,
+                                     uint32_t *d_pass_count, u64 *d_ids_off, uint32_t *d_ids,
+                                     u64 ids_capacity, uint32_t *d_err,
+                                     cudaStream_t st) const {
+  if (n_reads == 0) {
+    SBWT_CUDA(cudaMemsetAsync(d_ids_off, 0, 8, st));
+    return;
+  }
+  launch(d_vals, d_offs, nullptr, nullptr, n_reads, max_kmers, tau, flags, 0, d_pass_bits,
+         d_pass_count, nullptr, d_err, st);
+  scan_counts_kernel<<<1, 1024, 0, st>>>(d_pass_count, n_reads, d_ids_off);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const u64 blocks = std::min<u64>((n_reads + 7) / 8, (u64)sms * 16);
+  emit_ids_kernel<<<(unsigned)std::max<u64>(blocks, 1), 256, 0, st>>>(
+      d_pass_bits, view.row_words, d_ids_off, n_reads, d_ids, ids_capacity);
+  SBWT_CUDA(cudaGetLastError());
+}
+
+void ColorsImpl::prepare_launch(u64 max_kmers) const {
+  const uint32_t P = planes_for(max_kmers);
+  const size_t smem = (size_t)kColorWarps * P * 32 * view.words_per_lane * 8;
+  SBWT_CUDA(cudaFuncSetAttribute(colors_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  SBWT_CUDA(cudaFuncSetAttribute(colors_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+}
+
 static u64 max_span(const u64 *offs, u64 n_reads) {
   u64 m = 0;
   for (u64 r = 0; r < n_reads; ++r) {

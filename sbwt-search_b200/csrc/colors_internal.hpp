@@ -39,6 +39,14 @@ struct ColorsImpl {
               u64 *d_pass_bits, uint32_t *d_pass_count, uint32_t *d_counts,
               uint32_t *d_err, cudaStream_t st) const;
 
+  void enqueue_pseudoalign(const u64 *d_vals, const u64 *d_offs, u64 n_reads, u64 max_kmers,
+                           double tau, u32 flags, u64 *d_pass_bits, uint32_t *d_pass_count,
+                           u64 *d_ids_off, uint32_t *d_ids, u64 ids_capacity,
+                           uint32_t *d_err, cudaStream_t st) const;
+  // sets the shared-memory attribute for batches of up to max_kmers k-mers per
+  // read (must precede a stream capture)
+  void prepare_launch(u64 max_kmers) const;
+
   int device = 0;
   u64 num_colors = 0;
   u64 device_bytes = 0;

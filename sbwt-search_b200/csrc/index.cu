@@ -326,6 +326,8 @@ struct ReadsView {
   uint64_t *out;
   uint64_t out_capacity;
   uint32_t probe_len;       // L of the absent-prefix probe (0 = off)
+  const uint64_t *n_kmers_dev;  // if set, the k-mer total is read from here
+  unsigned long long *queue;    // work-queue counter (tiles handed out), zeroed
 };
 
 __device__ __forceinline__ bool invalid_at(const uint32_t *inv, uint64_t i) {
@@ -488,9 +490,11 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
   constexpr I NONE = NM::kNone;
   const uint32_t k = s.k;
   const uint32_t L = rv.probe_len;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t n_kmers = rv.n_kmers_dev ? *rv.n_kmers_dev : rv.n_kmers;
+  const uint64_t n_tiles = (n_kmers + rv.tile - 1) / rv.tile;
   uint64_t n_pre = 0, n_block = 0, n_sg = 0, n_probe = 0;
-  uint64_t tile = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  bool exhausted = false;  // the work queue is empty for this lane
   uint64_t slot = 0, slot_end = 0, r = 0, r_next = 0, pos = 0, skip_until = 0;
   int64_t last_inv = -1;
   I v = NONE;  // node of the previous k-mer of this read
@@ -501,6 +505,25 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
   CharWindow cw;
   cw.init(rv.packed, rv.invalid);
   while (true) {
+    // ---- work queue (warp-collective): lanes out of k-mers take a new tile;
+    // one atomic per warp hands out consecutive tiles.
+    __syncwarp();
+    const bool need = !exhausted && mode == M_NEW && slot >= slot_end;
+    const unsigned need_mask = __ballot_sync(0xFFFFFFFFu, need);
+    uint64_t new_tile = ~0ULL;
+    if (need_mask) {
+      const int leader = __ffs(need_mask) - 1;
+      unsigned long long base = 0;
+      if ((int)lane == leader) base = atomicAdd(rv.queue, (unsigned long long)__popc(need_mask));
+      base = __shfl_sync(0xFFFFFFFFu, base, leader);
+      if (need) {
+        new_tile = base + __popc(need_mask & ((1u << lane) - 1u));
+        if (new_tile >= n_tiles) {
+          exhausted = true;
+          new_tile = ~0ULL;
+        }
+      }
+    }
     // ---- phase 1 (per lane): what to load --------------------------------
     uint32_t kind = K_NONE;
     I pa = 0, pb = 0;
@@ -509,14 +532,15 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
       if (mode == M_NEW) {
         while (true) {
           if (slot >= slot_end) {  // next tile
-            if (tile >= rv.n_tiles) {
-              done = true;
+            if (new_tile == ~0ULL) {  // none this iteration
+              done = exhausted;
               break;
             }
+            const uint64_t tile = new_tile;
+            new_tile = ~0ULL;
             slot = tile * rv.tile;
-            slot_end = min(slot + rv.tile, rv.n_kmers);
+            slot_end = min(slot + rv.tile, n_kmers);
             r = __ldg(tile_read + tile);
-            tile += stride;
             r_next = __ldg(rv.kmer_off + r + 1);
             pos = (r ? __ldg(rv.ends + r - 1) : rv.base) - rv.base +
                   (slot - __ldg(rv.kmer_off + r));
@@ -559,7 +583,7 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
           ++slot;
           ++pos;
         }
-        if (!done) {
+        if (!done && slot < slot_end) {
           if (STREAM && v != NONE) {
             kind = K_BLOCK;
             c = SMALLK ? cw.char_at(pos + k - 1) : char_at(rv.packed, pos + k - 1);
@@ -608,7 +632,7 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
       n_sg += kind == K_SGW;
       n_probe += (mode == M_PPRE || mode == M_PROBE);
     }
-    if (done) continue;
+    if (done || kind == K_NONE) continue;
     // ---- phase 3: one shared rank computation, then per-mode updates ------
     const uint32_t qa = (uint32_t)(pa - ba * kBlockBits), qb = (uint32_t)(pb - bb * kBlockBits);
     const I ra = NM::rank(s, c, ba, A, qa);
@@ -816,13 +840,16 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
                                  const LaunchAttrs &la) {
   Profile &p = profile();
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (p.enabled) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(st, &cap);
+  const bool timed = p.enabled && cap == cudaStreamCaptureStatusNone;
+  if (timed) {
     SBWT_CUDA(cudaEventCreate(&e0));
     SBWT_CUDA(cudaEventCreate(&e1));
     SBWT_CUDA(cudaEventRecord(e0, st));
   }
   unsigned long long *ctr = nullptr;
-  if (p.enabled && p.count) {
+  if (timed && p.count) {
     std::lock_guard<std::mutex> g(p.mu);
     if (p.d_counters.size() == 0) {
       p.d_counters.resize(64);
@@ -856,7 +883,7 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
   }
 #undef SBWT_LAUNCH
   SBWT_CUDA(cudaGetLastError());
-  if (p.enabled) {
+  if (timed) {
     SBWT_CUDA(cudaEventRecord(e1, st));
     SBWT_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
@@ -1024,7 +1051,7 @@ struct Workspace {
   int device = -1;
   cudaStream_t streams[2] = {nullptr, nullptr};
   DeviceBuffer chars[2], ends[2], kmer_off[2], packed[2], invalid[2], results[2],
-      block_sums[2], total[2], tile_read[2], positions, bits;
+      block_sums[2], total[2], tile_read[2], queue[2], positions, bits;
   uint32_t *err_host = nullptr;  // pinned
   DeviceBuffer err_dev;
   cudaEvent_t done[2] = {nullptr, nullptr};
@@ -1080,17 +1107,6 @@ static int grid_for(int dev, u64 work, int threads, int per_sm) {
   return (int)std::max<u64>(g, 1);
 }
 
-// Device scratch of one read batch: scan outputs, packed chars, invalid
-// bits, the tile table and the error word.
-struct ReadsScratch {
-  u64 *kmer_off;    // n_reads + 1
-  u64 *packed;      // n_words + 2
-  uint32_t *invalid;  // n_words + 2
-  u64 *block_sums;  // ceil(n_reads / kScanTile)
-  u64 *total;       // 1
-  u64 *tile_read;   // n_tiles
-  uint32_t *err;    // 1
-};
 
 // Length L of the absent-prefix probe: a random L-mer is a suffix of some
 // node with probability about N / 4^L, so L = ceil(log4 N) + 3 makes a probe
@@ -1153,6 +1169,9 @@ static void launch_search(const IndexImpl &ix, const u64 *d_ends, u64 n_reads, u
   rv.out = d_out;
   rv.out_capacity = out_capacity;
   rv.probe_len = probe_length(ix.num_bits, ix.k, cfg);
+  rv.n_kmers_dev = nullptr;
+  rv.queue = sc.queue;
+  SBWT_CUDA(cudaMemsetAsync(sc.queue, 0, 8, st));
   tile_reads_kernel<<<grid_for(ix.device, n_reads, 256, 16), 256, 0, st>>>(
       sc.kmer_off, n_reads, rv.tile, sc.tile_read);
   SBWT_CUDA(cudaGetLastError());
@@ -1179,6 +1198,52 @@ static void launch_search(const IndexImpl &ix, const u64 *d_ends, u64 n_reads, u
                                : LaunchAttrs{});
 }
 
+// The index step of one device-resident batch without any host
+// synchronisation (capturable in a CUDA graph): scan, pack, tile table and
+// the search kernel.  The k-mer total is taken from device memory inside the
+// kernel; tiles are sized from max_kmers (an upper bound, e.g. n_chars) and
+// the tile table must hold max_kmers / tile + 2 entries.
+void enqueue_index_step(const IndexImpl &ix, const char *d_chars, u64 n_chars,
+                        const u64 *d_ends, u64 n_reads, const ReadsScratch &sc, u64 *d_out,
+                        u64 out_capacity, u64 max_kmers, u32 flags, const LaunchConfig &cfg,
+                        cudaStream_t st) {
+  SBWT_CUDA(cudaMemsetAsync(sc.err, 0, 4, st));
+  SBWT_CUDA(cudaMemsetAsync(sc.queue, 0, 8, st));
+  if (n_reads == 0) {
+    SBWT_CUDA(cudaMemsetAsync(sc.total, 0, 8, st));
+    return;
+  }
+  launch_prepare(ix.device, ix.k, d_chars, n_chars, d_ends, n_reads, 0, sc, st);
+  ReadsView rv{};
+  rv.packed = sc.packed;
+  rv.invalid = sc.invalid;
+  rv.ends = d_ends;
+  rv.kmer_off = sc.kmer_off;
+  rv.base = 0;
+  rv.n_reads = n_reads;
+  rv.n_kmers = 0;
+  rv.n_kmers_dev = sc.total;
+  rv.tile = tile_size(ix.device, std::max<u64>(max_kmers, 1), cfg);
+  rv.n_tiles = 0;  // computed on the device from the total
+  rv.out = d_out;
+  rv.out_capacity = out_capacity;
+  rv.probe_len = probe_length(ix.num_bits, ix.k, cfg);
+  rv.queue = sc.queue;
+  tile_reads_kernel<<<grid_for(ix.device, n_reads, 256, 16), 256, 0, st>>>(
+      sc.kmer_off, n_reads, rv.tile, sc.tile_read);
+  const int grid = (int)((u64)sm_count(ix.device) * cfg.blocks_per_sm);
+  const SbwtView sv = ix.view_for(cfg.presearch_letters);
+  const bool stream = !(flags & SBWT_PER_KMER_WALK) && ix.view.suffix_group_starts;
+  const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
+  launch_search_kernel(stream, sv, rv, sc.tile_read, mtk, sc.err, grid, 256, st,
+                       LaunchAttrs{});
+  note_launches(1);
+}
+
+u64 index_tile_size(const IndexImpl &ix, u64 max_kmers, const LaunchConfig &cfg) {
+  return tile_size(ix.device, std::max<u64>(max_kmers, 1), cfg);
+}
+
 // Grows the workspace buffers of slot b for a batch and returns raw pointers.
 static ReadsScratch scratch_for(Workspace &ws, int b, u64 n_chars, u64 n_reads,
                                 u64 n_kmers_max, u64 tile_min) {
@@ -1189,10 +1254,12 @@ static ReadsScratch scratch_for(Workspace &ws, int b, u64 n_chars, u64 n_reads,
   ws.block_sums[b].ensure(((n_reads + kScanTile - 1) / kScanTile + 1) * 8);
   ws.total[b].ensure(8);
   ws.tile_read[b].ensure((n_kmers_max / tile_min + 2) * 8);
+  ws.queue[b].ensure(8);
   return ReadsScratch{ws.kmer_off[b].get<u64>(), ws.packed[b].get<u64>(),
                       ws.invalid[b].get<uint32_t>(), ws.block_sums[b].get<u64>(),
                       ws.total[b].get<u64>(), ws.tile_read[b].get<u64>(),
-                      ws.err_dev.get<uint32_t>()};
+                      ws.err_dev.get<uint32_t>(),
+                      ws.queue[b].get<unsigned long long>()};
 }
 
 u64 count_kmers_host(const u64 *ends, u64 n_reads, u32 k, u64 base) {
@@ -1356,6 +1423,7 @@ constexpr u64 kNoAllocOffBlockSums =
 constexpr u64 kNoAllocOffTotal =
     kNoAllocOffBlockSums + ((kNoAllocMaxReads + kScanTile - 1) / kScanTile + 1) * 8;
 constexpr u64 kNoAllocOffErr = kNoAllocOffTotal + 8;
+constexpr u64 kNoAllocOffQueue = kNoAllocOffErr + 8;
 constexpr u64 kNoAllocOffTileRead = kNoAllocOffErr + 248;  // keeps 8-byte alignment
 constexpr u64 kNoAllocTileMin = 16;
 constexpr u64 kNoAllocBytes =
@@ -1400,9 +1468,12 @@ void IndexImpl::search_reads_noalloc(const char *d_chars, u64 n_chars, const u64
                   reinterpret_cast<u64 *>(base + kNoAllocOffBlockSums),
                   reinterpret_cast<u64 *>(base + kNoAllocOffTotal),
                   reinterpret_cast<u64 *>(base + kNoAllocOffTileRead),
-                  reinterpret_cast<uint32_t *>(base + kNoAllocOffErr)};
-  // the error word keeps the last call's value: clear it first
+                  reinterpret_cast<uint32_t *>(base + kNoAllocOffErr),
+                  reinterpret_cast<unsigned long long *>(base + kNoAllocOffQueue)};
+  // the error word and the work-queue counter keep the last call's values:
+  // clear them first
   SBWT_CUDA(cudaMemsetAsync(sc.err, 0, 4, st));
+  SBWT_CUDA(cudaMemsetAsync(sc.queue, 0, 8, st));
   u64 n_k = 0;
   uint32_t err = 0;
   if (n_reads) {
@@ -1431,6 +1502,7 @@ void IndexImpl::search_reads_noalloc(const char *d_chars, u64 n_chars, const u64
   rv.out = d_results;
   rv.out_capacity = capacity;
   rv.probe_len = probe_length(num_bits, k, cfg);
+  rv.queue = sc.queue;
   tile_reads_kernel<<<grid_for(device, n_reads, 256, 16), 256, 0, st>>>(sc.kmer_off, n_reads,
                                                                         rv.tile, sc.tile_read);
   const int grid = grid_for(device, rv.n_tiles, 256, cfg.blocks_per_sm);

@@ -50,6 +50,26 @@ struct IndexImpl {
 
 u64 count_kmers_host(const u64 *ends, u64 n_reads, u32 k, u64 base);
 
+// Device scratch of one read batch: scan outputs, packed chars, invalid
+// bits, the tile table, the error word and the work-queue counter.
+struct ReadsScratch {
+  u64 *kmer_off;      // n_reads + 1
+  u64 *packed;        // n_words + 2
+  uint32_t *invalid;  // n_words + 2
+  u64 *block_sums;    // ceil(n_reads / 4096) + 1
+  u64 *total;         // 1
+  u64 *tile_read;     // n_tiles + 2
+  uint32_t *err;      // 1
+  unsigned long long *queue;  // 1
+};
+
+void enqueue_index_step(const IndexImpl &ix, const char *d_chars, u64 n_chars,
+                        const u64 *d_ends, u64 n_reads, const ReadsScratch &sc, u64 *d_out,
+                        u64 out_capacity, u64 max_kmers, u32 flags, const LaunchConfig &cfg,
+                        cudaStream_t st);
+u64 index_tile_size(const IndexImpl &ix, u64 max_kmers, const LaunchConfig &cfg);
+LaunchConfig &default_launch_config();
+
 }  // namespace sbwt
 
 struct sbwt_index {

@@ -85,6 +85,25 @@ def lib():
             L.sbwt_color_counts.argtypes = [vp, vp, vp, u64, vp, u32, vp]
             L.sbwt_pseudoalign.argtypes = [vp, vp, vp, vp, vp, u64, C.c_double, u32,
                                            vp, u64, vp, vp]
+        L.sbwt_pipeline_create.argtypes = [vp, vp, u64, u64, u32, C.c_double,
+                                           C.POINTER(vp)]
+        L.sbwt_pipeline_free.argtypes = [vp]
+        L.sbwt_pipeline_free.restype = None
+        L.sbwt_pipeline_run.argtypes = [vp, vp, u64, vp, u64, vp, u64, C.POINTER(u64),
+                                        vp, u64, vp]
+        L.sbwt_server_create.argtypes = [vp, vp, u64, u64, C.c_int, u32, C.c_double,
+                                         C.POINTER(vp)]
+        L.sbwt_server_free.argtypes = [vp]
+        L.sbwt_server_free.restype = None
+        L.sbwt_server_submit.argtypes = [vp, vp, u64, vp, u64, C.POINTER(u64)]
+        L.sbwt_server_wait.argtypes = [vp, u64, C.c_double, C.POINTER(vp), C.POINTER(u64),
+                                       C.POINTER(vp), C.POINTER(u64), C.POINTER(vp),
+                                       C.POINTER(u64)]
+        L.sbwt_server_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                        C.POINTER(u64), C.POINTER(u64), C.POINTER(u64),
+                                        C.POINTER(C.c_double), C.c_int]
+        L.sbwt_free.argtypes = [vp]
+        L.sbwt_free.restype = None
         _L = L
     return _L
 
@@ -284,3 +303,125 @@ class ColorIndex:
             check(rc)
             break
         return [ids[int(offs[r]):int(offs[r + 1])].tolist() for r in range(n)], offs, ids
+
+
+def _np_chars(chars):
+    if isinstance(chars, (bytes, bytearray)):
+        chars = np.frombuffer(chars, dtype=np.uint8)
+    return np.ascontiguousarray(chars, dtype=np.uint8)
+
+
+class Pipeline:
+    """A reusable device pipeline (one CUDA graph per batch): index step, and
+    the colors step too when a ColorIndex is given."""
+
+    def __init__(self, index: SbwtIndex, colors: "ColorIndex | None", max_chars: int,
+                 max_reads: int, tau: float = 0.7, include_not_found: bool = False,
+                 include_invalid: bool = False, move_to_key_kmer: bool = False):
+        flags = (INCLUDE_NOT_FOUND if include_not_found else 0) | \
+            (INCLUDE_INVALID if include_invalid else 0) | \
+            (MOVE_TO_KEY_KMER if move_to_key_kmer else 0)
+        h = C.c_void_p()
+        check(lib().sbwt_pipeline_create(index._h, colors._h if colors else None, max_chars,
+                                         max_reads, flags, tau, C.byref(h)))
+        self._h = h
+        self.index, self.colors = index, colors
+
+    def close(self):
+        if self._h:
+            lib().sbwt_pipeline_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, chars, read_ends):
+        chars = _np_chars(chars)
+        read_ends = np.ascontiguousarray(read_ends, dtype=np.uint64)
+        n = len(read_ends)
+        nres = C.c_uint64(0)
+        if self.colors is None:
+            out = np.empty(max(self.index.count_kmers(read_ends), 1), np.uint64)
+            check(lib().sbwt_pipeline_run(self._h, _ptr(chars) if len(chars) else None,
+                                          len(chars), _ptr(read_ends) if n else None, n,
+                                          _ptr(out), len(out), C.byref(nres), None, 0, None))
+            return out[:nres.value]
+        offs = np.zeros(n + 1, np.uint64)
+        cap = max(1, n * 8)
+        while True:
+            ids = np.zeros(cap, np.uint32)
+            rc = lib().sbwt_pipeline_run(self._h, _ptr(chars) if len(chars) else None,
+                                         len(chars), _ptr(read_ends) if n else None, n, None, 0,
+                                         C.byref(nres), _ptr(ids), cap, _ptr(offs))
+            if rc == E_CAPACITY:
+                cap = int(offs[n]) + 1
+                continue
+            check(rc)
+            return [ids[int(offs[r]):int(offs[r + 1])].tolist() for r in range(n)]
+
+
+class Server:
+    """Continuous-batching serving loop over resident indexes."""
+
+    def __init__(self, index: SbwtIndex, colors: "ColorIndex | None" = None,
+                 batch_chars: int = 32 << 20, batch_reads: int = 1 << 18, slots: int = 3,
+                 tau: float = 0.7, include_not_found: bool = False,
+                 include_invalid: bool = False):
+        flags = (INCLUDE_NOT_FOUND if include_not_found else 0) | \
+            (INCLUDE_INVALID if include_invalid else 0)
+        h = C.c_void_p()
+        check(lib().sbwt_server_create(index._h, colors._h if colors else None, batch_chars,
+                                       batch_reads, slots, flags, tau, C.byref(h)))
+        self._h = h
+        self.colors = colors
+
+    def close(self):
+        if self._h:
+            lib().sbwt_server_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, chars, read_ends) -> int:
+        chars = _np_chars(chars)
+        read_ends = np.ascontiguousarray(read_ends, dtype=np.uint64)
+        rid = C.c_uint64(0)
+        check(lib().sbwt_server_submit(self._h, _ptr(chars) if len(chars) else None,
+                                       len(chars), _ptr(read_ends) if len(read_ends) else None,
+                                       len(read_ends), C.byref(rid)))
+        return rid.value
+
+    def wait(self, rid: int, timeout_ms: float = -1.0):
+        vals, ids, offs = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        nv, ni, nr = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        check(lib().sbwt_server_wait(self._h, rid, timeout_ms, C.byref(vals), C.byref(nv),
+                                     C.byref(ids), C.byref(ni), C.byref(offs), C.byref(nr)))
+        L = lib()
+        try:
+            o = np.ctypeslib.as_array(C.cast(offs, C.POINTER(C.c_uint64)),
+                                      (nr.value + 1,)).copy()
+            if self.colors is None:
+                v = np.ctypeslib.as_array(C.cast(vals, C.POINTER(C.c_uint64)),
+                                          (max(nv.value, 1),))[:nv.value].copy()
+                return v, o
+            i = np.ctypeslib.as_array(C.cast(ids, C.POINTER(C.c_uint32)),
+                                      (max(ni.value, 1),))[:ni.value].copy()
+            return [i[int(o[r]):int(o[r + 1])].tolist() for r in range(nr.value)]
+        finally:
+            for p in (vals, ids, offs):
+                L.sbwt_free(p)
+
+    def stats(self, reset: bool = False) -> dict:
+        p50, p99, el = C.c_double(), C.c_double(), C.c_double()
+        nd, rd, nb = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        check(lib().sbwt_server_stats(self._h, C.byref(p50), C.byref(p99), C.byref(nd),
+                                      C.byref(rd), C.byref(nb), C.byref(el), int(reset)))
+        return {"p50_s": p50.value, "p99_s": p99.value, "requests": nd.value,
+                "reads": rd.value, "batches": nb.value, "elapsed_s": el.value}

@@ -56,3 +56,39 @@ def oracle_results(index, chars: np.ndarray, ends: np.ndarray) -> np.ndarray:
     reads = T.split_reads(chars, ends)
     rows = O.index_search_reads(index, reads)
     return np.concatenate(rows) if rows else np.zeros(0, np.uint64)
+
+
+def key_marks_for(index, d: int, seed: int = 0) -> np.ndarray:
+    """Key k-mer marks for the d > 1 forward walk (IndexSearcher.cuh:60-70 of
+    the reference): about one node in d is a key, every node without an
+    outgoing edge bit is a key, and every cycle of first-edge successors holds
+    a key, so the walk from any node ends."""
+    import oracle as O
+    N = index.num_bits
+    rng = np.random.default_rng(seed)
+    key = rng.random(N) < 1.0 / d
+    succ = np.full(N, -1, np.int64)
+    bits = [np.unpackbits(a.view(np.uint8), bitorder="little")[:N] for a in index.acgt]
+    L = O.lib()
+    for i in range(N):
+        for c in range(4):
+            if bits[c][i]:
+                succ[i] = int(index.c_map[c]) + L.oracle_rank(
+                    O._p(index.acgt_pad[c]), O._p(index.l0[c]), O._p(index.l12[c]), i)
+                break
+    key |= succ < 0
+    state = np.zeros(N, np.int8)  # 0 new, 1 on stack, 2 resolved
+    for s in range(N):
+        path = []
+        x = s
+        while not key[x] and state[x] == 0:
+            state[x] = 1
+            path.append(x)
+            x = int(succ[x])
+        if not key[x] and state[x] == 1:  # a cycle without a key
+            key[x] = True
+        for y in path:
+            state[y] = 2
+    words = np.packbits(key.astype(np.uint8), bitorder="little")
+    words = np.concatenate([words, np.zeros((-len(words)) % 8, np.uint8)])
+    return words.view(np.uint64)

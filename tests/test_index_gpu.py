@@ -145,3 +145,39 @@ def test_absent_prefix_probe_is_exact(probe):
     finally:
         S.set_probe_length(0)
     assert np.array_equal(got, exp) and np.array_equal(got2, exp)
+
+
+@pytest.mark.parametrize("d", [2, 7])
+def test_move_to_key_kmer_matches_oracle_and_reference(d):
+    """The d > 1 forward walk to the next key k-mer (reference flag -k)."""
+    from helpers import key_marks_for
+    g, path, sb = synthetic(9, 2, 3000, 31, 1, 0.02)
+    oi = oracle_index(path, 8)
+    keys = key_marks_for(oi, d, seed=d)
+    idx = S.SbwtIndex.from_arrays(sb.acgt, sb.num_bits, sb.k, sb.suffix_group_starts,
+                                  key_kmer_marks=keys)
+    chars, ends = mixed_reads(g, 13, 800, sub=0.01, n_rate=0.003)
+    exp = np.concatenate(O.index_search_reads(oi, T.split_reads(chars, ends), keys))
+    assert np.array_equal(idx.search_reads(chars, ends, move_to_key_kmer=True), exp)
+    bits, _ = O.seq_to_bits(chars.tobytes())
+    pos = O.positions_of(ends, 31)
+    got = idx.search(bits, pos, move_to_key_kmer=True)
+    assert np.array_equal(got, oi.search_positions(bits, pos, keys))
+    if O.ref_lib() is not None:
+        ref = O.OracleIndex(sb.acgt, sb.num_bits, sb.k, use_ref=True)
+        assert np.array_equal(got, ref.search_positions(bits, pos, keys))
+
+
+def test_tdbg_without_variant_string(tmp_path):
+    """A .tdbg file is a .sbwt without the leading "plain-matrix" string
+    (scripts/modifiers/themisto_tdbg_to_sbwt.py:23-32 of the reference)."""
+    import struct
+    g, path, sb = synthetic(4, 2, 4000, 31, 1, 0.02)
+    data = open(path, "rb").read()
+    n = struct.unpack_from("<Q", data, 0)[0]
+    assert data[8:8 + n] == b"plain-matrix"
+    tdbg = tmp_path / "x.tdbg"
+    tdbg.write_bytes(data[8 + n:])
+    a, b = S.SbwtIndex.open(path), S.SbwtIndex.open(tdbg)
+    chars, ends = mixed_reads(g, 5, 300)
+    assert np.array_equal(a.search_reads(chars, ends), b.search_reads(chars, ends))

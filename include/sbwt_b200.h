@@ -307,6 +307,16 @@ int sbwt_profile_enable(int enabled, int count_work);
  * per thread (1, 2, 4 or 8): the roofline denominator of the search kernels. */
 int sbwt_measure_random_sectors(int device, uint64_t bytes, int chains,
                                 double *gbs, double *sectors_per_s);
+/* Autotuner: times the read search on the first sample_chars chars of a
+ * device-resident batch over presearch depth 8..12, tile size (k-mers per
+ * lane work unit) {auto, 64, 256, 1024} and blocks per SM {2, 3, 4, 6, 8},
+ * checks that every configuration gives the same results, and makes the
+ * fastest the process-wide launch configuration. */
+int sbwt_autotune(const sbwt_index_t *index, const char *d_chars,
+                  uint64_t n_chars, const uint64_t *d_read_ends,
+                  uint64_t n_reads, uint64_t sample_chars,
+                  uint32_t *best_presearch, uint32_t *best_blocks_per_sm,
+                  uint64_t *best_tile, double *best_ms);
 /* Reads and resets the totals (any pointer may be NULL). */
 int sbwt_profile_read(double *search_ms, uint64_t *search_launches,
                       uint64_t *launches, uint64_t counters[4]);

@@ -1,5 +1,6 @@
 #include "formats.hpp"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -113,7 +114,11 @@ void IntVector::assign(const std::vector<u64> &values, u8 w) {
   width = w;
   num_bits = values.size() * static_cast<u64>(w);
   words.assign((num_bits + 63) / 64, 0);
-  for (u64 i = 0; i < values.size(); ++i) {
+  // chunks of 64 values start on word boundaries, so chunks never share words
+  const long chunks = (long)((values.size() + 63) / 64);
+#pragma omp parallel for schedule(static)
+  for (long ch = 0; ch < chunks; ++ch)
+  for (u64 i = (u64)ch * 64; i < std::min<u64>(values.size(), (u64)ch * 64 + 64); ++i) {
     u64 bit = i * w, wi = bit / 64, off = bit % 64;
     u64 v = w == 64 ? values[i] : (values[i] & ((1ULL << w) - 1));
     words[wi] |= v << off;

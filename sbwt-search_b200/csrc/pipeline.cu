@@ -697,3 +697,91 @@ int sbwt_server_stats(sbwt_server_t *s, double *p50_s, double *p99_s, uint64_t *
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Autotuner
+// ---------------------------------------------------------------------------
+extern "C" {
+// Times the read search (device-resident inputs, the first reads of the given
+// batch up to sample_chars chars) over presearch depths 8..12 (not above the
+// index's), tile sizes {64, 256, 1024, auto} and 256-thread blocks per SM
+// {2, 3, 4, 6, 8}; every configuration must reproduce the first run's
+// results.  The fastest becomes the process-wide launch configuration and is
+// written to *best (presearch, blocks_per_sm, tile) with its time in ms.
+int sbwt_autotune(const sbwt_index_t *index, const char *d_chars, uint64_t n_chars,
+                  const uint64_t *d_read_ends, uint64_t n_reads, uint64_t sample_chars,
+                  uint32_t *best_presearch, uint32_t *best_blocks_per_sm,
+                  uint64_t *best_tile, double *best_ms) {
+  if (!index || !d_chars || !d_read_ends || !n_reads) {
+    set_last_error("null argument");
+    return SBWT_E_INVALID;
+  }
+  return guarded([&] {
+    const IndexImpl &ix = *index->impl;
+    DeviceGuard g(ix.device);
+    // sample: the reads whose ends are within sample_chars
+    std::vector<u64> ends(n_reads);
+    SBWT_CUDA(cudaMemcpy(ends.data(), d_read_ends, n_reads * 8, cudaMemcpyDeviceToHost));
+    u64 nr = 0;
+    while (nr < n_reads && ends[nr] <= std::min<u64>(sample_chars, n_chars)) ++nr;
+    if (nr == 0) nr = 1;
+    const u64 nc = ends[nr - 1];
+    const u64 nk = count_kmers_host(ends.data(), nr, ix.k, 0);
+    DeviceBuffer out(std::max<u64>(nk, 1) * 8), ref(std::max<u64>(nk, 1) * 8);
+    cudaStream_t st;
+    SBWT_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cudaEvent_t e0, e1;
+    SBWT_CUDA(cudaEventCreate(&e0));
+    SBWT_CUDA(cudaEventCreate(&e1));
+    LaunchConfig saved = default_launch_config();
+    double best = 1e30;
+    LaunchConfig best_cfg = saved;
+    bool have_ref = false;
+    std::vector<u64> h_ref, h_out;
+    for (u32 p = std::min<u32>(12, ix.p_max); p >= std::min<u32>(8, ix.p_max); --p) {
+      for (u64 tile : {0ULL, 64ULL, 256ULL, 1024ULL}) {
+        for (u32 bps : {2u, 3u, 4u, 6u, 8u}) {
+          LaunchConfig c = saved;
+          c.presearch_letters = p;
+          c.tile = tile;
+          c.blocks_per_sm = bps;
+          default_launch_config() = c;
+          u64 n = 0;
+          ix.search_reads(d_chars, nc, d_read_ends, nr, out.get<u64>(), nk, &n,
+                          SBWT_DEVICE_POINTERS, st, c);  // warm
+          SBWT_CUDA(cudaEventRecord(e0, st));
+          for (int rep = 0; rep < 3; ++rep)
+            ix.search_reads(d_chars, nc, d_read_ends, nr, out.get<u64>(), nk, &n,
+                            SBWT_DEVICE_POINTERS, st, c);
+          SBWT_CUDA(cudaEventRecord(e1, st));
+          SBWT_CUDA(cudaEventSynchronize(e1));
+          float ms = 0;
+          SBWT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          h_out.resize(nk);
+          SBWT_CUDA(cudaMemcpy(h_out.data(), out.get(), nk * 8, cudaMemcpyDeviceToHost));
+          if (!have_ref) {
+            h_ref = h_out;
+            have_ref = true;
+          } else if (h_out != h_ref) {
+            default_launch_config() = saved;
+            throw Error(SBWT_E_CUDA, "autotune: a configuration changed the results");
+          }
+          if (ms / 3 < best) {
+            best = ms / 3;
+            best_cfg = c;
+          }
+        }
+      }
+      if (p == 0) break;
+    }
+    default_launch_config() = best_cfg;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    if (best_presearch) *best_presearch = best_cfg.presearch_letters;
+    if (best_blocks_per_sm) *best_blocks_per_sm = best_cfg.blocks_per_sm;
+    if (best_tile) *best_tile = best_cfg.tile;
+    if (best_ms) *best_ms = best;
+  });
+}
+}

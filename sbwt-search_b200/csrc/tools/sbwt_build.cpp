@@ -17,8 +17,11 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <random>
@@ -31,6 +34,13 @@
 
 namespace sbwt {
 namespace tools {
+
+// Phase timing on stderr when SBWT_TOOLS_VERBOSE is set.
+static double wall() { return omp_get_wtime(); }
+static void phase(const char *name, double &t) {
+  if (std::getenv("SBWT_TOOLS_VERBOSE")) std::fprintf(stderr, "[tools] %-28s %.2f s\n", name, wall() - t);
+  t = wall();
+}
 
 static inline int code_of(char c) {
   switch (c) {
@@ -358,71 +368,152 @@ u64 sbwt_tools_build_colored(const char *const *genomes, const u64 *lens,
                              const char *sbwt_path, const char *tcolors_path) {
   try {
     if (k < 1 || k > 31) throw std::runtime_error("builder supports 1 <= k <= 31");
-    std::vector<const char *> sv(genomes, genomes + n_genomes);
-    std::vector<u64> lv(lens, lens + n_genomes);
-    auto keys = extract_kmers(sv, lv, k, add_rc != 0);
-    sort_unique(keys);
-    Built b = build_from_keys(std::move(keys), k);
-    write_sbwt(sbwt_path, b.sbwt);
-    const u64 n = b.kmers.size();
-    // (k-mer rank, color) pairs, per genome in parallel
-    std::vector<std::vector<u64>> per(n_genomes);
-#pragma omp parallel for schedule(dynamic, 1)
+    double tt = wall();
+    // (k-mer, genome) pairs of every genome (both strands), sorted by k-mer
+    // then genome: the runs give the k-mer set and each k-mer's color list.
+    struct KG {
+      u64 key;
+      u64 g;
+      bool operator<(const KG &o) const { return key < o.key || (key == o.key && g < o.g); }
+    };
+    std::vector<u64> gbase(n_genomes + 1, 0);
     for (u64 g = 0; g < n_genomes; ++g) {
-      auto ks = extract_kmers({genomes[g]}, {lens[g]}, k, add_rc != 0);
-      std::sort(ks.begin(), ks.end());
-      ks.erase(std::unique(ks.begin(), ks.end()), ks.end());
-      auto &v = per[g];
-      v.reserve(ks.size());
-      u64 cur = 0;
-      for (u64 x : ks) {
-        while (b.kmers[cur] < x) ++cur;
-        v.push_back(cur);
+      const u64 m = lens[g] >= (u64)k ? lens[g] - k + 1 : 0;
+      gbase[g + 1] = gbase[g] + m * (add_rc ? 2 : 1);
+    }
+    std::vector<KG> pairs(gbase[n_genomes]);
+    std::vector<u8> pvalid(gbase[n_genomes], 0);
+    {
+      const u64 top = 2ULL * (k - 1);
+      const u64 kmask = (1ULL << (2 * k)) - 1;
+#pragma omp parallel for schedule(dynamic, 1)
+      for (u64 g = 0; g < n_genomes; ++g) {
+        const char *p = genomes[g];
+        u64 fwd = 0, rev = 0, o = gbase[g];
+        int run = 0;
+        for (u64 i = 0; i < lens[g]; ++i) {
+          const int c = code_of(p[i]);
+          if (c < 0) {
+            run = 0;
+            fwd = rev = 0;
+          } else {
+            fwd = (fwd >> 2) | ((u64)c << top);
+            rev = ((rev << 2) | (u64)(3 - c)) & kmask;
+            ++run;
+          }
+          if (i + 1 >= (u64)k && run >= k) {
+            const u64 slot = (i + 1 - k) * (add_rc ? 2 : 1);
+            pairs[o + slot] = KG{fwd, g};
+            pvalid[o + slot] = 1;
+            if (add_rc) {
+              pairs[o + slot + 1] = KG{rev, g};
+              pvalid[o + slot + 1] = 1;
+            }
+          }
+        }
       }
     }
-    // color list per k-mer (CSR)
-    std::vector<u64> cnt(n + 1, 0);
-    for (auto &v : per)
-      for (u64 r : v) cnt[r + 1]++;
-    for (u64 i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
-    std::vector<u32> colors(cnt[n]);
-    {
-      std::vector<u64> pos(cnt.begin(), cnt.end() - 1);
-      for (u64 g = 0; g < n_genomes; ++g)
-        for (u64 r : per[g]) colors[pos[r]++] = (u32)g;
+    phase("extract pairs", tt);
+    {  // bucket by the top 12 key bits, sort each bucket
+      const int B = 4096, shift = 2 * k - 12 > 0 ? 2 * k - 12 : 0;
+      const u64 np = pairs.size();
+      std::vector<u64> bstart(B + 2, 0);
+      for (u64 i = 0; i < np; ++i)
+        if (pvalid[i]) bstart[std::min<u64>(pairs[i].key >> shift, B - 1) + 1]++;
+      for (int x = 0; x < B; ++x) bstart[x + 1] += bstart[x];
+      std::vector<KG> out(bstart[B]);
+      std::vector<u64> cur(bstart.begin(), bstart.begin() + B);
+      for (u64 i = 0; i < np; ++i)
+        if (pvalid[i]) out[cur[std::min<u64>(pairs[i].key >> shift, B - 1)]++] = pairs[i];
+      pairs.swap(out);
+      std::vector<u8>().swap(pvalid);
+#pragma omp parallel for schedule(dynamic, 8)
+      for (int x = 0; x < B; ++x) std::sort(pairs.begin() + bstart[x], pairs.begin() + bstart[x + 1]);
     }
-    per.clear();
-    // dedupe color sets by hash of the sorted lists
-    std::unordered_map<u64, std::vector<u64>> buckets;
+    phase("sort pairs", tt);
+    // unique k-mers + CSR of unique (k-mer, genome) colors
+    std::vector<u64> keys;
+    std::vector<u64> cnt;
+    std::vector<u32> colors;
+    keys.reserve(pairs.size() / 2);
+    cnt.reserve(pairs.size() / 2 + 1);
+    colors.reserve(pairs.size() / 2);
+    cnt.push_back(0);
+    for (u64 i = 0; i < pairs.size(); ++i) {
+      if (i == 0 || pairs[i].key != pairs[i - 1].key) {
+        if (i) cnt.push_back(colors.size());
+        keys.push_back(pairs[i].key);
+        colors.push_back((u32)pairs[i].g);
+      } else if (pairs[i].g != pairs[i - 1].g) {
+        colors.push_back((u32)pairs[i].g);
+      }
+    }
+    cnt.push_back(colors.size());
+    std::vector<KG>().swap(pairs);
+    phase("k-mer set + colors", tt);
+    Built b = build_from_keys(std::move(keys), k);
+    phase("build_from_keys", tt);
+    write_sbwt(sbwt_path, b.sbwt);
+    phase("write_sbwt", tt);
+    const u64 n = b.kmers.size();
+    // dedupe color sets: singletons by color, the rest by hash
     std::vector<u64> set_of_kmer(n);
     std::vector<u64> set_first;  // k-mer rank whose list defines the set
-    auto hash_of = [&](u64 r) {
-      u64 h = 1469598103934665603ULL ^ (cnt[r + 1] - cnt[r]);
-      for (u64 t = cnt[r]; t < cnt[r + 1]; ++t)
-        h = (h ^ colors[t]) * 1099511628211ULL;
-      return h;
-    };
-    auto same = [&](u64 a, u64 bb) {
-      u64 la = cnt[a + 1] - cnt[a], lb = cnt[bb + 1] - cnt[bb];
-      return la == lb && std::equal(colors.begin() + cnt[a],
-                                    colors.begin() + cnt[a + 1],
-                                    colors.begin() + cnt[bb]);
-    };
-    for (u64 r = 0; r < n; ++r) {
-      auto &bk = buckets[hash_of(r)];
-      u64 id = ~0ULL;
-      for (u64 s : bk)
-        if (same(set_first[s], r)) {
-          id = s;
-          break;
+    {
+      std::vector<u64> single_first(n_genomes, ~0ULL);
+      for (u64 r = 0; r < n; ++r)
+        if (cnt[r + 1] - cnt[r] == 1 && single_first[colors[cnt[r]]] == ~0ULL)
+          single_first[colors[cnt[r]]] = r;
+      std::vector<u64> single_id(n_genomes, ~0ULL);
+      for (u64 g = 0; g < n_genomes; ++g)
+        if (single_first[g] != ~0ULL) {
+          single_id[g] = set_first.size();
+          set_first.push_back(single_first[g]);
         }
-      if (id == ~0ULL) {
-        id = set_first.size();
-        set_first.push_back(r);
-        bk.push_back(id);
+      auto hash_of = [&](u64 r) {
+        u64 h = 1469598103934665603ULL ^ (cnt[r + 1] - cnt[r]);
+        for (u64 t = cnt[r]; t < cnt[r + 1]; ++t) h = (h ^ colors[t]) * 1099511628211ULL;
+        h ^= h >> 29;
+        return h * 0xBF58476D1CE4E5B9ULL;
+      };
+      auto same = [&](u64 a, u64 bb) {
+        u64 la = cnt[a + 1] - cnt[a], lb = cnt[bb + 1] - cnt[bb];
+        return la == lb && std::equal(colors.begin() + cnt[a], colors.begin() + cnt[a + 1],
+                                      colors.begin() + cnt[bb]);
+      };
+      std::vector<std::pair<u64, u64>> multi;  // (hash, rank)
+      for (u64 r = 0; r < n; ++r) {
+        if (cnt[r + 1] - cnt[r] == 1)
+          set_of_kmer[r] = single_id[colors[cnt[r]]];
+        else
+          multi.push_back({0, r});
       }
-      set_of_kmer[r] = id;
+#pragma omp parallel for schedule(static)
+      for (u64 i = 0; i < multi.size(); ++i) multi[i].first = hash_of(multi[i].second);
+      std::sort(multi.begin(), multi.end());
+      for (u64 i = 0; i < multi.size();) {
+        u64 j = i;
+        while (j < multi.size() && multi[j].first == multi[i].first) ++j;
+        std::vector<u64> local;
+        for (u64 q = i; q < j; ++q) {
+          const u64 r = multi[q].second;
+          u64 id = ~0ULL;
+          for (u64 f : local)
+            if (same(set_first[f], r)) {
+              id = f;
+              break;
+            }
+          if (id == ~0ULL) {
+            id = set_first.size();
+            set_first.push_back(r);
+            local.push_back(id);
+          }
+          set_of_kmer[r] = id;
+        }
+        i = j;
+      }
     }
+    phase("csr + dedupe", tt);
     const u64 C = n_genomes;
     const u64 S = set_first.size();
     // dense iff |set| > C/64 (the rule Themisto's hybrid storage uses)
@@ -433,6 +524,7 @@ u64 sbwt_tools_build_colored(const char *const *genomes, const u64 *lens,
     }
     // color set ids: renumber so ids follow first appearance (any order is
     // valid for the format); dense/sparse payloads in id order.
+    double t0 = tt;
     TColorsFile t;
     t.is_dense_marks.resize(S);
     std::vector<u64> dense_iv{0}, sparse_iv{0}, sparse_vals;
@@ -481,7 +573,9 @@ u64 sbwt_tools_build_colored(const char *const *genomes, const u64 *lens,
     t.sum_color_set_sizes = 0;
     for (u64 s = 0; s < S; ++s)
       t.sum_color_set_sizes += cnt[set_first[s] + 1] - cnt[set_first[s]];
+    phase("payloads", t0);
     write_tcolors(tcolors_path, t);
+    phase("write_tcolors", t0);
     return b.sbwt.n_nodes;
   } catch (const std::exception &e) {
     g_tools_err = e.what();

@@ -104,6 +104,8 @@ def lib():
                                         C.POINTER(C.c_double), C.c_int]
         L.sbwt_free.argtypes = [vp]
         L.sbwt_free.restype = None
+        L.sbwt_autotune.argtypes = [vp, vp, u64, vp, u64, u64, C.POINTER(u32),
+                                    C.POINTER(u32), C.POINTER(u64), C.POINTER(C.c_double)]
         _L = L
     return _L
 
@@ -425,3 +427,42 @@ class Server:
                                       C.byref(rd), C.byref(nb), C.byref(el), int(reset)))
         return {"p50_s": p50.value, "p99_s": p99.value, "requests": nd.value,
                 "reads": rd.value, "batches": nb.value, "elapsed_s": el.value}
+
+
+AUTOTUNE_CACHE = HERE / "_build" / "autotune.json"
+
+
+def autotune(index: SbwtIndex, d_chars, d_read_ends, sample_chars: int = 256 << 20,
+             use_cache: bool = True) -> dict:
+    """Chooses presearch depth, tile size and blocks per SM for this GPU and
+    index with the library's autotuner (sbwt_autotune) and applies them; the
+    choice is cached per (GPU name, SBWT nodes, k) in _build/autotune.json."""
+    import json
+    try:
+        import torch
+        gpu = torch.cuda.get_device_name(index.device)
+    except Exception:
+        gpu = "cuda"
+    key = f"{gpu}|{index.num_bits}|{index.k}"
+    cache = {}
+    if use_cache and AUTOTUNE_CACHE.exists():
+        try:
+            cache = json.loads(AUTOTUNE_CACHE.read_text())
+        except Exception:
+            cache = {}
+    if use_cache and key in cache:
+        c = cache[key]
+        set_launch_config(c["presearch"], c["blocks_per_sm"], c["tile"], 0)
+        return dict(c, cached=True)
+    p, b = C.c_uint32(), C.c_uint32()
+    t, ms = C.c_uint64(), C.c_double()
+    check(lib().sbwt_autotune(index._h, _ptr(d_chars), d_chars.numel(), _ptr(d_read_ends),
+                              d_read_ends.numel(), sample_chars, C.byref(p), C.byref(b),
+                              C.byref(t), C.byref(ms)))
+    c = {"presearch": p.value, "blocks_per_sm": b.value, "tile": t.value,
+         "sample_ms": ms.value}
+    if use_cache:
+        cache[key] = c
+        AUTOTUNE_CACHE.parent.mkdir(parents=True, exist_ok=True)
+        AUTOTUNE_CACHE.write_text(json.dumps(cache, indent=1))
+    return dict(c, cached=False)

@@ -44,6 +44,217 @@ CFG = dict(n_genomes=40, genome_len=2_500_000, n_founders=4, sub=0.02, indel=0.0
            len_max=1000, read_sub=0.005, n_rate=0.001)
 
 
+# pseudoalignment workload: 2000 genomes of 100 kbp from 8 random founders at
+# 1-5 % divergence, k = 31, both strands; 5 M reads of 150 bp from random
+# genomes with 0.5 % substitutions; tau = 0.7, not-found / invalid excluded.
+CFG3 = dict(n_genomes=2000, genome_len=100_000, n_founders=8, sub_lo=0.01, sub_hi=0.05,
+            k=31, n_reads=5_000_000, read_len=150, read_sub=0.005, tau=0.7)
+# batched mixed workload against the index above: 256 files, read counts
+# log-uniform in [50, 1e5] (the [1e3, 2e6] of the full-size workload scaled
+# by 1/20 in read count so that it fits the default run), 10 % of the files
+# with 1-10 kbp reads, the rest 100 bp, 5 % substitutions.
+CFG4 = dict(n_files=256, reads_lo=50, reads_hi=100_000, long_frac=0.1, short_len=100,
+            long_lo=1000, long_hi=10_000, sub=0.05)
+
+
+def bench_batched(args, idx, S, torch, dev, scratch):
+    """Batched (one call over all files = one persistent launch fed by the
+    device work queue, after the autotuner) vs plain (one call per file, the
+    reference's per-file launch pattern), device-resident, bit-exact."""
+    import sbwt_tools as T
+    rng = np.random.default_rng(7)
+    g = T.gen_genomes(20240601, CFG["n_genomes"], CFG["genome_len"], CFG["n_founders"],
+                      CFG["sub"], CFG["sub"], CFG["indel"])
+    files = []
+    for f in range(CFG4["n_files"]):
+        n = int(np.exp(rng.uniform(np.log(CFG4["reads_lo"]), np.log(CFG4["reads_hi"]))))
+        if rng.random() < CFG4["long_frac"]:
+            ch, en = T.gen_reads(9000 + f, g, n, 1.0, 3000, 0.6, CFG4["long_lo"],
+                                 CFG4["long_hi"], CFG4["sub"], 0.0)
+        else:
+            ch, en = T.gen_reads(9000 + f, g, n, 1.0, CFG4["short_len"], 0.0,
+                                 CFG4["short_len"], CFG4["short_len"], CFG4["sub"], 0.0)
+        files.append((ch, en))
+    chars = np.concatenate([f[0] for f in files])
+    base = np.cumsum([0] + [len(f[0]) for f in files])[:-1]
+    ends = np.concatenate([f[1] + b for f, b in zip(files, base)]).astype(np.uint64)
+    n_k = idx.count_kmers(ends)
+    d_chars = torch.from_numpy(chars).to(f"cuda:{dev}")
+    d_ends = torch.from_numpy(ends.view(np.int64)).to(f"cuda:{dev}")
+    d_out = torch.empty(n_k, dtype=torch.int64, device=f"cuda:{dev}")
+    # plain: one call per file (each call synchronises, as the reference's
+    # per-batch copy-kernel-copy does)
+    fk = [idx.count_kmers(f[1]) for f in files]
+    koff = np.cumsum([0] + fk)
+    d_files = [(torch.from_numpy(f[0]).to(f"cuda:{dev}"),
+                torch.from_numpy(f[1].view(np.int64)).to(f"cuda:{dev}")) for f in files]
+    d_plain = torch.empty(n_k, dtype=torch.int64, device=f"cuda:{dev}")
+    S.set_launch_config()
+
+    def plain():
+        for i, (dc, de) in enumerate(d_files):
+            if fk[i]:
+                idx.search_reads(dc, de, out=d_plain[int(koff[i]):int(koff[i + 1])])
+
+    plain()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain()
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    tune = S.autotune(idx, d_chars, d_ends, sample_chars=64 << 20, use_cache=False)
+    idx.search_reads(d_chars, d_ends, out=d_out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        idx.search_reads(d_chars, d_ends, out=d_out)
+    e1.record()
+    torch.cuda.synchronize()
+    t_batch = e0.elapsed_time(e1) / 3 / 1e3
+    exact = bool(torch.equal(d_out, d_plain))
+    S.set_launch_config()
+    return {"workload": "256 files vs the 100 Mbp index, reads/file log-uniform [50, 1e5] "
+                        "(full-size range [1e3, 2e6] scaled 1/20), 10% files of 1-10 kbp "
+                        "reads, 5% substitutions", "files": len(files),
+            "reads": int(len(ends)), "kmers": int(n_k),
+            "batched_kmers_per_s": n_k / t_batch, "plain_kmers_per_s": n_k / t_plain,
+            "speedup": t_plain / t_batch, "bit_exact": exact, "autotune": tune}
+
+
+def bench_colors_and_serving(args, S, torch, dev, tmpdir, rank):
+    """Pseudoalignment reads/s (colors step, device-resident), the fused
+    reads -> colors pipeline (host in, host out), the CPU oracle on a sample,
+    and the serving loop's p50 / p99 latency at Poisson offered loads."""
+    import threading
+    import sbwt_tools as T
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as O
+    c = CFG3
+    t0 = time.time()
+    g = T.gen_genomes(33, c["n_genomes"], c["genome_len"], c["n_founders"], c["sub_lo"],
+                      c["sub_hi"], 0.0)
+    sp, cp = os.path.join(tmpdir, "cfg3.sbwt"), os.path.join(tmpdir, "cfg3.tcolors")
+    nodes = T.build_colored(g, c["k"], sp, cp)
+    chars, ends = T.gen_reads(34, g, args.colors_reads, 1.0, c["read_len"], 0.0,
+                              c["read_len"], c["read_len"], c["read_sub"], 0.0)
+    t_setup = time.time() - t0
+    idx, ci = S.SbwtIndex.open(sp, device=dev), S.ColorIndex.open(cp, device=dev)
+    n_reads = len(ends)
+    n_k = idx.count_kmers(ends)
+    d_chars = torch.from_numpy(chars).to(f"cuda:{dev}")
+    d_ends = torch.from_numpy(ends.view(np.int64)).to(f"cuda:{dev}")
+    d_res = torch.empty(n_k, dtype=torch.int64, device=f"cuda:{dev}")
+    idx.search_reads(d_chars, d_ends, out=d_res)
+    # the colors step's input: found indexes per read (+ -1 / -2 counts)
+    kpr = n_k // n_reads  # fixed-length reads
+    res2 = d_res.view(n_reads, kpr)
+    found_mask = (res2 >= 0)
+    d_found = d_res[found_mask.view(-1)].contiguous()
+    d_offs = torch.zeros(n_reads + 1, dtype=torch.int64, device=f"cuda:{dev}")
+    d_offs[1:] = torch.cumsum(found_mask.sum(1), 0)
+    d_ids_off = torch.empty(n_reads + 1, dtype=torch.int64, device=f"cuda:{dev}")
+    cap = n_reads * 64
+    d_ids = torch.empty(cap, dtype=torch.int32, device=f"cuda:{dev}")
+    L = S.lib()
+    stream = torch.cuda.current_stream(dev)
+
+    def colors_step():
+        S.check(L.sbwt_pseudoalign(ci._h, d_found.data_ptr(), d_offs.data_ptr(), None, None,
+                                   n_reads, c["tau"], S.DEVICE_POINTERS, d_ids.data_ptr(), cap,
+                                   d_ids_off.data_ptr(), stream.cuda_stream))
+
+    for _ in range(2):
+        colors_step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(3):
+        colors_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_col = e0.elapsed_time(e1) / 3 / 1e3
+    n_ids = int(d_ids_off[-1].item())
+    # parity spot check against the oracle on the first reads
+    chk = 2000
+    offs_h = d_offs[:chk + 1].cpu().numpy().view(np.uint64)
+    found_h = d_found[:int(offs_h[-1])].cpu().numpy().view(np.uint64)
+    ids_off_h = d_ids_off[:chk + 1].cpu().numpy()
+    ids_h = d_ids[:int(ids_off_h[-1])].cpu().numpy()
+    got = [ids_h[ids_off_h[r]:ids_off_h[r + 1]].tolist() for r in range(chk)]
+    oc = O.OracleColors(O.ColorsFile.read(cp))
+    t1 = time.perf_counter()
+    exp = oc.pseudoalign([found_h[offs_h[r]:offs_h[r + 1]] for r in range(chk)], [0] * chk,
+                         [0] * chk, c["tau"])
+    t_cpu = time.perf_counter() - t1
+    colors = {"workload": "2000 genomes x 100 kbp from 8 founders (1-5% divergence), k=31, "
+                          f"{n_reads} reads x 150 bp, 0.5% substitutions, tau 0.7",
+              "nodes": nodes, "reads": n_reads, "kmers": int(n_k), "ids": n_ids,
+              "reads_per_s": n_reads / t_col, "ms_per_step": t_col * 1e3,
+              "bit_exact_sample": got == exp, "setup_s": t_setup,
+              "cpu_baseline": {"value": chk / t_cpu, "unit": "reads/s", "cores": 1,
+                               "kind": "port", "sample": f"first {chk} reads"}}
+    del d_res, d_found, d_ids, found_mask, res2
+    torch.cuda.empty_cache()
+    # fused reads -> colors pipeline from host memory (CUDA graph per batch)
+    batch = 1 << 20
+    pipe = S.Pipeline(idx, ci, batch * c["read_len"], batch, tau=c["tau"])
+    nb = min(4, n_reads // batch)
+    pipe.run(chars[:int(ends[batch - 1])], ends[:batch], raw=True)
+    t1 = time.perf_counter()
+    for b in range(nb):
+        lo = b * batch
+        base = int(ends[lo - 1]) if lo else 0
+        pipe.run(chars[base:int(ends[lo + batch - 1])], ends[lo:lo + batch] - base, raw=True)
+    t_pipe = time.perf_counter() - t1
+    colors["fused_pipeline_reads_per_s"] = nb * batch / t_pipe
+    pipe.close()
+    # serving loop: Poisson arrivals, log-uniform request sizes in [1, 1e5]
+    srv = S.Server(idx, ci, batch_chars=32 << 20, batch_reads=1 << 18, slots=3, tau=c["tau"])
+    rng = np.random.default_rng(11)
+    serving = {"offline_reads_per_s": colors["fused_pipeline_reads_per_s"], "loads": []}
+    for offered in (1e5, 1e6, 1e7):
+        mean_size = (1e5 - 1) / np.log(1e5)
+        rate = offered / mean_size
+        pending = []
+        stop = threading.Event()
+
+        def collector():
+            while not stop.is_set() or pending:
+                if pending:
+                    srv.wait(pending.pop(0), raw=True)
+                else:
+                    time.sleep(0.0005)
+
+        th = threading.Thread(target=collector)
+        th.start()
+        srv.stats(reset=True)
+        t_start = time.perf_counter()
+        t_next = t_start
+        while t_next - t_start < args.serve_seconds:
+            now = time.perf_counter()
+            if now < t_next:
+                time.sleep(min(t_next - now, 0.002))
+                continue
+            size = int(np.exp(rng.uniform(0, np.log(1e5))))
+            lo = int(rng.integers(0, n_reads - size))
+            base = int(ends[lo - 1]) if lo else 0
+            pending.append(srv.submit(chars[base:int(ends[lo + size - 1])],
+                                      ends[lo:lo + size] - base))
+            t_next += rng.exponential(1.0 / rate)
+        t_window = time.perf_counter() - t_start
+        stop.set()
+        th.join()
+        st = srv.stats()
+        serving["loads"].append({"offered_reads_per_s": offered,
+                                 "achieved_reads_per_s": st["reads"] / max(st["elapsed_s"], 1e-9),
+                                 "arrival_window_s": t_window, "drain_s": st["elapsed_s"] - t_window,
+                                 "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3,
+                                 "requests": st["requests"], "batches": st["batches"]})
+    srv.close()
+    return {"colors": colors, "serving": serving}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -54,7 +265,25 @@ def parse():
     ap.add_argument("--presearch", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-sample-reads", type=int, default=60_000)
+    ap.add_argument("--index-only", action="store_true",
+                    help="skip the batched, colors and serving sections")
+    ap.add_argument("--colors-reads", type=int, default=CFG3["n_reads"])
+    ap.add_argument("--serve-seconds", type=float, default=3.0)
     return ap.parse_args()
+
+
+def profiled_traffic_per_kmer():
+    """DRAM bytes (read + write) per k-mer of the search kernel from the
+    committed ncu capture of the 1 M-read case; traffic grows with the k-mers
+    processed, so it scales to a full launch by the k-mer count."""
+    p = REPO / "profiles" / "search_reads_kernel_100Mbp_1Mreads_full.md"
+    try:
+        for ln in p.read_text().splitlines():
+            if ln.startswith("traffic_bytes_per_kmer:"):
+                return float(ln.split(":")[1])
+    except OSError:
+        pass
+    return None
 
 
 def load_peaks():
@@ -305,6 +534,21 @@ def main():
     # packed input + 1 invalid bit per char.
     alg_bytes = ((n_pre + n_block + n_sg) * 32 + n_kmers * 8 + n_chars / 4 + n_chars / 8)
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9
+    traffic_pk = profiled_traffic_per_kmer()
+
+    extra = {}
+    if not args.index_only:
+        torch.cuda.empty_cache()
+        try:
+            extra["batched"] = bench_batched(args, idx, S, torch, dev, d_out)
+        except Exception as e:  # reported, never hides the headline
+            extra["batched"] = {"error": repr(e)}
+        del d_out, d_chars, d_ends
+        torch.cuda.empty_cache()
+        try:
+            extra.update(bench_colors_and_serving(args, S, torch, dev, tmp.name, rank))
+        except Exception as e:
+            extra["colors"] = {"error": repr(e)}
 
     cpu = None
     if rank == 0:
@@ -332,7 +576,10 @@ def main():
                    "presearch_letters": idx.presearch_letters},
         "gpu_launches": int(launches.value),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak,
+                     "traffic": (None if traffic_pk is None else traffic_pk * n_kmers),
+                     "traffic_source": "ncu capture of the 1 M-read case scaled by k-mers "
+                                       "(profiles/search_reads_kernel_100Mbp_1Mreads_full.md)",
                      "peak_kind": peak_kind, "kernel": "search_reads_kernel",
                      "kernel_ms": kern_ms,
                      "work": {"presearch_lookups": n_pre, "rank_block_sectors": n_block,
@@ -343,6 +590,7 @@ def main():
         "clocks": clk.summary(),
         "setup_s": t_gen,
     }
+    line.update(extra)
     if rank == 0:
         print(json.dumps(line), flush=True)
     idx.close()

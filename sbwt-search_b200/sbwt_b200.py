@@ -340,7 +340,9 @@ class Pipeline:
         except Exception:
             pass
 
-    def run(self, chars, read_ends):
+    def run(self, chars, read_ends, raw: bool = False):
+        """Index mode: u64 per k-mer.  Colors mode: per-read id lists, or with
+        raw=True the (ids, offsets) arrays without building Python lists."""
         chars = _np_chars(chars)
         read_ends = np.ascontiguousarray(read_ends, dtype=np.uint64)
         n = len(read_ends)
@@ -362,6 +364,8 @@ class Pipeline:
                 cap = int(offs[n]) + 1
                 continue
             check(rc)
+            if raw:
+                return ids[:int(offs[n])], offs
             return [ids[int(offs[r]):int(offs[r + 1])].tolist() for r in range(n)]
 
 
@@ -400,7 +404,9 @@ class Server:
                                        len(read_ends), C.byref(rid)))
         return rid.value
 
-    def wait(self, rid: int, timeout_ms: float = -1.0):
+    def wait(self, rid: int, timeout_ms: float = -1.0, raw: bool = False):
+        """Index mode: (values, offsets).  Colors mode: per-read id lists, or
+        with raw=True the (ids, offsets) arrays."""
         vals, ids, offs = C.c_void_p(), C.c_void_p(), C.c_void_p()
         nv, ni, nr = C.c_uint64(), C.c_uint64(), C.c_uint64()
         check(lib().sbwt_server_wait(self._h, rid, timeout_ms, C.byref(vals), C.byref(nv),
@@ -415,6 +421,8 @@ class Server:
                 return v, o
             i = np.ctypeslib.as_array(C.cast(ids, C.POINTER(C.c_uint32)),
                                       (max(ni.value, 1),))[:ni.value].copy()
+            if raw:
+                return i, o
             return [i[int(o[r]):int(o[r + 1])].tolist() for r in range(nr.value)]
         finally:
             for p in (vals, ids, offs):

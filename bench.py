@@ -354,16 +354,12 @@ def make_workload(seed_reads: int, n_reads: int, tmpdir: str):
 
 
 def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    pg = None
-    if world > 1:
-        import torch.distributed as dist
-        import datetime
-        backend = "nccl" if args.impl == "ours" else "gloo"
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
-        pg = dist
+    import replicas as R
+    world, rank, local = R.world()
+    if world > 1 and args.impl == "ours":
+        import torch
+        torch.cuda.set_device(local)
+    pg = R.init("nccl" if args.impl == "ours" else "gloo", timeout_s=900)
     return world, rank, local, pg
 
 
@@ -489,10 +485,8 @@ def main():
     L.sbwt_profile_read(C.byref(search_ms), C.byref(search_launches), C.byref(launches),
                         None)
     L.sbwt_profile_enable(0, 0)
-    if pg:
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    import replicas as R
+    ms = R.max_over_ranks(pg, ms, device=f"cuda:{dev}")  # slowest rank
     ms_step = ms / args.steps
     value = n_kmers * world / (ms_step / 1e3)
 
@@ -516,10 +510,7 @@ def main():
         for _ in range(e_steps):
             idx.search_reads(hc, he, out=ho)
         e_dt = (time.perf_counter() - t0) / e_steps
-        if pg:
-            t = torch.tensor([e_dt], dtype=torch.float64, device=f"cuda:{dev}")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            e_dt = float(t.item())
+        e_dt = R.max_over_ranks(pg, e_dt, device=f"cuda:{dev}")
         assert np.array_equal(ho[:200_000], out_host), "e2e output differs from device path"
         e2e = {"value": n_kmers * world / e_dt, "unit": UNIT,
                "h2d_bytes_per_step": int(chars.nbytes + ends.nbytes),
@@ -537,7 +528,7 @@ def main():
     traffic_pk = profiled_traffic_per_kmer()
 
     extra = {}
-    if not args.index_only:
+    if not args.index_only and rank == 0:  # per-GPU sections: rank 0 only
         torch.cuda.empty_cache()
         try:
             extra["batched"] = bench_batched(args, idx, S, torch, dev, d_out)

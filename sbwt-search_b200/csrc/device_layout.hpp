@@ -38,6 +38,12 @@ struct Block {
 struct SbwtView {
   const Block *blocks[4];
   const uint64_t *l0[4];
+  // the same arrays addressed arithmetically (vector c at base + c * stride),
+  // so a per-lane char does not index a parameter array
+  const Block *blocks0;
+  uint64_t block_stride;  // in blocks
+  const uint64_t *l00;
+  uint64_t l0_stride;     // in entries
   uint64_t c_map[5];
   const uint64_t *presearch;  // pyramid of levels 1..presearch_max
   const uint64_t *suffix_group_starts;  // N bits or nullptr

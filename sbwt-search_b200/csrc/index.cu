@@ -328,6 +328,7 @@ struct ReadsView {
   uint32_t probe_len;       // L of the absent-prefix probe (0 = off)
   const uint64_t *n_kmers_dev;  // if set, the k-mer total is read from here
   unsigned long long *queue;    // work-queue counter (tiles handed out), zeroed
+  uint64_t n_kmers_bound;       // > every chunk position, slot and read number
 };
 
 __device__ __forceinline__ bool invalid_at(const uint32_t *inv, uint64_t i) {
@@ -465,19 +466,66 @@ constexpr uint64_t kNarrowLimit = (uint64_t)kBlockBits << kSuperchunkShift;
 #define SBWT_SEARCH_MIN_BLOCKS 4  // 256-thread blocks per SM the register budget targets
 #endif
 
-// Node-index arithmetic of the search kernel: 32-bit when the SBWT has fewer
-// than 224 * 2^24 nodes (one superchunk: no l0 table, all ranks fit in 32
-// bits), else 64-bit.
+// Index arithmetic of the search kernel: all 32-bit (nodes, chunk
+// positions, k-mer slots, read numbers) when the SBWT has fewer than
+// 224 * 2^24 nodes (one superchunk: no l0 table) and the batch fewer than
+// 2^32 chars, else all 64-bit.
 template <class I>
-struct NodeMath {
-  static constexpr I kNone = ~I(0);
-  __device__ __forceinline__ static I block(I i) {
-    return (I)((uint32_t)((uint64_t)i >> 5) / 7u);
+__device__ __forceinline__ I block_idx(I i) {
+  return (I)((uint32_t)((uint64_t)i >> 5) / 7u);
+}
+
+// Per-lane register window over the packed chars and invalid bits (see
+// CharWindow); index type I.
+template <class I>
+struct CharWin {
+  uint64_t w0, w1, inv;
+  I wbase;
+  __device__ __forceinline__ void init() {
+    wbase = (I)~(I)1;  // neither equal to nor one below any real word index
+    w0 = w1 = inv = 0;
   }
-  __device__ __forceinline__ static I rank(const SbwtView &s, uint32_t c, I b,
-                                           const Block &B, uint32_t q) {
-    if (sizeof(I) == 4) return (I)s.c_map[c] + (I)block_rank(B, q);
-    return (I)(s.c_map[c] + s.l0[c][(uint64_t)b >> kSuperchunkShift] + block_rank(B, q));
+  __device__ __forceinline__ void move_to(const uint64_t *packed, const uint32_t *invalid,
+                                          I pos) {
+    const I wb = pos >> 5;
+    if (wb == wbase) return;
+    if (wb == wbase + 1) {
+      w0 = w1;
+      w1 = __ldg(packed + wb + 1);
+      inv = (inv >> 32) | ((uint64_t)__ldg(invalid + wb + 1) << 32);
+    } else {
+      w0 = __ldg(packed + wb);
+      w1 = __ldg(packed + wb + 1);
+      inv = (uint64_t)__ldg(invalid + wb) | ((uint64_t)__ldg(invalid + wb + 1) << 32);
+    }
+    wbase = wb;
+  }
+  __device__ __forceinline__ uint32_t char_at(I i) const {
+    const uint32_t off = (uint32_t)(i - 32 * wbase);
+    const uint64_t w = off < 32 ? w0 : w1;
+    return (uint32_t)((w >> (62 - 2 * (off & 31))) & 3ULL);
+  }
+  __device__ __forceinline__ uint64_t prefix(I i, uint32_t n) const {
+    const uint32_t off = (uint32_t)(i - 32 * wbase);
+    uint64_t v;
+    if (off < 32) {
+      v = w0 << (2 * off);
+      if (off) v |= w1 >> (64 - 2 * off);
+    } else {
+      v = w1 << (2 * (off - 32));
+    }
+    return v >> (64 - 2 * n);
+  }
+  __device__ __forceinline__ bool invalid_at(I i) const {
+    return (inv >> (uint32_t)(i - 32 * wbase)) & 1ULL;
+  }
+  // 1 + highest invalid position in [a, b) (b - a <= 63), or 0
+  __device__ __forceinline__ I last_invalid1(I a, I b) const {
+    if (b <= a) return 0;
+    const uint32_t oa = (uint32_t)(a - 32 * wbase), ob = (uint32_t)(b - 32 * wbase);
+    uint64_t m = inv & (ob >= 64 ? ~0ULL : ((1ULL << ob) - 1));
+    m &= ~((1ULL << oa) - 1);
+    return m ? (I)(32 * wbase + 64 - __clzll(m)) : (I)0;
   }
 };
 
@@ -486,41 +534,47 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
     search_reads_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
                         uint32_t move_to_key, uint32_t *err,
                         unsigned long long *counters) {
-  using NM = NodeMath<I>;
-  constexpr I NONE = NM::kNone;
+  constexpr I NONE = ~I(0);
+  constexpr bool NARROW = sizeof(I) == 4;
+  __shared__ I sh_cmap[4];
+  if (threadIdx.x < 4) sh_cmap[threadIdx.x] = (I)s.c_map[threadIdx.x];
+  __syncthreads();
   const uint32_t k = s.k;
   const uint32_t L = rv.probe_len;
   const uint32_t lane = threadIdx.x & 31;
-  const uint64_t n_kmers = rv.n_kmers_dev ? *rv.n_kmers_dev : rv.n_kmers;
-  const uint64_t n_tiles = (n_kmers + rv.tile - 1) / rv.tile;
+  const I n_kmers = (I)(rv.n_kmers_dev ? *rv.n_kmers_dev : rv.n_kmers);
+  const I tsize = (I)rv.tile;
+  const I n_tiles = (n_kmers + tsize - 1) / tsize;
+  const I base = (I)rv.base;
   uint64_t n_pre = 0, n_block = 0, n_sg = 0, n_probe = 0;
   bool exhausted = false;  // the work queue is empty for this lane
-  uint64_t slot = 0, slot_end = 0, r = 0, r_next = 0, pos = 0, skip_until = 0;
-  int64_t last_inv = -1;
-  I v = NONE;  // node of the previous k-mer of this read
+  I slot = 0, slot_end = 0, r = 0, r_next = 0, pos = 0, skip_until = 0;
+  I last_inv1 = 0;  // 1 + last invalid char position (0 = none)
+  I v = NONE;       // node of the previous k-mer of this read
   I l = 0, rr = 0, u = 0;
-  uint64_t wi = 0, probe_end = 0, probe_skip = 0, pu = 0;
+  I wi = 0, probe_end = 0, probe_skip = 0, pu = 0;
   uint32_t mode = M_NEW, c = 0, ubit = 63;
   bool done = false;
-  CharWindow cw;
-  cw.init(rv.packed, rv.invalid);
+  CharWin<I> cw;
+  cw.init();
   while (true) {
     // ---- work queue (warp-collective): lanes out of k-mers take a new tile;
     // one atomic per warp hands out consecutive tiles.
     __syncwarp();
     const bool need = !exhausted && mode == M_NEW && slot >= slot_end;
     const unsigned need_mask = __ballot_sync(0xFFFFFFFFu, need);
-    uint64_t new_tile = ~0ULL;
+    I new_tile = NONE;
     if (need_mask) {
       const int leader = __ffs(need_mask) - 1;
-      unsigned long long base = 0;
-      if ((int)lane == leader) base = atomicAdd(rv.queue, (unsigned long long)__popc(need_mask));
-      base = __shfl_sync(0xFFFFFFFFu, base, leader);
+      unsigned long long qb = 0;
+      if ((int)lane == leader) qb = atomicAdd(rv.queue, (unsigned long long)__popc(need_mask));
+      qb = __shfl_sync(0xFFFFFFFFu, qb, leader);
       if (need) {
-        new_tile = base + __popc(need_mask & ((1u << lane) - 1u));
-        if (new_tile >= n_tiles) {
+        const unsigned long long t = qb + __popc(need_mask & ((1u << lane) - 1u));
+        if (t >= (unsigned long long)n_tiles) {
           exhausted = true;
-          new_tile = ~0ULL;
+        } else {
+          new_tile = (I)t;
         }
       }
     }
@@ -532,46 +586,44 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
       if (mode == M_NEW) {
         while (true) {
           if (slot >= slot_end) {  // next tile
-            if (new_tile == ~0ULL) {  // none this iteration
+            if (new_tile == NONE) {  // none this iteration
               done = exhausted;
               break;
             }
-            const uint64_t tile = new_tile;
-            new_tile = ~0ULL;
-            slot = tile * rv.tile;
-            slot_end = min(slot + rv.tile, n_kmers);
-            r = __ldg(tile_read + tile);
-            r_next = __ldg(rv.kmer_off + r + 1);
-            pos = (r ? __ldg(rv.ends + r - 1) : rv.base) - rv.base +
-                  (slot - __ldg(rv.kmer_off + r));
+            slot = new_tile * tsize;
+            new_tile = NONE;
+            slot_end = min(slot + tsize, n_kmers);
+            r = (I)__ldg(tile_read + slot / tsize);
+            r_next = (I)__ldg(rv.kmer_off + r + 1);
+            pos = (r ? (I)__ldg(rv.ends + r - 1) : base) - base +
+                  (slot - (I)__ldg(rv.kmer_off + r));
             if (SMALLK) {
               cw.move_to(rv.packed, rv.invalid, pos);
-              last_inv = cw.last_invalid(pos, pos + k - 1);
+              last_inv1 = cw.last_invalid1(pos, pos + k - 1);
             } else {
-              last_inv = last_invalid(rv.invalid, pos, pos + k - 1);
+              last_inv1 = (I)(last_invalid(rv.invalid, pos, pos + k - 1) + 1);
             }
             v = NONE;
             skip_until = 0;
           } else if (slot == r_next) {  // next read
             do {
-              r_next = __ldg(rv.kmer_off + (++r) + 1);
+              r_next = (I)__ldg(rv.kmer_off + (++r) + 1);
             } while (r_next == slot);
-            pos = __ldg(rv.ends + r - 1) - rv.base;
+            pos = (I)__ldg(rv.ends + r - 1) - base;
             if (SMALLK) {
               cw.move_to(rv.packed, rv.invalid, pos);
-              last_inv = cw.last_invalid(pos, pos + k - 1);
+              last_inv1 = cw.last_invalid1(pos, pos + k - 1);
             } else {
-              last_inv = last_invalid(rv.invalid, pos, pos + k - 1);
+              last_inv1 = (I)(last_invalid(rv.invalid, pos, pos + k - 1) + 1);
             }
             v = NONE;
             skip_until = 0;
           }
-          const uint64_t newc = pos + k - 1;
+          const I newc = pos + k - 1;
           if (SMALLK) cw.move_to(rv.packed, rv.invalid, pos);
-          if (SMALLK ? cw.invalid_at(newc) : invalid_at(rv.invalid, newc))
-            last_inv = (int64_t)newc;
+          if (SMALLK ? cw.invalid_at(newc) : invalid_at(rv.invalid, newc)) last_inv1 = newc + 1;
           uint64_t known = 0;
-          if (last_inv >= (int64_t)pos) {
+          if (last_inv1 > pos) {
             known = SBWT_INVALID;
           } else if (slot < skip_until) {
             known = SBWT_NOT_FOUND;
@@ -612,11 +664,12 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
     }
     if (__all_sync(0xFFFFFFFFu, done)) break;
     // ---- phase 2 (converged): the loads ------------------------------------
-    const I ba = NM::block(pa), bb = NM::block(pb);
+    const I ba = block_idx(pa), bb = block_idx(pb);
+    const Block *bc = s.blocks0 + (uint64_t)c * s.block_stride;
     const Block *addrA = nullptr, *addrB = nullptr;
     if (kind == K_BLOCK) {
-      addrA = s.blocks[c] + ba;
-      if (bb != ba) addrB = s.blocks[c] + bb;
+      addrA = bc + ba;
+      if (bb != ba) addrB = bc + bb;
     } else if (kind == K_PRE) {
       addrA = s.wide ? chunk_of(s.presearch, 2 * pre_e) : chunk_of(s.presearch, pre_e);
     } else if (kind == K_SGW) {
@@ -635,8 +688,13 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
     if (done || kind == K_NONE) continue;
     // ---- phase 3: one shared rank computation, then per-mode updates ------
     const uint32_t qa = (uint32_t)(pa - ba * kBlockBits), qb = (uint32_t)(pb - bb * kBlockBits);
-    const I ra = NM::rank(s, c, ba, A, qa);
-    const I rb = NM::rank(s, c, bb, B, qb);
+    I ra = sh_cmap[c] + (I)block_rank(A, qa);
+    I rb = sh_cmap[c] + (I)block_rank(B, qb);
+    if (!NARROW) {
+      const uint64_t *l0c = s.l00 + (uint64_t)c * s.l0_stride;
+      ra += (I)l0c[(uint64_t)ba >> kSuperchunkShift];
+      rb += (I)l0c[(uint64_t)bb >> kSuperchunkShift];
+    }
     const bool bita = block_bit(A, qa);
     I pl = 0, pr = 0;
     if (kind == K_PRE) {
@@ -651,7 +709,7 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
     }
     I emit = 0;
     bool emitted = false;
-    int64_t fail_at = -1;  // char where a search of this k-mer failed
+    I fail_at = NONE;  // char where a search of this k-mer failed
     switch (mode) {
       case M_NEW:
         if (kind == K_BLOCK) {  // stream step from v
@@ -683,7 +741,7 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
         if (l > rr) {
           emit = NONE;
           emitted = true;
-          fail_at = (int64_t)wi - 1;
+          fail_at = wi - 1;
         } else if (wi == pos + k) {
           emit = l;
           emitted = true;
@@ -696,7 +754,7 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
           if (g == v) {  // v starts its group and has no edge c
             emit = NONE;
             emitted = true;
-            fail_at = (int64_t)(pos + k - 1);
+            fail_at = pos + k - 1;
           } else {
             u = g;
             mode = M_GS;
@@ -716,7 +774,7 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
           emit = ra;
         } else {
           emit = NONE;
-          fail_at = (int64_t)(pos + k - 1);
+          fail_at = pos + k - 1;
         }
         break;
       case M_PPRE:
@@ -750,9 +808,9 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
       if (move_to_key && res != SBWT_NOT_FOUND) res = key_walk(s, res, err);
       if (slot < rv.out_capacity) __stcs(rv.out + slot, (unsigned long long)res);
       // a failed search may prove the next k-mers absent: probe x[m..f]
-      if (L && fail_at >= 0 && (uint64_t)fail_at >= pos + L + 1) {
-        const uint64_t m = (uint64_t)fail_at - L + 1;  // > pos + 1
-        probe_end = (uint64_t)fail_at;
+      if (L && fail_at != NONE && fail_at >= pos + L + 1) {
+        const I m = fail_at - L + 1;  // > pos + 1
+        probe_end = fail_at;
         probe_skip = slot + (m - pos) + 1;  // slots of k-mers starting at pos+1..m
         pu = m;
         ubit = min(L, s.p);
@@ -858,7 +916,7 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
     ctr = p.d_counters.get<unsigned long long>();
   }
   const bool small = sv.k <= 33;
-  const bool narrow = sv.num_bits < kNarrowLimit;
+  const bool narrow = sv.num_bits < kNarrowLimit && rv.n_kmers_bound < (1ULL << 32);
 #define SBWT_LAUNCH(S_, C_, K_)                                                          \
   do {                                                                                   \
     if (narrow)                                                                          \
@@ -992,15 +1050,20 @@ IndexImpl::IndexImpl(const u64 *const acgt[4], u64 num_bits_, u32 k_,
   hot.resize(hot_bytes);
   SBWT_CUDA(cudaMemset(hot.get(), 0, hot_bytes));
   unsigned char *hp = hot.get<unsigned char>();
+  const u64 n_l0 = hl0[0].size();
+  l0_all.resize(4 * n_l0 * 8);
   for (int c = 0; c < 4; ++c) {
     SBWT_CUDA(cudaMemcpy(hp + off[c], hb[c].data(), hb[c].size() * sizeof(Block),
                          cudaMemcpyHostToDevice));
-    l0[c].resize(hl0[c].size() * 8);
-    SBWT_CUDA(cudaMemcpy(l0[c].get(), hl0[c].data(), hl0[c].size() * 8,
+    SBWT_CUDA(cudaMemcpy(l0_all.get<u64>() + c * n_l0, hl0[c].data(), n_l0 * 8,
                          cudaMemcpyHostToDevice));
     view.blocks[c] = reinterpret_cast<const Block *>(hp + off[c]);
-    view.l0[c] = l0[c].get<u64>();
+    view.l0[c] = l0_all.get<u64>() + c * n_l0;
   }
+  view.blocks0 = reinterpret_cast<const Block *>(hp);
+  view.block_stride = off[1] / sizeof(Block);
+  view.l00 = l0_all.get<u64>();
+  view.l0_stride = n_l0;
   if (sg) {
     SBWT_CUDA(cudaMemcpy(hp + off[4], sg, nw * 8, cudaMemcpyHostToDevice));
     view.suffix_group_starts = reinterpret_cast<const u64 *>(hp + off[4]);
@@ -1036,8 +1099,7 @@ IndexImpl::IndexImpl(const u64 *const acgt[4], u64 num_bits_, u32 k_,
     SBWT_CUDA(cudaGetLastError());
   }
   SBWT_CUDA(cudaDeviceSynchronize());
-  device_bytes = presearch.size() + hot.size() + key_buf.size();
-  for (int c = 0; c < 4; ++c) device_bytes += l0[c].size();
+  device_bytes = presearch.size() + hot.size() + key_buf.size() + l0_all.size();
 }
 
 SbwtView IndexImpl::view_for(u32 p) const {
@@ -1151,12 +1213,14 @@ static void launch_prepare(int device, u32 k, const char *d_chars, u64 n_chars,
 }
 
 // Tile table + the read search kernel over a prepared batch of n_kmers.
-static void launch_search(const IndexImpl &ix, const u64 *d_ends, u64 n_reads, u64 base,
+static void launch_search(const IndexImpl &ix, u64 n_chars, const u64 *d_ends, u64 n_reads,
+                          u64 base,
                           u64 n_kmers, u64 *d_out, u64 out_capacity, u32 flags,
                           const LaunchConfig &cfg, const ReadsScratch &sc,
                           cudaStream_t st) {
   if (n_reads == 0 || n_kmers == 0) return;
   ReadsView rv{};
+  rv.n_kmers_bound = std::max<u64>(n_chars, n_reads) + 64;
   rv.packed = sc.packed;
   rv.invalid = sc.invalid;
   rv.ends = d_ends;
@@ -1215,6 +1279,7 @@ void enqueue_index_step(const IndexImpl &ix, const char *d_chars, u64 n_chars,
   }
   launch_prepare(ix.device, ix.k, d_chars, n_chars, d_ends, n_reads, 0, sc, st);
   ReadsView rv{};
+  rv.n_kmers_bound = std::max<u64>(n_chars, n_reads) + 64;
   rv.packed = sc.packed;
   rv.invalid = sc.invalid;
   rv.ends = d_ends;
@@ -1293,7 +1358,7 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
       if (n_results) *n_results = n_k;
       if (n_k > capacity)
         throw Error(SBWT_E_CAPACITY, "results_capacity smaller than the k-mer count");
-      launch_search(*this, read_ends, n_reads, 0, n_k, results, capacity, flags, cfg, sc,
+      launch_search(*this, n_chars, read_ends, n_reads, 0, n_k, results, capacity, flags, cfg, sc,
                     user_stream);
       check_err_word(ws, user_stream);
     } else if (n_results) {
@@ -1350,7 +1415,7 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
                               cudaMemcpyHostToDevice, st));
     launch_prepare(device, k, ws.chars[b].get<char>(), nc, ws.ends[b].get<u64>(), nr, ch.c0,
                    sc, st);
-    launch_search(*this, ws.ends[b].get<u64>(), nr, ch.c0, ch.nk, ws.results[b].get<u64>(),
+    launch_search(*this, nc, ws.ends[b].get<u64>(), nr, ch.c0, ch.nk, ws.results[b].get<u64>(),
                   ch.nk, flags, cfg, sc, st);
     if (ch.nk)
       SBWT_CUDA(cudaMemcpyAsync(results + ch.k0, ws.results[b].get(), ch.nk * 8,
@@ -1490,6 +1555,7 @@ void IndexImpl::search_reads_noalloc(const char *d_chars, u64 n_chars, const u64
   LaunchConfig cfg = cfg_in;  // the tile table is sized for tiles of >= 16
   if (cfg.tile && cfg.tile < kNoAllocTileMin) cfg.tile = kNoAllocTileMin;
   ReadsView rv{};
+  rv.n_kmers_bound = std::max<u64>(n_chars, n_reads) + 64;
   rv.packed = sc.packed;
   rv.invalid = sc.invalid;
   rv.ends = d_ends;
@@ -1509,7 +1575,7 @@ void IndexImpl::search_reads_noalloc(const char *d_chars, u64 n_chars, const u64
   const SbwtView sv = view_for(cfg.presearch_letters);
   const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
   const bool stream = !(flags & SBWT_PER_KMER_WALK) && view.suffix_group_starts;
-  const bool narrow = sv.num_bits < kNarrowLimit;
+  const bool narrow = sv.num_bits < kNarrowLimit && rv.n_kmers_bound < (1ULL << 32);
 #define SBWT_NA_LAUNCH(S_, K_)                                                          \
   do {                                                                                  \
     if (narrow)                                                                         \

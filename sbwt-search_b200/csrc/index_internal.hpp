@@ -44,7 +44,7 @@ struct IndexImpl {
   u64 device_bytes = 0;
   SbwtView view{};
   DeviceBuffer hot;  // rank blocks of A/C/G/T + suffix-group words, contiguous
-  DeviceBuffer l0[4], presearch, key_buf;
+  DeviceBuffer l0_all, presearch, key_buf;
   u64 window_bytes = 0;   // L2 access-policy window over `hot`
 };
 

@@ -197,9 +197,9 @@ def bench_colors_and_serving(args, S, torch, dev, tmpdir, rank):
     del d_res, d_found, d_ids, found_mask, res2
     torch.cuda.empty_cache()
     # fused reads -> colors pipeline from host memory (CUDA graph per batch)
-    batch = 1 << 20
+    batch = min(1 << 20, n_reads)
     pipe = S.Pipeline(idx, ci, batch * c["read_len"], batch, tau=c["tau"])
-    nb = min(4, n_reads // batch)
+    nb = max(1, min(4, n_reads // batch))
     pipe.run(chars[:int(ends[batch - 1])], ends[:batch], raw=True)
     t1 = time.perf_counter()
     for b in range(nb):
@@ -213,7 +213,7 @@ def bench_colors_and_serving(args, S, torch, dev, tmpdir, rank):
     srv = S.Server(idx, ci, batch_chars=32 << 20, batch_reads=1 << 18, slots=3, tau=c["tau"])
     rng = np.random.default_rng(11)
     serving = {"offline_reads_per_s": colors["fused_pipeline_reads_per_s"], "loads": []}
-    for offered in (1e5, 1e6, 1e7):
+    for offered in (1e5, 1e6, 1e7, 0.8 * colors["fused_pipeline_reads_per_s"]):
         mean_size = (1e5 - 1) / np.log(1e5)
         rate = offered / mean_size
         pending = []

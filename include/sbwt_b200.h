@@ -169,6 +169,15 @@ int sbwt_colors_open(const char *tcolors_path, int device, sbwt_colors_t **out);
 void sbwt_colors_free(sbwt_colors_t *colors);
 uint64_t sbwt_colors_num_colors(const sbwt_colors_t *colors);
 
+/* Builds (enable != 0) or drops the per-node color set table: 8 bytes per
+ * SBWT node that resolve an index to its color set in one load instead of the
+ * rank over the key k-mer marks, the color set index and the set descriptor
+ * that the reference reads (src/ColorSearcher/ColorSearcher.cuh:68-206).
+ * Results are identical either way.  sbwt_colors_open builds it when it fits
+ * (at most 16 GiB and half the free device memory).  *built (optional)
+ * receives 1 when the table is in use.  No counterpart in the reference. */
+int sbwt_colors_set_node_table(sbwt_colors_t *colors, int enable, int *built);
+
 /* Per-read color counts, the reference's ColorSearcher::search seam
  * (src/ColorSearcher/ColorSearcher.h:43-48, kernels
  * src/ColorSearcher/ColorSearcher.cuh:68-206 and

@@ -183,6 +183,17 @@ uint64_t sbwt_colors_num_colors(const sbwt_colors_t *colors) {
   return colors ? colors->impl->num_colors : 0;
 }
 
+int sbwt_colors_set_node_table(sbwt_colors_t *colors, int enable, int *built) {
+  if (!colors) {
+    set_last_error("null color index");
+    return SBWT_E_INVALID;
+  }
+  return guarded([&] {
+    const bool b = colors->impl->set_node_table(enable != 0);
+    if (built) *built = b ? 1 : 0;
+  });
+}
+
 int sbwt_color_counts(const sbwt_colors_t *colors, const uint64_t *sbwt_idxs,
                       const uint64_t *idx_offsets, uint64_t n_reads, uint32_t *counts,
                       uint32_t flags, void *stream) {

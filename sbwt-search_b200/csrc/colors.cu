@@ -10,12 +10,16 @@
 // holds c.  The reference gets there with one thread per k-mer, a warp-wide
 // loop over the color span and u8 per-(warp, color) partial counts summed by
 // a second kernel into an R x C u64 matrix copied to the host.  Here one warp
-// owns one read: lane i owns colors [64 i, 64 i + 64) (and i + 32, ... for
-// more than 2048 colors) as bit-sliced counters in shared memory (plane j
-// holds bit j of 64 counters), a dense color row is added with a ripple-carry
-// over the planes (no atomics, no conflicts), a sparse list is turned into the
-// same per-lane row words with warp shuffles, and the threshold is a
-// bit-sliced comparison; only the passing color bitmask leaves the kernel.
+// owns one read and one tile of up to 8192 colors (more colors -> more tiles
+// per read): lane i owns colors [64 i, 64 i + 64) (and i + 32, ...) of the
+// tile as bit-sliced counters in shared memory (plane j holds bit j of 64
+// counters), a dense color row is added with a ripple-carry over the planes
+// (no atomics, no conflicts), a sparse list is turned into the same per-lane
+// row words with warp shuffles, the k-mers of a window that share a color set
+// add it once with their multiplicity, and the threshold is a bit-sliced
+// comparison; only the passing color bitmask leaves the kernel.  Each k-mer's
+// set is one 8-byte record load from a per-node table when that table is
+// resident (else rank over the key k-mer marks, color set index, record).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,6 +35,19 @@
 namespace sbwt {
 
 constexpr int kColorWarps = 4;  // warps (reads in flight) per block
+
+// Packed set record: start (42 bits) | len (21 bits) | dense (1 bit).  len is
+// row words for a dense set, ids for a sparse one; start indexes the dense
+// words or the sparse ids.
+constexpr uint64_t kRecNone = ~0ULL;
+constexpr int kRecLenBits = 21;
+__host__ __device__ __forceinline__ uint64_t make_rec(uint64_t start, uint64_t len, bool dense) {
+  return (start << (kRecLenBits + 1)) | (len << 1) | (dense ? 1ULL : 0ULL);
+}
+__device__ __forceinline__ uint64_t rec_start(uint64_t rec) { return rec >> (kRecLenBits + 1); }
+__device__ __forceinline__ uint32_t rec_len(uint64_t rec) {
+  return (uint32_t)(rec >> 1) & ((1u << kRecLenBits) - 1);
+}
 
 struct ColorsJob {
   const uint64_t *vals;     // SBWT indexes (markers allowed when counted)
@@ -52,98 +69,177 @@ __device__ __forceinline__ uint64_t rank_key(const ColorsView &cv, uint64_t i) {
   return cv.key_l0[b >> kSuperchunkShift] + block_rank(B, (uint32_t)(i - b * kBlockBits));
 }
 
-// Adds one row word x (64 colors, one bit each) into the bit-sliced counters
-// planes[j * stride] (j = 0..P-1): ripple carry, stops when the carry dies.
-__device__ __forceinline__ void add_word(uint64_t *planes, uint32_t stride, uint32_t P,
-                                         uint64_t x) {
-  for (uint32_t j = 0; j < P && x; ++j) {
+// The packed set record of SBWT index v < key_bits: the set of key k-mer
+// number rank(key_marks, v), as the reference's ColorSearcher resolves it
+// (rank of v among the key k-mer marks, then color_set_idxs).  kRecNone when
+// the rank is past the last key k-mer.  DIRECT reads the per-node table that
+// holds exactly these values.
+template <bool DIRECT>
+__device__ __forceinline__ uint64_t set_record(const ColorsView &cv, uint64_t v) {
+  if (DIRECT) return __ldg(cv.node_rec + v);
+  const uint64_t j = rank_key(cv, v);
+  if (j >= cv.n_keys) return kRecNone;
+  const uint32_t s = __ldg(cv.csi + j);
+  return s < cv.n_sets ? __ldg(cv.recs + s) : kRecNone;
+}
+
+// node_rec[v] = set_record(v) for every v < key_bits.
+__global__ void node_record_kernel(ColorsView cv, uint64_t *out) {
+  const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < cv.key_bits; v += step)
+    out[v] = set_record<false>(cv, v);
+}
+
+// Adds x << j0 (one bit per color, shifted to plane j0) into the bit-sliced
+// counters planes[j * stride] (j = 0..P-1): ripple carry, stops when the
+// carry dies.  Counts never exceed 2^P - 1 (P covers the longest read), so
+// no carry leaves plane P - 1.
+__device__ __forceinline__ void add_word_at(uint64_t *planes, uint32_t stride, uint32_t j0,
+                                            uint32_t P, uint64_t x) {
+  for (uint32_t j = j0; j < P && x; ++j) {
     const uint64_t p = planes[j * stride];
     planes[j * stride] = p ^ x;
     x &= p;
   }
 }
 
+// Adds m copies of row word x: one ripple per set bit of m.
+__device__ __forceinline__ void add_weighted(uint64_t *planes, uint32_t stride, uint32_t P,
+                                             uint64_t x, uint32_t m) {
+  while (m) {
+    const uint32_t b = __ffs(m) - 1;
+    m &= m - 1;
+    add_word_at(planes, stride, b, P, x);
+  }
+}
+
+constexpr int kRowsInFlight = 4;  // dense rows loaded before the adds
+constexpr int kWindows = 4;       // windows of 32 k-mers whose lookups overlap
+constexpr int kColorBlocksPerSm = 6;
+
+// Adds m copies of the sparse color list sparse[start, start + len) to this
+// warp's counters for the row words [wbase, wbase + 32 * WL).  Warp-uniform.
+__device__ __forceinline__ void add_sparse(const ColorsView &cv, uint64_t *planes,
+                                           uint32_t stride, uint32_t P, uint32_t WL,
+                                           uint32_t wbase, uint32_t lane, uint64_t start,
+                                           uint32_t len, uint32_t m) {
+  const uint32_t span = 32 * WL;
+  for (uint32_t c0 = 0; c0 < len; c0 += 32) {
+    const uint32_t id = (c0 + lane < len) ? __ldg(cv.sparse + start + c0 + lane) : 0xFFFFFFFFu;
+    const uint32_t n = min(32u, len - c0);
+    if (cv.tiles > 1 && cv.sparse_sorted) {  // ascending ids: skip chunks outside the tile
+      if ((__shfl_sync(0xFFFFFFFFu, id, n - 1) >> 6) < wbase) continue;
+      if ((__shfl_sync(0xFFFFFFFFu, id, 0) >> 6) >= wbase + span) break;
+    }
+    uint64_t x[4] = {0, 0, 0, 0};
+    for (uint32_t q = 0; q < n; ++q) {
+      const uint32_t c = __shfl_sync(0xFFFFFFFFu, id, q);
+      const uint32_t local = (c >> 6) - wbase;  // wraps above span when below the tile
+      const uint64_t bit = (local < span && (local & 31) == lane) ? 1ULL << (c & 63) : 0;
+#pragma unroll
+      for (uint32_t w = 0; w < 4; ++w) x[w] |= (local >> 5) == w ? bit : 0;
+    }
+#pragma unroll
+    for (uint32_t w = 0; w < 4; ++w)
+      if (w < WL && x[w]) add_weighted(planes + lane + 32 * w, stride, P, x[w], m);
+  }
+}
+
+// One warp per work item (read r, color tile): tile t covers row words
+// [t * 32 * WL, (t + 1) * 32 * WL), lane i owns words i, i + 32, ... of it.
+// The k-mers are taken 32 * kWindows at a time: every lane issues the set
+// record loads of its kWindows k-mers together, then each window of 32 adds
+// its distinct records once with their multiplicity (__match_any_sync), rows
+// kRowsInFlight at a time.  Counts are sums, so the order and grouping of the
+// adds does not change them.
 // mode 0: pass bitmask + count per read; mode 1: full counts.
-template <int MODE>
-__global__ void __launch_bounds__(32 * kColorWarps) colors_kernel(ColorsView cv,
-                                                                  ColorsJob job,
-                                                                  uint32_t *err) {
+template <int MODE, bool DIRECT>
+__global__ void __launch_bounds__(32 * kColorWarps, kColorBlocksPerSm)
+    colors_kernel(ColorsView cv, ColorsJob job, uint32_t *err) {
+  constexpr uint32_t FULL = 0xFFFFFFFFu;
   extern __shared__ uint64_t smem[];
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const uint32_t WL = cv.words_per_lane, P = job.planes;
+  const uint32_t WL = cv.words_per_lane, P = job.planes, T = cv.tiles;
   // per warp: P planes x (32 * WL) words, plane-major so lanes are contiguous
   const uint32_t stride = 32 * WL;
   uint64_t *planes = smem + (uint64_t)wid * P * stride;
   const uint64_t warps = (uint64_t)gridDim.x * kColorWarps;
-  for (uint64_t r = blockIdx.x * (uint64_t)kColorWarps + wid; r < job.n_reads; r += warps) {
+  const uint64_t n_items = job.n_reads * T;
+  for (uint64_t item = blockIdx.x * (uint64_t)kColorWarps + wid; item < n_items; item += warps) {
+    const uint64_t r = T == 1 ? item : item / T;
+    const uint32_t wbase = (uint32_t)(item - r * T) * stride;
     for (uint32_t q = lane; q < P * stride; q += 32) planes[q] = 0;
     __syncwarp();
     const uint64_t o0 = job.offs[r], o1 = job.offs[r + 1];
     uint32_t found = 0, not_found = 0, invalid = 0;
-    for (uint64_t base = o0; base < o1; base += 32) {
-      // lookup phase: lane t resolves the color set of k-mer base + t
-      const uint64_t t = base + lane;
-      bool have = false;
-      ulonglong2 d = make_ulonglong2(0, 0);
-      if (t < o1) {
-        const uint64_t v = job.vals[t];
-        if (v == SBWT_NOT_FOUND) {
-          ++not_found;
-        } else if (v == SBWT_INVALID) {
-          ++invalid;
-        } else if (v >= cv.key_bits) {
-          atomicOr(err, 1u);
-        } else {
-          ++found;
-          const uint64_t j = rank_key(cv, v);
-          if (j >= cv.n_keys) {
-            atomicOr(err, 1u);
-          } else {
-            const uint32_t s = __ldg(cv.csi + j);
-            if (s >= cv.n_sets) {
-              atomicOr(err, 1u);
-            } else {
-              d = __ldg(cv.desc + s);
-              have = true;
-            }
-          }
-        }
+    for (uint64_t base = o0; base < o1; base += 32 * kWindows) {
+      // lookup phase: lane t classifies k-mers base + 32 l + t (l < kWindows)
+      uint64_t v[kWindows], rec[kWindows];
+      uint32_t cand = 0, bad = 0;
+#pragma unroll
+      for (int l = 0; l < kWindows; ++l) {
+        const uint64_t t = base + 32 * l + lane;
+        const bool in = t < o1;
+        v[l] = in ? job.vals[t] : kRecNone;
+        not_found += in && v[l] == SBWT_NOT_FOUND;
+        invalid += in && v[l] == SBWT_INVALID;
+        if (in && v[l] < SBWT_INVALID && v[l] >= cv.key_bits) bad = 1;
+        if (in && v[l] < cv.key_bits) cand |= 1u << l;
       }
-      // add phase: the warp adds the (up to 32) sets one after the other
-      uint32_t todo = __ballot_sync(0xFFFFFFFFu, have);
-      while (todo) {
-        const int src = __ffs(todo) - 1;
-        todo &= todo - 1;
-        const uint64_t start = __shfl_sync(0xFFFFFFFFu, d.x, src);
-        const uint64_t meta = __shfl_sync(0xFFFFFFFFu, d.y, src);
-        const uint32_t len = (uint32_t)(meta >> 1);
-        if (meta & 1ULL) {  // dense: len = words of the row
+      found += __popc(cand);
+#pragma unroll
+      for (int l = 0; l < kWindows; ++l)
+        rec[l] = (cand >> l) & 1u ? set_record<DIRECT>(cv, v[l]) : kRecNone;
+#pragma unroll
+      for (int l = 0; l < kWindows; ++l)
+        if (((cand >> l) & 1u) && rec[l] == kRecNone) bad = 1;
+      if (bad) atomicOr(err, 1u);
+      // add phase, one window after the other (records rotate into rec[0])
+#pragma unroll 1
+      for (int l = 0; l < kWindows && base + 32 * l < o1; ++l) {
+        const uint64_t r0 = rec[0];
+#pragma unroll
+        for (int q = 0; q + 1 < kWindows; ++q) rec[q] = rec[q + 1];
+        const uint32_t group = __match_any_sync(FULL, r0);
+        const uint32_t weight = __popc(group);
+        uint32_t todo = __ballot_sync(FULL, r0 != kRecNone && __ffs(group) - 1 == (int)lane);
+        while (todo) {
+          uint64_t rr[kRowsInFlight];
+          uint32_t wt[kRowsInFlight];
+#pragma unroll
+          for (int u = 0; u < kRowsInFlight; ++u) {
+            const int src = todo ? __ffs(todo) - 1 : 0;
+            const uint32_t live = todo ? 1u : 0u;
+            todo &= todo - 1;
+            rr[u] = __shfl_sync(FULL, r0, src);
+            wt[u] = live * __shfl_sync(FULL, weight, src);
+          }
           for (uint32_t w = 0; w < WL; ++w) {
-            const uint32_t word = lane + 32 * w;
-            if (word < len) add_word(planes + word, stride, P, __ldg(cv.dense + start + word));
+            const uint32_t local = lane + 32 * w, word = wbase + local;
+            uint64_t x[kRowsInFlight];
+#pragma unroll
+            for (int u = 0; u < kRowsInFlight; ++u)
+              x[u] = (wt[u] && (rr[u] & 1ULL) && word < rec_len(rr[u]))
+                         ? __ldg(cv.dense + rec_start(rr[u]) + word)
+                         : 0;
+#pragma unroll
+            for (int u = 0; u < kRowsInFlight; ++u)
+              if (x[u]) add_weighted(planes + local, stride, P, x[u], wt[u]);
           }
-        } else {  // sparse: len ids, turned into per-lane row words
-          for (uint32_t c0 = 0; c0 < len; c0 += 32) {
-            const uint32_t id = (c0 + lane < len) ? __ldg(cv.sparse + start + c0 + lane) : 0xFFFFFFFFu;
-            const uint32_t m = min(32u, len - c0);
-            uint64_t x[4] = {0, 0, 0, 0};  // up to WL <= 4 words per lane in registers
-            for (uint32_t q = 0; q < m; ++q) {
-              const uint32_t c = __shfl_sync(0xFFFFFFFFu, id, q);
-              const uint32_t word = c >> 6;
-              if ((word & 31) == lane && (word >> 5) < WL) x[(word >> 5) & 3] |= 1ULL << (c & 63);
-            }
-            for (uint32_t w = 0; w < WL && w < 4; ++w)
-              if (x[w]) add_word(planes + lane + 32 * w, stride, P, x[w]);
-          }
+#pragma unroll
+          for (int u = 0; u < kRowsInFlight; ++u)
+            if (wt[u] && !(rr[u] & 1ULL))
+              add_sparse(cv, planes, stride, P, WL, wbase, lane, rec_start(rr[u]),
+                         rec_len(rr[u]), wt[u]);
         }
       }
     }
     __syncwarp();
     // per-read sizes
     for (int o = 16; o; o >>= 1) {
-      found += __shfl_xor_sync(0xFFFFFFFFu, found, o);
-      not_found += __shfl_xor_sync(0xFFFFFFFFu, not_found, o);
-      invalid += __shfl_xor_sync(0xFFFFFFFFu, invalid, o);
+      found += __shfl_xor_sync(FULL, found, o);
+      not_found += __shfl_xor_sync(FULL, not_found, o);
+      invalid += __shfl_xor_sync(FULL, invalid, o);
     }
     if (job.not_found) not_found += (uint32_t)job.not_found[r];
     if (job.invalid) invalid += (uint32_t)job.invalid[r];
@@ -153,12 +249,12 @@ __global__ void __launch_bounds__(32 * kColorWarps) colors_kernel(ColorsView cv,
       const uint64_t minimum = (uint64_t)ceil((double)size * job.tau);
       uint32_t passing = 0;
       for (uint32_t w = 0; w < WL; ++w) {
-        const uint32_t word = lane + 32 * w;
+        const uint32_t local = lane + 32 * w, word = wbase + local;
         uint64_t ge = 0;
         if (minimum > 0 && word < cv.row_words && (P >= 64 || (minimum >> P) == 0)) {
           uint64_t gt = 0, eq = ~0ULL;
           for (int j = (int)P - 1; j >= 0; --j) {
-            const uint64_t pl = planes[(uint32_t)j * stride + word];
+            const uint64_t pl = planes[(uint32_t)j * stride + local];
             if ((minimum >> j) & 1ULL) {
               eq &= pl;
             } else {
@@ -173,18 +269,23 @@ __global__ void __launch_bounds__(32 * kColorWarps) colors_kernel(ColorsView cv,
         if (word < cv.row_words) job.pass_bits[r * cv.row_words + word] = ge;
         passing += __popcll(ge);
       }
-      for (int o = 16; o; o >>= 1) passing += __shfl_xor_sync(0xFFFFFFFFu, passing, o);
-      if (lane == 0) job.pass_count[r] = passing;
+      for (int o = 16; o; o >>= 1) passing += __shfl_xor_sync(FULL, passing, o);
+      if (lane == 0) {
+        if (T == 1)
+          job.pass_count[r] = passing;
+        else
+          atomicAdd(job.pass_count + r, passing);  // zeroed before the launch
+      }
     } else {
       for (uint32_t w = 0; w < WL; ++w) {
-        const uint32_t word = lane + 32 * w;
+        const uint32_t local = lane + 32 * w, word = wbase + local;
         if (word >= cv.row_words) continue;
         for (uint32_t b = 0; b < 64; ++b) {
           const uint32_t c = word * 64 + b;
           if (c >= cv.num_colors) break;
           uint32_t cnt = 0;
           for (uint32_t j = 0; j < P; ++j)
-            cnt |= (uint32_t)((planes[j * stride + word] >> b) & 1ULL) << j;
+            cnt |= (uint32_t)((planes[j * stride + local] >> b) & 1ULL) << j;
           job.counts[r * cv.num_colors + c] = cnt;
         }
       }
@@ -223,39 +324,124 @@ __global__ void emit_ids_kernel(const uint64_t *pass_bits, uint32_t row_words,
   }
 }
 
-// Exclusive scan of u32 counts into u64 offsets (one block; small inputs are
-// the common case, large ones loop).
-__global__ void scan_counts_kernel(const uint32_t *cnt, uint64_t n, uint64_t *off) {
-  __shared__ uint64_t carry;
+// Exclusive scan of u32 counts into u64 offsets off[0..n] in three launches
+// and no scratch: block b of the first launch leaves the total of counts
+// [b * kScanSpan, (b + 1) * kScanSpan) in off[b * kScanSpan], one block
+// scans those totals in place (and writes off[n]), and the last launch
+// replaces every block's range with its offsets.
+constexpr uint32_t kScanThreads = 1024, kScanPer = 4, kScanSpan = kScanThreads * kScanPer;
+
+// Block-wide exclusive scan of one u64 per thread; the block total comes back
+// through *total.  All threads of the block must call it.
+__device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t v, uint64_t *total) {
   __shared__ uint64_t wsum[32];
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (uint64_t b0 = 0; b0 < n; b0 += blockDim.x) {
-    const uint64_t i = b0 + threadIdx.x;
-    uint64_t v = i < n ? cnt[i] : 0, x = v;
+  uint64_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  if (lane == 31) wsum[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    uint64_t s = lane < blockDim.x / 32 ? wsum[lane] : 0;
     for (int o = 1; o < 32; o <<= 1) {
-      uint64_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-      if (lane >= (uint32_t)o) x += y;
+      const uint64_t y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+      if (lane >= (uint32_t)o) s += y;
     }
-    if (lane == 31) wsum[wid] = x;
-    __syncthreads();
-    if (wid == 0) {
-      uint64_t s = lane < blockDim.x / 32 ? wsum[lane] : 0;
-      for (int o = 1; o < 32; o <<= 1) {
-        uint64_t y = __shfl_up_sync(0xFFFFFFFFu, s, o);
-        if (lane >= (uint32_t)o) s += y;
-      }
-      wsum[lane] = s;
-    }
-    __syncthreads();
-    const uint64_t ex = carry + (wid ? wsum[wid - 1] : 0) + x - v;
-    if (i < n) off[i] = ex;
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry = ex + v;
-    __syncthreads();
+    wsum[lane] = s;
+  }
+  __syncthreads();
+  const uint64_t ex = (wid ? wsum[wid - 1] : 0) + x - v;
+  *total = wsum[blockDim.x / 32 - 1];
+  __syncthreads();  // wsum is reused by the next call
+  return ex;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_totals_kernel(const uint32_t *cnt, uint64_t n,
+                                                                   uint64_t *off) {
+  const uint64_t b0 = blockIdx.x * (uint64_t)kScanSpan;
+  uint64_t v = 0;
+  for (uint32_t k = 0; k < kScanPer; ++k) {
+    const uint64_t i = b0 + k * kScanThreads + threadIdx.x;
+    if (i < n) v += cnt[i];
+  }
+  uint64_t total = 0;
+  block_exclusive_scan(v, &total);
+  if (threadIdx.x == 0) off[b0] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_tops_kernel(uint64_t *off, uint64_t n,
+                                                                 uint64_t n_blocks) {
+  uint64_t carry = 0;
+  for (uint64_t b = 0; b < n_blocks; b += kScanThreads) {
+    const uint64_t i = b + threadIdx.x;
+    const uint64_t v = i < n_blocks ? off[i * kScanSpan] : 0;
+    uint64_t total = 0;
+    const uint64_t ex = block_exclusive_scan(v, &total);
+    if (i < n_blocks) off[i * kScanSpan] = carry + ex;
+    carry += total;
   }
   if (threadIdx.x == 0) off[n] = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_write_kernel(const uint32_t *cnt, uint64_t n,
+                                                                  uint64_t *off) {
+  __shared__ uint64_t base;
+  const uint64_t b0 = blockIdx.x * (uint64_t)kScanSpan;
+  if (threadIdx.x == 0) base = off[b0];
+  __syncthreads();
+  const uint64_t i0 = b0 + (uint64_t)threadIdx.x * kScanPer;
+  uint32_t c[kScanPer];
+  uint64_t v = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kScanPer; ++k) {
+    c[k] = i0 + k < n ? cnt[i0 + k] : 0;
+    v += c[k];
+  }
+  uint64_t total = 0;
+  uint64_t at = base + block_exclusive_scan(v, &total);
+#pragma unroll
+  for (uint32_t k = 0; k < kScanPer; ++k) {
+    if (i0 + k < n) off[i0 + k] = at;
+    at += c[k];
+  }
+}
+
+static void enqueue_scan_counts(const uint32_t *d_cnt, uint64_t n, uint64_t *d_off,
+                                cudaStream_t st) {
+  if (n == 0) {
+    SBWT_CUDA(cudaMemsetAsync(d_off, 0, 8, st));
+    return;
+  }
+  const uint64_t nb = (n + kScanSpan - 1) / kScanSpan;
+  scan_totals_kernel<<<(unsigned)nb, kScanThreads, 0, st>>>(d_cnt, n, d_off);
+  scan_tops_kernel<<<1, kScanThreads, 0, st>>>(d_off, n, nb);
+  scan_write_kernel<<<(unsigned)nb, kScanThreads, 0, st>>>(d_cnt, n, d_off);
+  SBWT_CUDA(cudaGetLastError());
+}
+
+// out[0] = max over reads of offs[r + 1] - offs[r]; out[1] = 1 when some
+// offset decreases.  out is zeroed before the launch.
+__global__ void max_span_kernel(const uint64_t *offs, uint64_t n_reads,
+                                unsigned long long *out) {
+  unsigned long long m = 0, bad = 0;
+  const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n_reads; r += step) {
+    const uint64_t a = offs[r], b = offs[r + 1];
+    if (b < a)
+      bad = 1;
+    else
+      m = max(m, (unsigned long long)(b - a));
+  }
+  for (int o = 16; o; o >>= 1) {
+    m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    bad |= __shfl_xor_sync(0xFFFFFFFFu, bad, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (m) atomicMax(out, m);
+    if (bad) atomicOr(out + 1, bad);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -272,8 +458,8 @@ ColorsImpl::ColorsImpl(const TColorsFile &t, int device_) {
     throw Error(SBWT_E_FORMAT, "number of colors out of range");
   const u64 n_sets = t.is_dense_marks.num_bits;
   const u64 n_keys = t.color_set_idxs.size();
-  // per-set descriptors + word-aligned dense rows + u32 sparse ids
-  std::vector<ulonglong2> desc(std::max<u64>(n_sets, 1));
+  // per-set packed records + dense rows (aligned) + u32 sparse ids
+  std::vector<u64> recs(std::max<u64>(n_sets, 1));
   std::vector<u64> dense_words;
   std::vector<uint32_t> sparse(std::max<u64>(t.sparse_arrays.size(), 1));
   for (u64 i = 0; i < t.sparse_arrays.size(); ++i) {
@@ -282,6 +468,7 @@ ColorsImpl::ColorsImpl(const TColorsFile &t, int device_) {
     sparse[i] = (uint32_t)v;
   }
   u64 n_dense = 0, n_sparse = 0;
+  bool sparse_sorted = true;  // every sparse list strictly ascending
   const u64 n_dense_iv = t.dense_arrays_intervals.size();
   const u64 n_sparse_iv = t.sparse_arrays_intervals.size();
   for (u64 s = 0; s < n_sets; ++s) {
@@ -292,11 +479,14 @@ ColorsImpl::ColorsImpl(const TColorsFile &t, int device_) {
       if (en < st || en > t.dense_arrays.num_bits || en - st > num_colors)
         throw Error(SBWT_E_FORMAT, "dense interval out of range");
       const u64 nbits = en - st, nw = (nbits + 63) / 64;
-      const u64 at = dense_words.size();
+      // a row starts on a 64-byte boundary (on its own size when smaller),
+      // so it spans the fewest sectors and DRAM bursts
+      const u64 align = nw >= 8 ? 8 : nw >= 4 ? 4 : nw >= 2 ? 2 : 1;
+      const u64 at = (dense_words.size() + align - 1) / align * align;
       dense_words.resize(at + nw, 0);
       for (u64 c = 0; c < nbits; ++c)
         if (t.dense_arrays.get(st + c)) dense_words[at + c / 64] |= 1ULL << (c % 64);
-      desc[s] = make_ulonglong2(at, (nw << 1) | 1ULL);
+      recs[s] = make_rec(at, nw, true);
       ++n_dense;
     } else {
       if (n_sparse + 1 >= n_sparse_iv) throw Error(SBWT_E_FORMAT, "sparse intervals too short");
@@ -304,11 +494,15 @@ ColorsImpl::ColorsImpl(const TColorsFile &t, int device_) {
       const u64 en = t.sparse_arrays_intervals.get(n_sparse + 1);
       if (en < st || en > t.sparse_arrays.size())
         throw Error(SBWT_E_FORMAT, "sparse interval out of range");
-      desc[s] = make_ulonglong2(st, (en - st) << 1);
+      if (en - st >= (1ULL << kRecLenBits)) throw Error(SBWT_E_FORMAT, "sparse color set too long");
+      for (u64 i = st + 1; i < en && sparse_sorted; ++i) sparse_sorted = sparse[i - 1] < sparse[i];
+      recs[s] = make_rec(st, en - st, false);
       ++n_sparse;
     }
   }
   if (dense_words.empty()) dense_words.push_back(0);
+  if (std::max<u64>(dense_words.size(), t.sparse_arrays.size()) >= (1ULL << (63 - kRecLenBits)))
+    throw Error(SBWT_E_FORMAT, "color arrays too large");
   std::vector<uint32_t> csi(std::max<u64>(n_keys, 1));
   for (u64 j = 0; j < n_keys; ++j) {
     const u64 v = t.color_set_idxs.get(j);
@@ -329,7 +523,7 @@ ColorsImpl::ColorsImpl(const TColorsFile &t, int device_) {
   up(key_blocks, kb.data(), kb.size() * sizeof(Block));
   up(key_l0, kl0.data(), kl0.size() * 8);
   up(csi_buf, csi.data(), csi.size() * 4);
-  up(desc_buf, desc.data(), desc.size() * sizeof(ulonglong2));
+  up(recs_buf, recs.data(), recs.size() * 8);
   up(dense_buf, dense_words.data(), dense_words.size() * 8);
   up(sparse_buf, sparse.data(), sparse.size() * 4);
   view = ColorsView{};
@@ -338,22 +532,52 @@ ColorsImpl::ColorsImpl(const TColorsFile &t, int device_) {
   view.key_bits = t.key_kmer_marks.num_bits;
   view.csi = csi_buf.get<uint32_t>();
   view.n_keys = n_keys;
-  view.desc = desc_buf.get<ulonglong2>();
+  view.recs = recs_buf.get<u64>();
   view.n_sets = n_sets;
   view.dense = dense_buf.get<u64>();
   view.sparse = sparse_buf.get<uint32_t>();
   view.num_colors = (uint32_t)num_colors;
   view.row_words = (uint32_t)((num_colors + 63) / 64);
-  view.words_per_lane = (view.row_words + 31) / 32;
-  if (view.words_per_lane > 4)
-    throw Error(SBWT_E_FORMAT, "more than 8192 colors are not supported");
-  device_bytes = key_blocks.size() + key_l0.size() + csi_buf.size() + desc_buf.size() +
-                 dense_buf.size() + sparse_buf.size();
+  // color tiles of at most 32 lanes x 4 words (8192 colors) per warp
+  view.words_per_lane = std::min<uint32_t>((view.row_words + 31) / 32, 4);
+  view.tiles = (view.row_words + 32 * view.words_per_lane - 1) / (32 * view.words_per_lane);
+  view.sparse_sorted = sparse_sorted ? 1 : 0;
+  set_node_table(true);
+}
+
+u64 ColorsImpl::device_footprint() const {
+  return key_blocks.size() + key_l0.size() + csi_buf.size() + recs_buf.size() +
+         dense_buf.size() + sparse_buf.size() + node_buf.size();
+}
+
+// The per-node record table turns the k-mer -> color set lookup (rank block,
+// color set index, set record: three dependent random loads) into one load.
+// It costs 8 bytes per SBWT node and is only built when that stays within
+// kNodeTableMaxBytes and half of the free device memory.
+bool ColorsImpl::set_node_table(bool enable) {
+  DeviceGuard g(device);
+  view.node_rec = nullptr;
+  node_buf.release();
+  if (enable) {
+    const u64 bytes = std::max<u64>(view.key_bits, 1) * 8;
+    size_t free_b = 0, total_b = 0;
+    SBWT_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    if (bytes <= kNodeTableMaxBytes && bytes <= free_b / 2) {
+      node_buf.resize(bytes);
+      const u64 blocks = std::min<u64>((view.key_bits + 255) / 256, 148 * 16);
+      node_record_kernel<<<(unsigned)std::max<u64>(blocks, 1), 256>>>(view, node_buf.get<u64>());
+      SBWT_CUDA(cudaGetLastError());
+      SBWT_CUDA(cudaDeviceSynchronize());
+      view.node_rec = node_buf.get<u64>();
+    }
+  }
+  device_bytes = device_footprint();
+  return view.node_rec != nullptr;
 }
 
 struct ColorsWorkspace {
   int device = -1;
-  DeviceBuffer vals, offs, nf, inv, pass_bits, pass_count, ids_off, ids, counts, err;
+  DeviceBuffer vals, offs, nf, inv, pass_bits, pass_count, ids_off, ids, counts, err, span;
   cudaStream_t stream = nullptr;
   ~ColorsWorkspace() {
     if (stream) cudaStreamDestroy(stream);
@@ -397,22 +621,26 @@ void ColorsImpl::launch(const u64 *d_vals, const u64 *d_offs, const u64 *d_nf,
   job.include_not_found = (flags & SBWT_INCLUDE_NOT_FOUND) ? 1 : 0;
   job.include_invalid = (flags & SBWT_INCLUDE_INVALID) ? 1 : 0;
   job.planes = planes_for(max_kmers);
+  if (mode == 0 && view.tiles > 1)  // tiles of a read add their passing counts
+    SBWT_CUDA(cudaMemsetAsync(d_pass_count, 0, n_reads * 4, st));
   job.pass_bits = d_pass_bits;
   job.pass_count = d_pass_count;
   job.counts = d_counts;
   const size_t smem = (size_t)kColorWarps * job.planes * 32 * view.words_per_lane * 8;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  const u64 blocks = std::min<u64>((n_reads + kColorWarps - 1) / kColorWarps, (u64)sms * 32);
-  if (mode == 0) {
-    SBWT_CUDA(cudaFuncSetAttribute(colors_kernel<0>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    colors_kernel<0><<<(unsigned)blocks, 32 * kColorWarps, smem, st>>>(view, job, d_err);
-  } else {
-    SBWT_CUDA(cudaFuncSetAttribute(colors_kernel<1>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    colors_kernel<1><<<(unsigned)blocks, 32 * kColorWarps, smem, st>>>(view, job, d_err);
-  }
+  const u64 items = n_reads * view.tiles;
+  const u64 blocks = std::min<u64>((items + kColorWarps - 1) / kColorWarps, (u64)sms * 32);
+  const bool direct = view.node_rec != nullptr;
+  auto go = [&](auto kernel) {
+    SBWT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    kernel<<<(unsigned)blocks, 32 * kColorWarps, smem, st>>>(view, job, d_err);
+  };
+  if (mode == 0)
+    direct ? go(colors_kernel<0, true>) : go(colors_kernel<0, false>);
+  else
+    direct ? go(colors_kernel<1, true>) : go(colors_kernel<1, false>);
   SBWT_CUDA(cudaGetLastError());
 }
 
@@ -432,7 +660,7 @@ void ColorsImpl::enqueue_pseudoalign(const u64 *d_vals, const u64 *d_offs, u64 n
   }
   launch(d_vals, d_offs, nullptr, nullptr, n_reads, max_kmers, tau, flags, 0, d_pass_bits,
          d_pass_count, nullptr, d_err, st);
-  scan_counts_kernel<<<1, 1024, 0, st>>>(d_pass_count, n_reads, d_ids_off);
+  enqueue_scan_counts(d_pass_count, n_reads, d_ids_off, st);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   const u64 blocks = std::min<u64>((n_reads + 7) / 8, (u64)sms * 16);
@@ -444,10 +672,10 @@ void ColorsImpl::enqueue_pseudoalign(const u64 *d_vals, const u64 *d_offs, u64 n
 void ColorsImpl::prepare_launch(u64 max_kmers) const {
   const uint32_t P = planes_for(max_kmers);
   const size_t smem = (size_t)kColorWarps * P * 32 * view.words_per_lane * 8;
-  SBWT_CUDA(cudaFuncSetAttribute(colors_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
-  SBWT_CUDA(cudaFuncSetAttribute(colors_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
+  for (auto kernel : {colors_kernel<0, true>, colors_kernel<0, false>, colors_kernel<1, true>,
+                      colors_kernel<1, false>})
+    SBWT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
 }
 
 static u64 max_span(const u64 *offs, u64 n_reads) {
@@ -457,6 +685,22 @@ static u64 max_span(const u64 *offs, u64 n_reads) {
     m = std::max(m, offs[r + 1] - offs[r]);
   }
   return m;
+}
+
+// Longest read of device-resident offsets (one small reduction, 16 bytes back).
+static u64 device_max_span(ColorsWorkspace &ws, const u64 *d_offs, u64 n_reads,
+                           cudaStream_t st) {
+  ws.span.ensure(16);
+  SBWT_CUDA(cudaMemsetAsync(ws.span.get(), 0, 16, st));
+  const u64 blocks = std::min<u64>((n_reads + 255) / 256, 148 * 8);
+  max_span_kernel<<<(unsigned)std::max<u64>(blocks, 1), 256, 0, st>>>(
+      d_offs, n_reads, ws.span.get<unsigned long long>());
+  SBWT_CUDA(cudaGetLastError());
+  unsigned long long h[2] = {0, 0};
+  SBWT_CUDA(cudaMemcpyAsync(h, ws.span.get(), 16, cudaMemcpyDeviceToHost, st));
+  SBWT_CUDA(cudaStreamSynchronize(st));
+  if (h[1]) throw Error(SBWT_E_INVALID, "offsets must be non-decreasing");
+  return h[0];
 }
 
 static void check_colors_err(ColorsWorkspace &ws, cudaStream_t st) {
@@ -475,11 +719,8 @@ void ColorsImpl::counts(const u64 *vals, const u64 *offs, u64 n_reads, uint32_t 
   ColorsWorkspace &ws = colors_workspace(device);
   if (n_reads == 0) return;
   if (flags & SBWT_DEVICE_POINTERS) {
-    std::vector<u64> h(n_reads + 1);
-    SBWT_CUDA(cudaMemcpyAsync(h.data(), offs, (n_reads + 1) * 8, cudaMemcpyDeviceToHost,
-                              user_stream));
-    SBWT_CUDA(cudaStreamSynchronize(user_stream));
-    launch(vals, offs, nullptr, nullptr, n_reads, max_span(h.data(), n_reads), 0.0, 0, 1,
+    launch(vals, offs, nullptr, nullptr, n_reads, device_max_span(ws, offs, n_reads, user_stream),
+           0.0, 0, 1,
            nullptr, nullptr, out, ws.err.get<uint32_t>(), user_stream);
     check_colors_err(ws, user_stream);
     return;
@@ -525,10 +766,7 @@ void ColorsImpl::pseudoalign(const u64 *vals, const u64 *offs, const u64 *nf,
   const u64 *d_vals = vals, *d_offs = offs, *d_nf = nf, *d_inv = inv;
   u64 mk = 0;
   if (dev) {
-    std::vector<u64> h(n_reads + 1);
-    SBWT_CUDA(cudaMemcpyAsync(h.data(), offs, (n_reads + 1) * 8, cudaMemcpyDeviceToHost, st));
-    SBWT_CUDA(cudaStreamSynchronize(st));
-    mk = max_span(h.data(), n_reads);
+    mk = device_max_span(ws, offs, n_reads, st);
   } else {
     mk = max_span(offs, n_reads);
     const u64 n_vals = offs[n_reads] - offs[0];
@@ -563,8 +801,7 @@ void ColorsImpl::pseudoalign(const u64 *vals, const u64 *offs, const u64 *nf,
   launch(d_vals, d_offs, d_nf, d_inv, n_reads, mk, tau, flags, 0, ws.pass_bits.get<u64>(),
          ws.pass_count.get<uint32_t>(), nullptr, ws.err.get<uint32_t>(), st);
   u64 *d_ids_off = dev ? ids_offsets : ws.ids_off.get<u64>();
-  scan_counts_kernel<<<1, 1024, 0, st>>>(ws.pass_count.get<uint32_t>(), n_reads, d_ids_off);
-  SBWT_CUDA(cudaGetLastError());
+  enqueue_scan_counts(ws.pass_count.get<uint32_t>(), n_reads, d_ids_off, st);
   u64 total = 0;
   SBWT_CUDA(cudaMemcpyAsync(&total, d_ids_off + n_reads, 8, cudaMemcpyDeviceToHost, st));
   check_colors_err(ws, st);

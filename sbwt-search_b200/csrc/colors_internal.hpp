@@ -9,6 +9,8 @@
 
 namespace sbwt {
 
+constexpr u64 kNodeTableMaxBytes = 16ULL << 30;  // per-node record table cap
+
 // Device view of the color index.
 struct ColorsView {
   const Block *key_blocks;  // rank blocks of the key k-mer marks
@@ -16,13 +18,16 @@ struct ColorsView {
   uint64_t key_bits;
   const uint32_t *csi;      // color set id per key k-mer
   uint64_t n_keys;
-  const ulonglong2 *desc;   // per set: x = start, y = (len << 1) | dense
+  const uint64_t *recs;     // per set: start << 22 | len << 1 | dense
   uint64_t n_sets;
+  const uint64_t *node_rec; // per SBWT node: the record of its color set, or nullptr
   const uint64_t *dense;    // word-aligned dense rows
   const uint32_t *sparse;   // sparse color ids
   uint32_t num_colors;
   uint32_t row_words;       // ceil(num_colors / 64)
-  uint32_t words_per_lane;  // ceil(row_words / 32)
+  uint32_t words_per_lane;  // row words per lane in one color tile (<= 4)
+  uint32_t tiles;           // color tiles per read: ceil(row_words / (32 * words_per_lane))
+  uint32_t sparse_sorted;   // 1 when every sparse list is strictly ascending
 };
 
 struct ColorsImpl {
@@ -46,11 +51,14 @@ struct ColorsImpl {
   // sets the shared-memory attribute for batches of up to max_kmers k-mers per
   // read (must precede a stream capture)
   void prepare_launch(u64 max_kmers) const;
+  // builds (or drops) the per-node set record table; false when not built
+  bool set_node_table(bool enable);
+  u64 device_footprint() const;
 
   int device = 0;
   u64 num_colors = 0;
   u64 device_bytes = 0;
-  DeviceBuffer key_blocks, key_l0, csi_buf, desc_buf, dense_buf, sparse_buf;
+  DeviceBuffer key_blocks, key_l0, csi_buf, recs_buf, dense_buf, sparse_buf, node_buf;
   ColorsView view{};
 };
 

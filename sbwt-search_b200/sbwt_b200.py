@@ -85,6 +85,7 @@ def lib():
             L.sbwt_color_counts.argtypes = [vp, vp, vp, u64, vp, u32, vp]
             L.sbwt_pseudoalign.argtypes = [vp, vp, vp, vp, vp, u64, C.c_double, u32,
                                            vp, u64, vp, vp]
+            L.sbwt_colors_set_node_table.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.sbwt_pipeline_create.argtypes = [vp, vp, u64, u64, u32, C.c_double,
                                            C.POINTER(vp)]
         L.sbwt_pipeline_free.argtypes = [vp]
@@ -271,6 +272,13 @@ class ColorIndex:
             self.close()
         except Exception:
             pass
+
+    def set_node_table(self, enable: bool) -> bool:
+        """Builds or drops the per-node color set table (same results either
+        way); returns whether the table is in use."""
+        built = C.c_int(0)
+        check(lib().sbwt_colors_set_node_table(self._h, int(enable), C.byref(built)))
+        return bool(built.value)
 
     def counts(self, sbwt_idxs: np.ndarray, idx_offsets: np.ndarray) -> np.ndarray:
         sbwt_idxs = np.ascontiguousarray(sbwt_idxs, dtype=np.uint64)

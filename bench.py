@@ -619,7 +619,7 @@ def main():
     try:
         rs_peak = random_sector_peak(S, dev, idx.device_bytes)
     except Exception:  # reported as unmeasured, never hides the headline
-        rs_peak = float("nan")
+        rs_peak = None
 
     extra = {}
     if not args.index_only and rank == 0:  # per-GPU sections: rank 0 only
@@ -675,8 +675,8 @@ def main():
                               "suffix_group_words": n_sg, "probe_iterations": n_probe,
                               "bytes_per_kmer": alg_bytes / n_kmers},
                      "random_sector": {"achieved_gsectors_s": rs_achieved / 1e9,
-                                       "peak_gsectors_s": rs_peak / 1e9,
-                                       "frac": rs_achieved / rs_peak,
+                                       "peak_gsectors_s": rs_peak and rs_peak / 1e9,
+                                       "frac": rs_peak and rs_achieved / rs_peak,
                                        "working_set_bytes": int(idx.device_bytes),
                                        "peak_source": "sbwt_measure_random_sectors over a "
                                                       "buffer of the index's device size, "

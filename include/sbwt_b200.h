@@ -270,6 +270,20 @@ int sbwt_server_stats(sbwt_server_t *s, double *p50_s, double *p99_s,
 int sbwt_fastx_read(const char *path, char **chars, uint64_t *n_chars,
                     uint64_t **read_ends, uint64_t *n_reads);
 void sbwt_free(void *p);
+/* Parses FASTA/FASTQ text (uncompressed, the bytes of a whole file) on
+ * `device` with the same record rules as sbwt_fastx_read (kseq's, as the
+ * reference uses them: src/SequenceFileParser/ContinuousSequenceFileParser.cpp
+ * :148-156; the reference parses on the host).  Writes the sequence chars of
+ * every record back to back into `chars` and each record's end offset into
+ * `read_ends`; *n_chars / *n_reads receive the totals, also when the
+ * capacities are too small (SBWT_E_CAPACITY; nothing written).  flags:
+ * SBWT_DEVICE_POINTERS when text / chars / read_ends are device memory (then
+ * `stream` orders the work; the call still returns after it ends), else host
+ * memory.  The chars need no more than n_bytes. */
+int sbwt_fastx_parse(const char *text, uint64_t n_bytes, char *chars,
+                     uint64_t chars_capacity, uint64_t *read_ends,
+                     uint64_t ends_capacity, uint64_t *n_chars, uint64_t *n_reads,
+                     uint32_t flags, int device, void *stream);
 /* Writes index results as the reference's printers do
  * (src/IndexResultsPrinter/ printers: format 0 ascii .txt, 1 binary .bin, 2 bool
  * .bool; optional length-prefixed format/version header). */

@@ -104,6 +104,8 @@ def lib():
                                         C.POINTER(u64), C.POINTER(u64), C.POINTER(u64),
                                         C.POINTER(C.c_double), C.c_int]
         L.sbwt_free.argtypes = [vp]
+        L.sbwt_fastx_parse.argtypes = [vp, u64, vp, u64, vp, u64, C.POINTER(u64),
+                                       C.POINTER(u64), u32, C.c_int, vp]
         L.sbwt_free.restype = None
         L.sbwt_autotune.argtypes = [vp, vp, u64, vp, u64, u64, C.POINTER(u32),
                                     C.POINTER(u32), C.POINTER(u64), C.POINTER(C.c_double)]
@@ -482,3 +484,22 @@ def autotune(index: SbwtIndex, d_chars, d_read_ends, sample_chars: int = 256 << 
         AUTOTUNE_CACHE.parent.mkdir(parents=True, exist_ok=True)
         AUTOTUNE_CACHE.write_text(json.dumps(cache, indent=1))
     return dict(c, cached=False)
+
+
+def fastx_parse(text, device: int = 0):
+    """FASTA/FASTQ text (bytes or np.uint8) parsed on the GPU: returns
+    (chars np.uint8, read_ends np.uint64), the same as fastx_read on a file."""
+    text = _np_chars(text)
+    n = len(text)
+    nc, nr = C.c_uint64(), C.c_uint64()
+    chars = np.zeros(max(n, 1), dtype=np.uint8)
+    rc = lib().sbwt_fastx_parse(_ptr(text) if n else None, n, _ptr(chars), n, None, 0,
+                                C.byref(nc), C.byref(nr), 0, device, None)
+    if rc == E_CAPACITY:
+        ends = np.zeros(max(nr.value, 1), dtype=np.uint64)
+        rc = lib().sbwt_fastx_parse(_ptr(text) if n else None, n, _ptr(chars), n, _ptr(ends),
+                                    len(ends), C.byref(nc), C.byref(nr), 0, device, None)
+    else:
+        ends = np.zeros(1, dtype=np.uint64)
+    check(rc)
+    return chars[:nc.value], ends[:nr.value]

@@ -92,3 +92,68 @@ def key_marks_for(index, d: int, seed: int = 0) -> np.ndarray:
     words = np.packbits(key.astype(np.uint8), bitorder="little")
     words = np.concatenate([words, np.zeros((-len(words)) % 8, np.uint8)])
     return words.view(np.uint64)
+
+
+def random_fastx(seed: int, n_records: int, fastq_frac: float = 0.5, max_line: int = 80,
+                 junk: bool = True, final_newline: bool = True) -> bytes:
+    """Seeded FASTA/FASTQ text that exercises the record rules: CRLF and LF
+    line ends, blank lines, empty records, multi-line sequences and qualities,
+    quality lines starting with '@', '>' or '+', zero-length FASTQ sequences,
+    leading junk lines and (optionally) no final newline."""
+    rng = np.random.default_rng(seed)
+    alphabet = np.frombuffer(b"ACGTACGTACGTacgtN", dtype=np.uint8)
+    qual = np.frombuffer(b"IIII#@>+!5", dtype=np.uint8)
+    lines: list[bytes] = []
+    if junk:
+        for _ in range(int(rng.integers(0, 4))):
+            lines.append(bytes(rng.choice(alphabet, int(rng.integers(0, 20)))))
+        if rng.random() < 0.5:
+            lines.append(b"+junk")
+    for r in range(n_records):
+        n = int(rng.integers(0, 400)) if rng.random() < 0.9 else 0
+        seq = bytes(rng.choice(alphabet, n))
+        width = int(rng.integers(1, max_line + 1)) if rng.random() < 0.6 else max(n, 1)
+        seq_lines = [seq[i:i + width] for i in range(0, n, width)] or ([] if rng.random() < 0.5
+                                                                       else [b""])
+        if rng.random() < 0.1:
+            seq_lines.insert(int(rng.integers(0, len(seq_lines) + 1)), b"")
+        if rng.random() < fastq_frac:
+            lines.append(b"@r%d" % r)
+            lines += seq_lines
+            lines.append(b"+" if rng.random() < 0.7 else b"+r%d" % r)
+            q = bytes(rng.choice(qual, n))
+            if n and rng.random() < 0.3:
+                q = bytes([int(rng.choice(np.frombuffer(b"@>+", np.uint8)))]) + q[1:]
+            qw = int(rng.integers(1, max_line + 1)) if rng.random() < 0.4 else max(n, 1)
+            lines += [q[i:i + qw] for i in range(0, n, qw)]
+        else:
+            lines.append(b">r%d some description" % r)
+            lines += seq_lines
+    out = bytearray()
+    for i, ln in enumerate(lines):
+        out += ln
+        out += b"\r\n" if rng.random() < 0.2 else b"\n"
+    if not final_newline and out.endswith(b"\n"):
+        out = out[:-2] if out.endswith(b"\r\n") else out[:-1]
+    return bytes(out)
+
+
+def host_fastx(text: bytes, path) -> tuple[bytes, np.ndarray]:
+    """The host reader (sbwt_fastx_read) on `text` written to `path`."""
+    import ctypes as C
+    import sbwt_b200 as S
+    Path(path).write_bytes(text)
+    L = S.lib()
+    L.sbwt_fastx_read.argtypes = [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]
+    L.sbwt_free.argtypes = [C.c_void_p]
+    ch, en = C.c_void_p(), C.c_void_p()
+    nc, nr = C.c_uint64(), C.c_uint64()
+    S.check(L.sbwt_fastx_read(str(path).encode(), C.byref(ch), C.byref(nc), C.byref(en),
+                              C.byref(nr)))
+    chars = C.string_at(ch, nc.value) if nc.value else b""
+    ends = np.ctypeslib.as_array(C.cast(en, C.POINTER(C.c_uint64)),
+                                 (max(nr.value, 1),))[:nr.value].copy()
+    L.sbwt_free(ch)
+    L.sbwt_free(en)
+    return chars, ends

@@ -131,3 +131,13 @@ def test_color_writers():
             assert vals == [0, 2, O.NOT_FOUND, O.NOT_FOUND, 1, O.NOT_FOUND]
         else:
             assert b == b"1,2,3\n1,0,1\n0,0,0\n0,1,0\n"
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_fastx_reader_matches_oracle_on_random_text(seed, tmp_path):
+    from helpers import host_fastx, random_fastx
+    text = random_fastx(seed, 300, final_newline=seed % 2 == 0)
+    chars, ends = host_fastx(text, tmp_path / "r.fx")
+    reads = O.parse_fastx(text)
+    assert chars == b"".join(reads)
+    assert ends.tolist() == np.cumsum([len(r) for r in reads]).tolist()

@@ -284,6 +284,27 @@ int sbwt_fastx_parse(const char *text, uint64_t n_bytes, char *chars,
                      uint64_t chars_capacity, uint64_t *read_ends,
                      uint64_t ends_capacity, uint64_t *n_chars, uint64_t *n_reads,
                      uint32_t flags, int device, void *stream);
+/* Formats index results on `device` into the bytes the reference's printers
+ * write for one batch, without the file header: format 0 ascii, 1 binary,
+ * 2 bool (src/IndexResultsPrinter/AsciiContinuousIndexResultsPrinter.cpp
+ * :50-55 and its binary / bool siblings; the reference formats on the host).
+ * results: one u64 per k-mer (SBWT_NOT_FOUND / SBWT_INVALID markers) in read
+ * order; read_ends: cumulative read lengths (k-mers per read = len - k + 1).
+ * *out_bytes receives the size, also on SBWT_E_CAPACITY.  flags:
+ * SBWT_DEVICE_POINTERS for device buffers (a binary `out` 8-byte aligned). */
+int sbwt_format_index_results(const uint64_t *results, const uint64_t *read_ends,
+                              uint64_t n_reads, uint32_t k, int format, char *out,
+                              uint64_t out_capacity, uint64_t *out_bytes,
+                              uint32_t flags, int device, void *stream);
+/* Formats pseudoalignment results (ids + ids_offsets as sbwt_pseudoalign
+ * writes them, offsets starting at 0) on `device`: format 0 ascii, 1 binary,
+ * 2 csv rows of num_colors (src/ColorResultsPrinter/
+ * AsciiContinuousColorResultsPrinter.cpp:74-79 and its binary / csv siblings;
+ * no header or csv title row).  Same conventions as above. */
+int sbwt_format_color_results(const uint32_t *ids, const uint64_t *ids_offsets,
+                              uint64_t n_reads, uint64_t num_colors, int format,
+                              char *out, uint64_t out_capacity, uint64_t *out_bytes,
+                              uint32_t flags, int device, void *stream);
 /* Writes index results as the reference's printers do
  * (src/IndexResultsPrinter/ printers: format 0 ascii .txt, 1 binary .bin, 2 bool
  * .bool; optional length-prefixed format/version header). */

@@ -12,6 +12,13 @@
 // (src/ArgumentParser/ArgumentParser.cpp:20-22); an unreadable input file is
 // reported and skipped (src/SequenceFileParser/
 // ContinuousSequenceFileParser.cpp:114-133).
+//
+// A query file whose text fits the device (with its results) is handled on
+// the GPU end to end: its bytes are copied once, parsed, searched and
+// formatted there, and only the formatted output comes back.  Larger files
+// stream through the host reader in batches of 256 M chars.
+#include <cuda_runtime.h>
+
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -111,6 +118,77 @@ void check(int rc) {
   if (rc != SBWT_OK) throw std::runtime_error(sbwt_last_error());
 }
 
+void check_cuda(cudaError_t e) {
+  if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
+}
+
+// Device / pinned host memory owned by the command line tool.
+struct DevMem {
+  void *p = nullptr;
+  explicit DevMem(size_t n) { check_cuda(cudaMalloc(&p, n ? n : 1)); }
+  ~DevMem() { cudaFree(p); }
+  template <class T>
+  T *get() const {
+    return static_cast<T *>(p);
+  }
+};
+struct HostMem {
+  void *p = nullptr;
+  explicit HostMem(size_t n) { check_cuda(cudaMallocHost(&p, n ? n : 1)); }
+  ~HostMem() { cudaFreeHost(p); }
+};
+
+struct Stream {
+  cudaStream_t s = nullptr;
+  Stream() { check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+  ~Stream() { cudaStreamDestroy(s); }
+};
+
+// Largest query text handled on the device in one piece: text, chars, read
+// ends, one u64 result and up to 22 formatted bytes per char stay within 80 %
+// of the free device memory.
+u64 device_text_budget(int device) {
+  size_t free_b = 0, total_b = 0;
+  check_cuda(cudaSetDevice(device));
+  check_cuda(cudaMemGetInfo(&free_b, &total_b));
+  return (u64)(0.8 * (double)free_b / 40.0);
+}
+
+// One whole query text through the GPU: parse, search, format; the formatted
+// bytes are appended to w.
+void index_text_on_device(sbwt_index_t *ix, const sbwt_index_info_t &info, uint32_t flags,
+                          const std::vector<char> &text, int format, IndexResultsWriter &w) {
+  const u64 n = text.size();
+  if (n == 0) return;
+  Stream st;
+  const uint32_t dp = SBWT_DEVICE_POINTERS;
+  DevMem d_text(n), d_chars(n);
+  check_cuda(cudaMemcpyAsync(d_text.p, text.data(), n, cudaMemcpyHostToDevice, st.s));
+  u64 nc = 0, nr = 0;
+  int rc = sbwt_fastx_parse(d_text.get<char>(), n, d_chars.get<char>(), n, nullptr, 0, &nc,
+                            &nr, dp, info.device, st.s);
+  if (rc != SBWT_E_CAPACITY) check(rc);
+  if (nr == 0) return;
+  DevMem d_ends(nr * 8);
+  check(sbwt_fastx_parse(d_text.get<char>(), n, d_chars.get<char>(), n, d_ends.get<u64>(), nr,
+                         &nc, &nr, dp, info.device, st.s));
+  DevMem d_res(std::max<u64>(nc, 1) * 8);
+  u64 nk = 0;
+  check(sbwt_search_reads(ix, d_chars.get<char>(), nc, d_ends.get<u64>(), nr, d_res.get<u64>(),
+                          std::max<u64>(nc, 1), &nk, flags | dp, st.s));
+  u64 nb = 0;
+  rc = sbwt_format_index_results(d_res.get<u64>(), d_ends.get<u64>(), nr, info.k, format,
+                                 nullptr, 0, &nb, dp, info.device, st.s);
+  if (rc != SBWT_E_CAPACITY) check(rc);
+  DevMem d_out(nb);
+  check(sbwt_format_index_results(d_res.get<u64>(), d_ends.get<u64>(), nr, info.k, format,
+                                  d_out.get<char>(), nb, &nb, dp, info.device, st.s));
+  HostMem h_out(nb);
+  check_cuda(cudaMemcpyAsync(h_out.p, d_out.p, nb, cudaMemcpyDeviceToHost, st.s));
+  check_cuda(cudaStreamSynchronize(st.s));
+  w.write_raw(static_cast<const char *>(h_out.p), nb);
+}
+
 int run_index(const Args &a) {
   if (a.flags.count("help")) {
     std::printf("%s", kIndexHelp);
@@ -136,15 +214,25 @@ int run_index(const Args &a) {
   if (ins.size() != outs.size())
     throw std::runtime_error("query and output lists differ in length");
   const u64 batch_chars = 256ULL << 20;
+  const int format = fmt == IndexFormat::Ascii ? 0 : fmt == IndexFormat::Binary ? 1 : 2;
+  const u64 budget = device_text_budget(info.device);
   std::vector<u64> results;
+  std::vector<char> text;
   for (size_t f = 0; f < ins.size(); ++f) {
-    std::unique_ptr<FastxReader> rd;
+    bool whole = false;
     try {
-      rd = std::make_unique<FastxReader>(ins[f]);
+      whole = read_whole_file(ins[f], budget, text);
     } catch (const std::exception &e) {
       std::fprintf(stderr, "[error] %s\n", e.what());
       continue;
     }
+    if (whole) {
+      IndexResultsWriter w(outs[f], fmt, headers);
+      index_text_on_device(ix, info, flags, text, format, w);
+      continue;
+    }
+    text = std::vector<char>();
+    std::unique_ptr<FastxReader> rd = std::make_unique<FastxReader>(ins[f]);
     IndexResultsWriter w(outs[f], fmt, headers);
     ReadBatch b;
     while (true) {
@@ -208,7 +296,16 @@ int run_colors(const Args &a) {
     }
     check(rc);
     ColorResultsWriter w(outs[f], fmt, headers, C);
-    w.write(ids.data(), offs.data(), n);
+    // ids formatted on the GPU (the same bytes as the host writer)
+    const int format = fmt == ColorFormat::Ascii ? 0 : fmt == ColorFormat::Binary ? 1 : 2;
+    u64 nb = 0;
+    rc = sbwt_format_color_results(ids.data(), offs.data(), n, C, format, nullptr, 0, &nb, 0, 0,
+                                   nullptr);
+    if (rc != SBWT_E_CAPACITY) check(rc);
+    std::vector<char> bytes(std::max<u64>(nb, 1));
+    check(sbwt_format_color_results(ids.data(), offs.data(), n, C, format, bytes.data(), nb, &nb,
+                                    0, 0, nullptr));
+    w.write_raw(bytes.data(), nb);
   }
   sbwt_colors_free(ci);
   return 0;

@@ -86,6 +86,31 @@ bool FastxReader::next_batch(ReadBatch &b, u64 max_chars, u64 max_reads) {
   return true;
 }
 
+bool read_whole_file(const std::string &path, u64 max_bytes, std::vector<char> &out) {
+  gzFile f = gzopen(path.c_str(), "rb");
+  if (!f) throw std::runtime_error("Unable to open file " + path);
+  gzbuffer(f, 1 << 20);
+  out.clear();
+  const size_t step = 64 << 20;
+  while (true) {
+    const size_t at = out.size();
+    if (at > max_bytes) {
+      gzclose(f);
+      return false;
+    }
+    out.resize(at + step);
+    const int n = gzread(f, out.data() + at, (unsigned)step);
+    if (n < 0) {
+      gzclose(f);
+      throw std::runtime_error("read error in sequence file");
+    }
+    out.resize(at + (size_t)n);
+    if (n == 0) break;
+  }
+  gzclose(f);
+  return out.size() <= max_bytes;
+}
+
 std::vector<std::string> expand_list(const std::string &name) {
   const std::string ext = ".list";
   if (name.size() >= ext.size() && name.compare(name.size() - ext.size(), ext.size(), ext) == 0) {

@@ -65,6 +65,8 @@ class IndexResultsWriter {
   // results: one u64 per k-mer of every read (SBWT_NOT_FOUND / SBWT_INVALID
   // markers), read_ends as passed to the search; k gives k-mers per read.
   void write(const u64 *results, const u64 *read_ends, u64 n_reads, u32 k);
+  // Appends bytes that are already in this format (formatted on the GPU).
+  void write_raw(const char *bytes, u64 n);
 
  private:
   FILE *f_ = nullptr;
@@ -82,6 +84,7 @@ class ColorResultsWriter {
                      u64 num_colors);
   ~ColorResultsWriter();
   void write(const uint32_t *ids, const u64 *ids_offsets, u64 n_reads);
+  void write_raw(const char *bytes, u64 n);
 
  private:
   FILE *f_ = nullptr;
@@ -100,6 +103,10 @@ struct IndexResults {
   std::vector<u64> not_found, invalid;
 };
 IndexResults read_index_results(const std::string &path);
+
+// The whole (gzip-transparent) file, or false when it holds more than
+// max_bytes bytes.
+bool read_whole_file(const std::string &path, u64 max_bytes, std::vector<char> &out);
 
 // `.list` handling (src/FilenamesParser/FilenamesParser.cpp:19-46): a name
 // ending in ".list" is a file with one name per line.

@@ -100,6 +100,11 @@ void IndexResultsWriter::write(const u64 *res, const u64 *ends, u64 n_reads, u32
   flush_buf(f_, buf_);
 }
 
+void IndexResultsWriter::write_raw(const char *bytes, u64 n) {
+  flush_buf(f_, buf_);
+  if (n && std::fwrite(bytes, 1, n, f_) != n) throw std::runtime_error("write failed");
+}
+
 ColorResultsWriter::ColorResultsWriter(const std::string &prefix, ColorFormat fmt,
                                        bool headers, u64 num_colors)
     : fmt_(fmt), num_colors_(num_colors) {
@@ -156,6 +161,11 @@ void ColorResultsWriter::write(const uint32_t *ids, const u64 *offs, u64 n_reads
     if (buf_.size() > (1u << 22)) flush_buf(f_, buf_);
   }
   flush_buf(f_, buf_);
+}
+
+void ColorResultsWriter::write_raw(const char *bytes, u64 n) {
+  flush_buf(f_, buf_);
+  if (n && std::fwrite(bytes, 1, n, f_) != n) throw std::runtime_error("write failed");
 }
 
 IndexResults read_index_results(const std::string &path) {

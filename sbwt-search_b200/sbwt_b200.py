@@ -106,6 +106,10 @@ def lib():
         L.sbwt_free.argtypes = [vp]
         L.sbwt_fastx_parse.argtypes = [vp, u64, vp, u64, vp, u64, C.POINTER(u64),
                                        C.POINTER(u64), u32, C.c_int, vp]
+        L.sbwt_format_index_results.argtypes = [vp, vp, u64, u32, C.c_int, vp, u64,
+                                                C.POINTER(u64), u32, C.c_int, vp]
+        L.sbwt_format_color_results.argtypes = [vp, vp, u64, u64, C.c_int, vp, u64,
+                                                C.POINTER(u64), u32, C.c_int, vp]
         L.sbwt_free.restype = None
         L.sbwt_autotune.argtypes = [vp, vp, u64, vp, u64, u64, C.POINTER(u32),
                                     C.POINTER(u32), C.POINTER(u64), C.POINTER(C.c_double)]
@@ -503,3 +507,33 @@ def fastx_parse(text, device: int = 0):
         ends = np.zeros(1, dtype=np.uint64)
     check(rc)
     return chars[:nc.value], ends[:nr.value]
+
+
+def _format(fn, *args, device=0):
+    nb = C.c_uint64()
+    rc = fn(*args, None, 0, C.byref(nb), 0, device, None)
+    if rc == OK:
+        return b""
+    if rc != E_CAPACITY:
+        check(rc)
+    out = np.zeros(max(nb.value, 1), dtype=np.uint8)
+    check(fn(*args, _ptr(out), len(out), C.byref(nb), 0, device, None))
+    return out[:nb.value].tobytes()
+
+
+def format_index_results(results, read_ends, k: int, fmt: int = 0, device: int = 0) -> bytes:
+    """Index results of one batch formatted on the GPU (0 ascii, 1 binary,
+    2 bool), byte for byte what the host writers emit after the header."""
+    res = np.ascontiguousarray(results, dtype=np.uint64)
+    ends = np.ascontiguousarray(read_ends, dtype=np.uint64)
+    return _format(lib().sbwt_format_index_results, _ptr(res) if len(res) else None,
+                   _ptr(ends) if len(ends) else None, len(ends), k, fmt, device=device)
+
+
+def format_color_results(ids, ids_offsets, num_colors: int, fmt: int = 0,
+                         device: int = 0) -> bytes:
+    """Pseudoalignment ids formatted on the GPU (0 ascii, 1 binary, 2 csv)."""
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    offs = np.ascontiguousarray(ids_offsets, dtype=np.uint64)
+    return _format(lib().sbwt_format_color_results, _ptr(ids) if len(ids) else None,
+                   _ptr(offs), len(offs) - 1, num_colors, fmt, device=device)

@@ -442,6 +442,128 @@ def bench_cfg1(args, S, torch, dev, tmpdir):
     return res
 
 
+def fastq_text(chars, ends):
+    """Reads as FASTQ records ("@r", sequence, "+", quality 'I'), vectorised."""
+    lens = np.diff(np.concatenate([[0], ends.astype(np.int64)]))
+    rec = 3 + lens + 1 + 2 + lens + 1
+    start = np.concatenate([[0], np.cumsum(rec)[:-1]])
+    out = np.full(int(rec.sum()), ord("I"), dtype=np.uint8)
+    for off, b in ((0, b"@"), (1, b"r"), (2, b"\n")):
+        out[start + off] = b[0]
+    seq_at = start + 3
+    idx = np.repeat(seq_at - np.concatenate([[0], ends[:-1].astype(np.int64)]), lens) + \
+        np.arange(int(lens.sum()))
+    out[idx] = chars[:int(lens.sum())]
+    out[seq_at + lens] = ord("\n")
+    out[seq_at + lens + 1] = ord("+")
+    out[seq_at + lens + 2] = ord("\n")
+    out[start + rec - 1] = ord("\n")
+    return out
+
+
+def bench_io(args, S, torch, dev, tmpdir, idx, path, chars, ends, d_out, d_ends, n_kmers):
+    """The reads' ends of the path on the GPU: FASTQ parsing (sbwt_fastx_parse)
+    against the host reader, ascii formatting of the timed run's results
+    (sbwt_format_index_results) against the host writer, and the command line
+    tool end to end on one FASTQ file."""
+    import subprocess
+    L = S.lib()
+    L.sbwt_fastx_read.argtypes = [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]
+    L.sbwt_free.argtypes = [C.c_void_p]
+    L.sbwt_write_index_results.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p,
+                                           C.c_void_p, C.c_uint64, C.c_uint32]
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    # parsing: 2 M reads as FASTQ
+    n_sub = min(2_000_000, len(ends))
+    sub_ends = ends[:n_sub]
+    text = fastq_text(chars, sub_ends)
+    fq = os.path.join(tmpdir, "q.fq")
+    text.tofile(fq)
+    d_text = torch.from_numpy(text).to(f"cuda:{dev}")
+    n_chars = int(sub_ends[-1])
+    d_pc = torch.empty(n_chars, dtype=torch.uint8, device=f"cuda:{dev}")
+    d_pe = torch.empty(n_sub, dtype=torch.int64, device=f"cuda:{dev}")
+    nc, nr = C.c_uint64(), C.c_uint64()
+
+    def parse():
+        S.check(L.sbwt_fastx_parse(d_text.data_ptr(), len(text), d_pc.data_ptr(), n_chars,
+                                   d_pe.data_ptr(), n_sub, C.byref(nc), C.byref(nr),
+                                   S.DEVICE_POINTERS, dev, stream.cuda_stream))
+
+    parse()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(3):
+        parse()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_dev = e0.elapsed_time(e1) / 3 / 1e3
+    exact = (nr.value == n_sub and np.array_equal(d_pe.cpu().numpy().view(np.uint64), sub_ends)
+             and np.array_equal(d_pc.cpu().numpy(), chars[:n_chars]))
+    ch, en, hc, hr = C.c_void_p(), C.c_void_p(), C.c_uint64(), C.c_uint64()
+    t0 = time.perf_counter()
+    S.check(L.sbwt_fastx_read(fq.encode(), C.byref(ch), C.byref(hc), C.byref(en), C.byref(hr)))
+    t_host = time.perf_counter() - t0
+    L.sbwt_free(ch)
+    L.sbwt_free(en)
+    out["parse"] = {"input": f"{n_sub} reads as FASTQ ({len(text)} bytes), device-resident",
+                    "device_gb_s": len(text) / t_dev / 1e9, "device_ms": t_dev * 1e3,
+                    "host_reader_gb_s": len(text) / t_host / 1e9, "host_threads": 1,
+                    "speedup": t_host / t_dev, "exact_vs_input": bool(exact)}
+    del d_text, d_pc, d_pe
+    # formatting the timed run's results (all reads, ascii)
+    nb = C.c_uint64()
+    fmt_args = (d_out.data_ptr(), d_ends.data_ptr(), len(ends), CFG["k"], 0)
+    rc = L.sbwt_format_index_results(*fmt_args, None, 0, C.byref(nb), S.DEVICE_POINTERS, dev,
+                                     stream.cuda_stream)
+    assert rc == S.E_CAPACITY, rc
+    d_fmt = torch.empty(nb.value, dtype=torch.uint8, device=f"cuda:{dev}")
+
+    def fmt():
+        S.check(L.sbwt_format_index_results(*fmt_args, d_fmt.data_ptr(), nb.value, C.byref(nb),
+                                            S.DEVICE_POINTERS, dev, stream.cuda_stream))
+
+    fmt()
+    e0.record(stream)
+    for _ in range(3):
+        fmt()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_fmt = e0.elapsed_time(e1) / 3 / 1e3
+    # the host writer on the first 2 M reads, and the bytes compared
+    n_sk = int(np.maximum(np.diff(np.concatenate([[0], sub_ends.astype(np.int64)])) -
+                          CFG["k"] + 1, 0).sum())
+    h_res = d_out[:n_sk].cpu().numpy().view(np.uint64)
+    t0 = time.perf_counter()
+    S.check(L.sbwt_write_index_results(os.path.join(tmpdir, "hw").encode(), 0, 0,
+                                       h_res.ctypes.data, sub_ends.ctypes.data, n_sub,
+                                       CFG["k"]))
+    t_hw = time.perf_counter() - t0
+    host_bytes = open(os.path.join(tmpdir, "hw.txt"), "rb").read()
+    same = d_fmt[:len(host_bytes)].cpu().numpy().tobytes() == host_bytes
+    out["format_ascii"] = {"kmers": int(n_kmers), "bytes": int(nb.value),
+                           "device_ms": t_fmt * 1e3, "device_kmers_per_s": n_kmers / t_fmt,
+                           "device_gb_s_written": nb.value / t_fmt / 1e9,
+                           "host_writer_kmers_per_s": n_sk / t_hw, "host_threads": 1,
+                           "sample_bytes_equal_host_writer": bool(same)}
+    del d_fmt
+    torch.cuda.empty_cache()
+    # the command line tool on the FASTQ file (index load + device path)
+    cli = REPO / "sbwt-search_b200" / "_build" / "sbwt_search"
+    t0 = time.perf_counter()
+    r = subprocess.run([str(cli), "index", "-i", path, "-q", fq, "-o",
+                        os.path.join(tmpdir, "cli"), "--no-headers"], capture_output=True)
+    t_cli = time.perf_counter() - t0
+    cli_same = r.returncode == 0 and open(os.path.join(tmpdir, "cli.txt"), "rb").read() == host_bytes
+    out["cli"] = {"command": "sbwt_search index -i <cfg2.sbwt> -q <2M-read FASTQ> -o <prefix> "
+                             "--no-headers", "wall_s": t_cli, "kmers": n_sk,
+                  "kmers_per_s_incl_index_load": n_sk / t_cli,
+                  "output_equal_host_writer": bool(cli_same), "rc": r.returncode}
+    return out
+
+
 def dist_setup(args):
     import replicas as R
     world, rank, local = R.world()
@@ -624,6 +746,11 @@ def main():
     extra = {}
     if not args.index_only and rank == 0:  # per-GPU sections: rank 0 only
         torch.cuda.empty_cache()
+        try:
+            extra["io"] = bench_io(args, S, torch, dev, tmp.name, idx, path, chars, ends, d_out,
+                                   d_ends, n_kmers)
+        except Exception as e:
+            extra["io"] = {"error": repr(e)}
         try:
             extra["cfg1"] = bench_cfg1(args, S, torch, dev, tmp.name)
         except Exception as e:

@@ -361,9 +361,12 @@ int sbwt_autotune(const sbwt_index_t *index, const char *d_chars,
                   uint64_t n_reads, uint64_t sample_chars,
                   uint32_t *best_presearch, uint32_t *best_blocks_per_sm,
                   uint64_t *best_tile, double *best_ms);
-/* Reads and resets the totals (any pointer may be NULL). */
+/* Reads and resets the totals (any pointer may be NULL).  counters (count
+ * mode): presearch lookups, rank-block sectors, suffix-group words, probe
+ * iterations, warp iterations, lane load steps, k-mers written without a
+ * search, k-mers searched. */
 int sbwt_profile_read(double *search_ms, uint64_t *search_launches,
-                      uint64_t *launches, uint64_t counters[4]);
+                      uint64_t *launches, uint64_t counters[8]);
 
 #ifdef __cplusplus
 }

@@ -4,16 +4,16 @@
 // (layer_0 per 2^32 bits, layer_1_2 per 1024 bits: src/Poppy/Poppy.h:19-27,
 // rank in src/UtilityKernels/Rank.cuh:26-65), so one rank reads a 256-bit basic
 // block of bits and an 8-byte layer_1_2 entry from another line.  Here the
-// count and the bits share one 32-byte DRAM sector, so a rank is ONE sector:
+// counts and the bits share one 32-byte DRAM sector, so a rank is ONE sector
+// and a handful of instructions (one masked popcount):
 //
-//   block b (32 bytes, 32-byte aligned) covers positions [224 b, 224 b + 224):
-//     w0 = ones before the block, relative to its superchunk (low 32 bits)
-//          | payload bits 0..31 << 32
-//     w1 = payload bits  32..95,  w2 = payload bits 96..159,
-//     w3 = payload bits 160..223
-//   superchunk s = blocks [2^24 s, 2^24 (s+1)) (3.76e9 positions);
+//   block b (32 bytes, 32-byte aligned) covers positions [192 b, 192 b + 192):
+//     w0, w1, w2 = payload bits 0..63, 64..127, 128..191
+//     w3 = ones before the block, relative to its superchunk (bits 0..31)
+//          | ones in w0 << 40 | ones in w0 and w1 << 48
+//   superchunk s = blocks [2^24 s, 2^24 (s+1)) (3.2e9 positions);
 //   l0[s] = ones before superchunk s (u64).
-// There are floor(N / 224) + 1 blocks, so rank(v, N) (reached from an
+// There are floor(N / 192) + 1 blocks, so rank(v, N) (reached from an
 // interval that ends at the last node) is defined and equals the total.
 #pragma once
 
@@ -27,7 +27,7 @@
 
 namespace sbwt {
 
-constexpr uint32_t kBlockBits = 224;
+constexpr uint32_t kBlockBits = 192;
 constexpr uint32_t kSuperchunkShift = 24;
 
 struct Block {

@@ -468,11 +468,11 @@ constexpr uint64_t kNarrowLimit = (uint64_t)kBlockBits << kSuperchunkShift;
 
 // Index arithmetic of the search kernel: all 32-bit (nodes, chunk
 // positions, k-mer slots, read numbers) when the SBWT has fewer than
-// 224 * 2^24 nodes (one superchunk: no l0 table) and the batch fewer than
+// 192 * 2^24 nodes (one superchunk: no l0 table) and the batch fewer than
 // 2^32 chars, else all 64-bit.
 template <class I>
 __device__ __forceinline__ I block_idx(I i) {
-  return (I)((uint32_t)((uint64_t)i >> 5) / 7u);
+  return (I)((uint32_t)((uint64_t)i >> 6) / 3u);
 }
 
 // Per-lane register window over the packed chars and invalid bits (see
@@ -546,7 +546,8 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
   const I tsize = (I)rv.tile;
   const I n_tiles = (n_kmers + tsize - 1) / tsize;
   const I base = (I)rv.base;
-  uint64_t n_pre = 0, n_block = 0, n_sg = 0, n_probe = 0;
+  uint64_t n_pre = 0, n_block = 0, n_sg = 0, n_probe = 0, n_iter = 0, n_lane = 0, n_known = 0,
+           n_searched = 0;
   bool exhausted = false;  // the work queue is empty for this lane
   I slot = 0, slot_end = 0, r = 0, r_next = 0, pos = 0, skip_until = 0;
   I last_inv1 = 0;  // 1 + last invalid char position (0 = none)
@@ -582,8 +583,12 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
     uint32_t kind = K_NONE;
     I pa = 0, pb = 0;
     uint64_t pre_e = 0;
+    I run_slot = 0, run_pos = 0;
+    uint32_t run_n = 0;
+    bool run_inv = false;
     if (!done) {
       if (mode == M_NEW) {
+        bool ready = false;
         while (true) {
           if (slot >= slot_end) {  // next tile
             if (new_tile == NONE) {  // none this iteration
@@ -622,20 +627,34 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
           const I newc = pos + k - 1;
           if (SMALLK) cw.move_to(rv.packed, rv.invalid, pos);
           if (SMALLK ? cw.invalid_at(newc) : invalid_at(rv.invalid, newc)) last_inv1 = newc + 1;
-          uint64_t known = 0;
-          if (last_inv1 > pos) {
-            known = SBWT_INVALID;
-          } else if (slot < skip_until) {
-            known = SBWT_NOT_FOUND;
-          } else {
-            break;  // a k-mer to search
+          const bool skip = slot < skip_until;
+          if (last_inv1 <= pos && !skip) {
+            ready = true;  // a k-mer to search
+            break;
           }
-          if (slot < rv.out_capacity) __stcs(rv.out + slot, (unsigned long long)known);
+          if (run_n) break;  // one run per iteration: this lane resumes next time
+          // a run of k-mers whose results are known without a search (an
+          // invalid char in each, or proven absent by the probe), up to the
+          // read / tile end; the warp writes it below
+          const I n = min(skip ? skip_until - slot : last_inv1 - pos, min(r_next, slot_end) - slot);
+          run_inv = !skip;
+          run_slot = slot;
+          run_pos = pos;
+          run_n = (uint32_t)n;
+          if (COUNT) n_known += n;
           v = NONE;
-          ++slot;
-          ++pos;
+          slot += n;
+          pos += n;
+          if (slot < min(r_next, slot_end)) {  // the window moved: its last invalid char
+            if (SMALLK) {
+              cw.move_to(rv.packed, rv.invalid, pos);
+              last_inv1 = cw.last_invalid1(pos, pos + k - 1);
+            } else {
+              last_inv1 = (I)(last_invalid(rv.invalid, pos, pos + k - 1) + 1);
+            }
+          }
         }
-        if (!done && slot < slot_end) {
+        if (ready) {
           if (STREAM && v != NONE) {
             kind = K_BLOCK;
             c = SMALLK ? cw.char_at(pos + k - 1) : char_at(rv.packed, pos + k - 1);
@@ -662,6 +681,22 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
                 (SMALLK ? cw.prefix(pu, ubit) : chars_prefix(rv.packed, pu, ubit));
       }
     }
+    // ---- known runs (converged): the warp writes each lane's run, 32 slots
+    // per store; a probe-proven run is -1 except where a k-mer holds an
+    // invalid char (-2 takes priority)
+    for (unsigned runs = __ballot_sync(0xFFFFFFFFu, run_n != 0); runs; runs &= runs - 1) {
+      const int q = __ffs(runs) - 1;
+      const I q_slot = __shfl_sync(0xFFFFFFFFu, run_slot, q);
+      const I q_pos = __shfl_sync(0xFFFFFFFFu, run_pos, q);
+      const uint32_t q_n = __shfl_sync(0xFFFFFFFFu, run_n, q);
+      const bool q_inv = __shfl_sync(0xFFFFFFFFu, (uint32_t)run_inv, q) != 0;
+      for (uint32_t j = lane; j < q_n; j += 32) {
+        const I p = q_pos + (I)j;
+        const bool inv = q_inv || last_invalid(rv.invalid, p, p + k) >= 0;
+        if (q_slot + j < rv.out_capacity)
+          __stcs(rv.out + q_slot + j, (unsigned long long)(inv ? SBWT_INVALID : SBWT_NOT_FOUND));
+      }
+    }
     if (__all_sync(0xFFFFFFFFu, done)) break;
     // ---- phase 2 (converged): the loads ------------------------------------
     const I ba = block_idx(pa), bb = block_idx(pb);
@@ -684,6 +719,8 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
       n_block += (kind == K_BLOCK) + (addrB != nullptr);
       n_sg += kind == K_SGW;
       n_probe += (mode == M_PPRE || mode == M_PROBE);
+      n_iter += lane == 0;
+      n_lane += kind != K_NONE;
     }
     if (done || kind == K_NONE) continue;
     // ---- phase 3: one shared rank computation, then per-mode updates ------
@@ -803,6 +840,7 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
         break;
     }
     if (emitted) {
+      if (COUNT) ++n_searched;
       v = emit;
       uint64_t res = emit == NONE ? SBWT_NOT_FOUND : (uint64_t)emit;
       if (move_to_key && res != SBWT_NOT_FOUND) res = key_walk(s, res, err);
@@ -828,6 +866,10 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
     atomicAdd(counters + 1, (unsigned long long)n_block);
     atomicAdd(counters + 2, (unsigned long long)n_sg);
     atomicAdd(counters + 3, (unsigned long long)n_probe);
+    atomicAdd(counters + 4, (unsigned long long)n_iter);
+    atomicAdd(counters + 5, (unsigned long long)n_lane);
+    atomicAdd(counters + 6, (unsigned long long)n_known);
+    atomicAdd(counters + 7, (unsigned long long)n_searched);
   }
 }
 
@@ -844,7 +886,7 @@ struct Profile {
   double search_ms = 0;
   uint64_t search_launches = 0;
   uint64_t launches = 0;
-  uint64_t counters[4] = {0, 0, 0, 0};
+  uint64_t counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   DeviceBuffer d_counters;
 };
 static Profile &profile() {
@@ -991,17 +1033,16 @@ void build_rank_blocks_host(const u64 *words, u64 num_bits,
       chunk_base = ones;
     }
     const u64 s = b * kBlockBits;
-    u64 p0 = clip(get64(s) & 0xFFFFFFFFULL, s, 32);
-    u64 p1 = clip(get64(s + 32), s + 32, 64);
-    u64 p2 = clip(get64(s + 96), s + 96, 64);
-    u64 p3 = clip(get64(s + 160), s + 160, 64);
+    const u64 p0 = clip(get64(s), s, 64);
+    const u64 p1 = clip(get64(s + 64), s + 64, 64);
+    const u64 p2 = clip(get64(s + 128), s + 128, 64);
+    const u64 c0 = __builtin_popcountll(p0), c1 = __builtin_popcountll(p1);
     Block &B = blocks[b];
-    B.w0 = ((ones - chunk_base) & 0xFFFFFFFFULL) | (p0 << 32);
+    B.w0 = p0;
     B.w1 = p1;
     B.w2 = p2;
-    B.w3 = p3;
-    ones += __builtin_popcountll(p0) + __builtin_popcountll(p1) +
-            __builtin_popcountll(p2) + __builtin_popcountll(p3);
+    B.w3 = ((ones - chunk_base) & 0xFFFFFFFFULL) | (c0 << 40) | ((c0 + c1) << 48);
+    ones += c0 + c1 + __builtin_popcountll(p2);
   }
   total = ones;
 }
@@ -1612,22 +1653,24 @@ int sbwt_profile_enable(int enabled, int count_work) {
   return SBWT_OK;
 }
 // search_ms: summed CUDA-event time of the read/position search kernels;
-// counters: [0] full searches, [1] streaming steps, [2] rank-block sectors of
-// full searches (count mode only).  Resets the totals.
+// counters (count mode only): [0] presearch lookups, [1] rank-block sectors,
+// [2] suffix-group words, [3] probe iterations, [4] warp iterations, [5] lane
+// load steps, [6] k-mers written without a search (invalid or proven absent),
+// [7] k-mers searched.  Resets the totals.
 int sbwt_profile_read(double *search_ms, uint64_t *search_launches,
-                      uint64_t *launches, uint64_t counters[4]) {
+                      uint64_t *launches, uint64_t counters[8]) {
   sbwt::Profile &p = sbwt::profile();
   std::lock_guard<std::mutex> g(p.mu);
   if (search_ms) *search_ms = p.search_ms;
   if (search_launches) *search_launches = p.search_launches;
   if (launches) *launches = p.launches;
   if (counters) {
-    uint64_t dc[4] = {0, 0, 0, 0};
+    uint64_t dc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (p.d_counters.size()) {
-      cudaMemcpy(dc, p.d_counters.get(), 32, cudaMemcpyDeviceToHost);
+      cudaMemcpy(dc, p.d_counters.get(), 64, cudaMemcpyDeviceToHost);
       cudaMemset(p.d_counters.get(), 0, 64);
     }
-    for (int i = 0; i < 4; ++i) counters[i] = dc[i];
+    for (int i = 0; i < 8; ++i) counters[i] = dc[i];
   }
   p.search_ms = 0;
   p.search_launches = 0;

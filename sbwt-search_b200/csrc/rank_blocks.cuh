@@ -25,28 +25,29 @@ __device__ __forceinline__ uint32_t clamp64(int t) {
   return t <= 0 ? 0u : (t >= 64 ? 64u : (uint32_t)t);
 }
 
-// Ones of the block strictly before in-block offset q (q in [0, 224)),
-// including the block's own 32-bit relative count.
+// Payload word of in-block offset q (q in [0, 192)).
+__device__ __forceinline__ unsigned long long block_word(const Block &b, uint32_t q) {
+  const uint32_t wi = q >> 6;
+  return wi == 0 ? b.w0 : (wi == 1 ? b.w1 : b.w2);
+}
+
+// Ones of the block strictly before in-block offset q (q in [0, 192)),
+// including the block's 32-bit count relative to its superchunk.
 __device__ __forceinline__ uint64_t block_rank(const Block &b, uint32_t q) {
-  const int Q = (int)q + 32;  // bit position inside the 256-bit block
-  uint32_t r = (uint32_t)(b.w0 & 0xFFFFFFFFULL);
-  r += __popcll(b.w0 & low_mask(clamp64(Q)) & 0xFFFFFFFF00000000ULL);
-  r += __popcll(b.w1 & low_mask(clamp64(Q - 64)));
-  r += __popcll(b.w2 & low_mask(clamp64(Q - 128)));
-  r += __popcll(b.w3 & low_mask(clamp64(Q - 192)));
-  return r;
+  const uint32_t hi = (uint32_t)(b.w3 >> 32);
+  const uint32_t sub = (hi >> (8 * (q >> 6))) & 0xFFu;  // 0 for the first word
+  return (uint32_t)b.w3 + sub +
+         (uint32_t)__popcll(block_word(b, q) & ((1ULL << (q & 63)) - 1ULL));
 }
 
 __device__ __forceinline__ bool block_bit(const Block &b, uint32_t q) {
-  const uint32_t Q = q + 32;
-  unsigned long long w = Q < 64 ? b.w0 : (Q < 128 ? b.w1 : (Q < 192 ? b.w2 : b.w3));
-  return (w >> (Q & 63)) & 1ULL;
+  return (block_word(b, q) >> (q & 63)) & 1ULL;
 }
 
 // Block of position i.  Indexes are < 2^37 (checked when an index is built),
-// so i / 224 = (i >> 5) / 7 is a 32-bit division by a constant.
+// so i / 192 = (i >> 6) / 3 is a 32-bit division by a constant.
 __device__ __forceinline__ uint64_t block_of(uint64_t i) {
-  return (uint64_t)((uint32_t)(i >> 5) / 7u);
+  return (uint64_t)((uint32_t)(i >> 6) / 3u);
 }
 
 // rank_c(i): ones of vector c in [0, i), i in [0, N].

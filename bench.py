@@ -395,7 +395,7 @@ def bench_cfg1(args, S, torch, dev, tmpdir):
     L.sbwt_profile_enable(1, 1)
     step()
     torch.cuda.synchronize()
-    ctr = (C.c_uint64 * 8)()
+    ctr = (C.c_uint64 * 16)()
     L.sbwt_profile_read(None, None, None, ctr)
     L.sbwt_profile_enable(0, 0)
     sectors = int(ctr[0]) + int(ctr[1]) + int(ctr[2])
@@ -671,7 +671,7 @@ def main():
     L.sbwt_profile_enable(1, 1)
     step_dev()
     torch.cuda.synchronize()
-    ctr = (C.c_uint64 * 8)()
+    ctr = (C.c_uint64 * 16)()
     L.sbwt_profile_read(None, None, None, ctr)
     n_pre, n_block, n_sg, n_probe = (int(ctr[0]), int(ctr[1]), int(ctr[2]), int(ctr[3]))
     n_iter, n_lane, n_known, n_searched = (int(ctr[4]), int(ctr[5]), int(ctr[6]), int(ctr[7]))
@@ -805,7 +805,11 @@ def main():
                               "warp_iterations": n_iter,
                               "lanes_loading_per_iteration": n_lane / max(n_iter, 1),
                               "kmers_written_without_search": n_known,
-                              "kmers_searched": n_searched},
+                              "kmers_searched": n_searched,
+                              "lane_steps_by_path": dict(zip(
+                                  ["stream", "presearch", "walk", "group_scan",
+                                   "group_start", "probe"], [int(x) for x in ctr[8:14]])),
+                              "distinct_paths_per_iteration": int(ctr[14]) / max(n_iter, 1)},
                      "random_sector": {"achieved_gsectors_s": rs_achieved / 1e9,
                                        "peak_gsectors_s": rs_peak and rs_peak / 1e9,
                                        "frac": rs_peak and rs_achieved / rs_peak,

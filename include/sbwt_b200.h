@@ -364,9 +364,11 @@ int sbwt_autotune(const sbwt_index_t *index, const char *d_chars,
 /* Reads and resets the totals (any pointer may be NULL).  counters (count
  * mode): presearch lookups, rank-block sectors, suffix-group words, probe
  * iterations, warp iterations, lane load steps, k-mers written without a
- * search, k-mers searched. */
+ * search, k-mers searched, lane steps of each search path (stream step,
+ * presearch of a new k-mer, walk, group scan, group-start check, probe),
+ * distinct paths per warp iteration (summed), and one unused entry. */
 int sbwt_profile_read(double *search_ms, uint64_t *search_launches,
-                      uint64_t *launches, uint64_t counters[8]);
+                      uint64_t *launches, uint64_t counters[16]);
 
 #ifdef __cplusplus
 }

@@ -388,15 +388,18 @@ __global__ void tile_reads_kernel(const uint64_t *kmer_off, uint64_t n_reads, ui
 // Every lane runs its own state machine; each loop iteration is one memory
 // round trip per active lane: addresses are computed per lane, the warp
 // reconverges (warp-uniform exit test) and issues the loads together, then
-// ONE shared rank computation serves every mode, followed by small per-mode
-// updates.
-//   M_NEW   : the k-mer at `slot` needs its first load (stream step if the
-//             previous k-mer was found, else the presearch entry);
-//   M_WALK  : full search, next char wi (rank blocks of l and r + 1);
-//   M_SG    : stream step, suffix-group-start word u (bits <= ubit);
-//   M_GS    : stream step, rank block of char c at the group start u;
-//   M_PPRE  : probe, presearch entry of x[m..m+lvl);
-//   M_PROBE : probe, next char wi up to probe_end.
+// ONE shared rank computation serves every mode.  Three of the modes are the
+// same backward-search step (rank blocks of l and rr + 1 for the char at wi),
+// so most lanes take one code path:
+//   M_NEW    : the k-mer at `slot` needs its first load (stream step if the
+//              previous k-mer was found, else the presearch entry);
+//   M_WALK   : search walk (also the single step at a group start g);
+//   M_STREAM : the step on [v, v] from the previous k-mer's node v; empty
+//              means no edge at v itself, so the group scan follows;
+//   M_SG     : suffix-group-start word u (bits <= ubit) below a failed stream
+//              step;
+//   M_PPRE   : probe, presearch entry of x[m..m+lvl);
+//   M_PROBE  : probe walk up to probe_end (nothing is emitted).
 // Per-lane register window over the packed chars and invalid bits of a read:
 // words wbase and wbase + 1, i.e. chunk positions [32 wbase, 32 wbase + 64).
 // With k <= 33 every char the lane needs for the k-mer at pos (and for a probe
@@ -457,7 +460,13 @@ struct CharWindow {
   }
 };
 
-enum : uint32_t { M_NEW = 0, M_WALK = 1, M_SG = 2, M_GS = 3, M_PPRE = 4, M_PROBE = 5 };
+// Lane modes: a new k-mer; the group-start scan of a failed stream step; the
+// presearch of a probe; and three walks that share one step (the backward
+// search step on [l, rr] with the char at wi): the walk of a k-mer search
+// (also the single step of a group start), the stream step from the previous
+// k-mer's node (an empty result sends the lane to the group scan), and the
+// walk of a probe (its end proves k-mers absent or not; nothing is emitted).
+enum : uint32_t { M_NEW = 0, M_SG = 1, M_PPRE = 2, M_WALK = 4, M_STREAM = 5, M_PROBE = 6 };
 enum : uint32_t { K_NONE = 0, K_BLOCK = 1, K_PRE = 2, K_SGW = 3 };
 // SBWTs with fewer nodes than this use 32-bit node arithmetic in the search.
 constexpr uint64_t kNarrowLimit = (uint64_t)kBlockBits << kSuperchunkShift;
@@ -547,7 +556,8 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
   const I n_tiles = (n_kmers + tsize - 1) / tsize;
   const I base = (I)rv.base;
   uint64_t n_pre = 0, n_block = 0, n_sg = 0, n_probe = 0, n_iter = 0, n_lane = 0, n_known = 0,
-           n_searched = 0;
+           n_searched = 0, n_distinct = 0;
+  uint64_t n_mode[6] = {0, 0, 0, 0, 0, 0};
   bool exhausted = false;  // the work queue is empty for this lane
   I slot = 0, slot_end = 0, r = 0, r_next = 0, pos = 0, skip_until = 0;
   I last_inv1 = 0;  // 1 + last invalid char position (0 = none)
@@ -655,27 +665,25 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
           }
         }
         if (ready) {
-          if (STREAM && v != NONE) {
-            kind = K_BLOCK;
-            c = SMALLK ? cw.char_at(pos + k - 1) : char_at(rv.packed, pos + k - 1);
-            pa = pb = v;
+          if (STREAM && v != NONE) {  // the stream step: one walk step on [v, v]
+            l = rr = v;
+            wi = pos + k - 1;
+            mode = M_STREAM;
           } else {
             kind = K_PRE;
             pre_e = presearch_level_offset(s.p) +
                     (SMALLK ? cw.prefix(pos, s.p) : chars_prefix(rv.packed, pos, s.p));
           }
         }
-      } else if (mode == M_WALK || mode == M_PROBE) {
+      }
+      if (mode >= M_WALK) {
         kind = K_BLOCK;
         c = SMALLK ? cw.char_at(wi) : char_at(rv.packed, wi);
         pa = l;
         pb = rr + 1;
       } else if (mode == M_SG) {
         kind = K_SGW;
-      } else if (mode == M_GS) {
-        kind = K_BLOCK;
-        pa = pb = u;
-      } else {  // M_PPRE: pu = probe start m, ubit = level
+      } else if (mode == M_PPRE) {  // pu = probe start m, ubit = level
         kind = K_PRE;
         pre_e = presearch_level_offset(ubit) +
                 (SMALLK ? cw.prefix(pu, ubit) : chars_prefix(rv.packed, pu, ubit));
@@ -721,6 +729,16 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
       n_probe += (mode == M_PPRE || mode == M_PROBE);
       n_iter += lane == 0;
       n_lane += kind != K_NONE;
+      // phase-3 paths: stream step, presearch of a new k-mer, walk, group
+      // scan, group-start check, probe (presearch or walk)
+      const uint32_t path = kind == K_NONE ? 6u
+                            : mode == M_STREAM ? 0u
+                            : mode == M_NEW ? 1u
+                            : mode == M_WALK ? 2u
+                            : mode == M_SG ? 3u : 5u;
+      if (path < 6) ++n_mode[path];
+      const uint32_t seen = __reduce_or_sync(0xFFFFFFFFu, path < 6 ? 1u << path : 0u);
+      n_distinct += lane == 0 ? __popc(seen) : 0;
     }
     if (done || kind == K_NONE) continue;
     // ---- phase 3: one shared rank computation, then per-mode updates ------
@@ -732,7 +750,6 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
       ra += (I)l0c[(uint64_t)ba >> kSuperchunkShift];
       rb += (I)l0c[(uint64_t)bb >> kSuperchunkShift];
     }
-    const bool bita = block_bit(A, qa);
     I pl = 0, pr = 0;
     if (kind == K_PRE) {
       if (!s.wide) {
@@ -747,97 +764,78 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
     I emit = 0;
     bool emitted = false;
     I fail_at = NONE;  // char where a search of this k-mer failed
-    switch (mode) {
-      case M_NEW:
-        if (kind == K_BLOCK) {  // stream step from v
-          if (bita) {
-            emit = ra;
-            emitted = true;
-          } else {
-            u = v >> 6;
-            ubit = (uint32_t)(v & 63);
-            mode = M_SG;
-          }
-        } else if (pl > pr) {
-          emit = NONE;
-          emitted = true;
-        } else if (s.p >= k) {
-          emit = pl;
-          emitted = true;
+    if (mode >= M_WALK) {  // one backward-search step (the common path)
+      l = ra;
+      rr = rb - 1;
+      ++wi;
+      if (l > rr) {
+        if (mode == M_STREAM) {  // no edge at v itself: find v's group start
+          u = v >> 6;
+          ubit = (uint32_t)(v & 63);
+          mode = M_SG;
+        } else if (mode == M_PROBE) {  // x[m..probe_end] is absent
+          skip_until = probe_skip;
+          mode = M_NEW;
         } else {
-          l = pl;
-          rr = pr;
-          wi = pos + s.p;
-          mode = M_WALK;
-        }
-        break;
-      case M_WALK:
-        l = ra;
-        rr = rb - 1;
-        ++wi;
-        if (l > rr) {
           emit = NONE;
           emitted = true;
           fail_at = wi - 1;
-        } else if (wi == pos + k) {
+        }
+      } else if (wi == (mode == M_PROBE ? probe_end + 1 : pos + k)) {
+        if (mode == M_PROBE) {
+          mode = M_NEW;  // present: nothing to skip
+        } else {
           emit = l;
           emitted = true;
         }
-        break;
-      case M_SG: {
-        const uint64_t w = chunk_word(A, (uint64_t)u) & low_mask(ubit + 1);
-        if (w) {
-          const I g = (I)((uint64_t)u * 64 + 63 - __clzll(w));
-          if (g == v) {  // v starts its group and has no edge c
-            emit = NONE;
-            emitted = true;
-            fail_at = pos + k - 1;
-          } else {
-            u = g;
-            mode = M_GS;
-          }
-        } else if (u == 0) {
-          emit = NONE;  // no group start below v: malformed SBWT
-          emitted = true;
-        } else {
-          --u;
-          ubit = 63;
-        }
-        break;
       }
-      case M_GS:
-        emitted = true;
-        if (bita) {
-          emit = ra;
+    } else if (kind == K_PRE) {  // presearch of a new k-mer or of a probe
+      const bool probe = mode == M_PPRE;
+      if (pl > pr) {
+        if (probe) {
+          skip_until = probe_skip;
+          mode = M_NEW;
         } else {
           emit = NONE;
-          fail_at = pos + k - 1;
+          emitted = true;
         }
-        break;
-      case M_PPRE:
-        if (pl > pr) {
-          skip_until = probe_skip;  // x[m..probe_end] is absent
-          mode = M_NEW;
-        } else if (pu + ubit > probe_end) {
-          mode = M_NEW;  // present: nothing to skip
+      } else {
+        const I start = probe ? pu + ubit : pos + s.p;
+        const I end = probe ? probe_end + 1 : pos + k;
+        if (start >= end) {  // the presearch covered every char
+          if (probe) {
+            mode = M_NEW;
+          } else {
+            emit = pl;
+            emitted = true;
+          }
         } else {
           l = pl;
           rr = pr;
-          wi = pu + ubit;
-          mode = M_PROBE;
+          wi = start;
+          mode = probe ? M_PROBE : M_WALK;
         }
-        break;
-      default:  // M_PROBE
-        l = ra;
-        rr = rb - 1;
-        ++wi;
-        if (l > rr) {
-          skip_until = probe_skip;
-          mode = M_NEW;
-        } else if (wi > probe_end) {
-          mode = M_NEW;
+      }
+    } else {  // M_SG: suffix-group starts at or below v, one word per step
+      const uint64_t w = chunk_word(A, (uint64_t)u) & low_mask(ubit + 1);
+      if (w) {
+        const I g = (I)((uint64_t)u * 64 + 63 - __clzll(w));
+        if (g == v) {  // v starts its group and has no edge c
+          emit = NONE;
+          emitted = true;
+          fail_at = pos + k - 1;
+        } else {  // the edge bit of v's group lives at g: one step on [g, g]
+          l = rr = g;
+          wi = pos + k - 1;
+          mode = M_WALK;
         }
-        break;
+      } else if (u == 0) {
+        emit = NONE;  // no group start below v: malformed SBWT
+        emitted = true;
+      } else {
+        --u;
+        ubit = 63;
+      }
     }
     if (emitted) {
       if (COUNT) ++n_searched;
@@ -870,6 +868,8 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
     atomicAdd(counters + 5, (unsigned long long)n_lane);
     atomicAdd(counters + 6, (unsigned long long)n_known);
     atomicAdd(counters + 7, (unsigned long long)n_searched);
+    for (int i = 0; i < 6; ++i) atomicAdd(counters + 8 + i, (unsigned long long)n_mode[i]);
+    atomicAdd(counters + 14, (unsigned long long)n_distinct);
   }
 }
 
@@ -886,7 +886,7 @@ struct Profile {
   double search_ms = 0;
   uint64_t search_launches = 0;
   uint64_t launches = 0;
-  uint64_t counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  uint64_t counters[16] = {};
   DeviceBuffer d_counters;
 };
 static Profile &profile() {
@@ -952,8 +952,8 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
   if (timed && p.count) {
     std::lock_guard<std::mutex> g(p.mu);
     if (p.d_counters.size() == 0) {
-      p.d_counters.resize(64);
-      SBWT_CUDA(cudaMemset(p.d_counters.get(), 0, 64));
+      p.d_counters.resize(128);
+      SBWT_CUDA(cudaMemset(p.d_counters.get(), 0, 128));
     }
     ctr = p.d_counters.get<unsigned long long>();
   }
@@ -1656,21 +1656,23 @@ int sbwt_profile_enable(int enabled, int count_work) {
 // counters (count mode only): [0] presearch lookups, [1] rank-block sectors,
 // [2] suffix-group words, [3] probe iterations, [4] warp iterations, [5] lane
 // load steps, [6] k-mers written without a search (invalid or proven absent),
-// [7] k-mers searched.  Resets the totals.
+// [7] k-mers searched, [8..13] lane steps of each phase-3 path (stream step,
+// presearch of a new k-mer, walk, group scan, group-start check, probe),
+// [14] distinct paths per warp iteration, summed.  Resets the totals.
 int sbwt_profile_read(double *search_ms, uint64_t *search_launches,
-                      uint64_t *launches, uint64_t counters[8]) {
+                      uint64_t *launches, uint64_t counters[16]) {
   sbwt::Profile &p = sbwt::profile();
   std::lock_guard<std::mutex> g(p.mu);
   if (search_ms) *search_ms = p.search_ms;
   if (search_launches) *search_launches = p.search_launches;
   if (launches) *launches = p.launches;
   if (counters) {
-    uint64_t dc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint64_t dc[16] = {};
     if (p.d_counters.size()) {
-      cudaMemcpy(dc, p.d_counters.get(), 64, cudaMemcpyDeviceToHost);
-      cudaMemset(p.d_counters.get(), 0, 64);
+      cudaMemcpy(dc, p.d_counters.get(), 128, cudaMemcpyDeviceToHost);
+      cudaMemset(p.d_counters.get(), 0, 128);
     }
-    for (int i = 0; i < 8; ++i) counters[i] = dc[i];
+    for (int i = 0; i < 16; ++i) counters[i] = dc[i];
   }
   p.search_ms = 0;
   p.search_launches = 0;

@@ -71,7 +71,10 @@ typedef struct {
 /* Loads a .sbwt / .tdbg file (and, when colors_path is not NULL, the key
  * k-mer marks of a .tcolors file for SBWT_MOVE_TO_KEY_KMER) onto `device`
  * and builds the rank blocks and the presearch table there.
- * presearch_letters: 0 = default (12, the reference's depth), else 1..12.
+ * presearch_letters: 0 = default (14 for SBWTs of 2^26 or more nodes, else
+ * the reference's 12), else 1..14 (deeper tables replace more search steps;
+ * results are the same; the depth-14 pyramid takes 2.9 GB, 5.7 GB for 2^32
+ * or more nodes).
  * Replaces SbwtBuilder::get_cpu_sbwt + CpuSbwtContainer::to_gpu +
  * Presearcher::presearch (src/SbwtBuilder/SbwtBuilder.cpp:41-56,
  * src/SbwtContainer/CpuSbwtContainer.cpp:23-35,

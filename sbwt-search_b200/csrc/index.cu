@@ -1058,8 +1058,13 @@ IndexImpl::IndexImpl(const u64 *const acgt[4], u64 num_bits_, u32 k_,
   DeviceGuard g(device);
   num_bits = num_bits_;
   k = k_;
-  p_max = presearch_letters ? presearch_letters : 12;
-  if (p_max > 12) throw Error(SBWT_E_INVALID, "presearch_letters must be <= 12");
+  // default depth: 14 for large SBWTs (each extra letter replaces a search
+  // step), the reference's 12 for small ones (whose deeper tables would only
+  // move lookups from L2 to DRAM)
+  p_max = presearch_letters ? presearch_letters
+                            : (num_bits_ >= (1ULL << 26) ? kPresearchMaxLetters : 12u);
+  if (p_max > kPresearchMaxLetters)
+    throw Error(SBWT_E_INVALID, "presearch_letters must be <= 14");
   if (p_max > k) p_max = k;
   wide = num_bits >= (1ULL << 32) ? 1 : 0;
   // rank blocks, one host thread per vector

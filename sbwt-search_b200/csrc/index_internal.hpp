@@ -9,6 +9,10 @@
 namespace sbwt {
 
 // Launch parameters chosen by the autotuner (0 = built-in default).
+// Deepest presearch table (4^14 entries: 2 GiB at 8 bytes per entry, 2.9 GB
+// with the shallower levels); the reference fixes 12.
+constexpr uint32_t kPresearchMaxLetters = 14;
+
 struct LaunchConfig {
   uint32_t presearch_letters = 0;  // <= the handle's pyramid depth
   uint32_t blocks_per_sm = 8;      // 256-thread blocks per SM in the grid

@@ -738,7 +738,7 @@ int sbwt_autotune(const sbwt_index_t *index, const char *d_chars, uint64_t n_cha
     LaunchConfig best_cfg = saved;
     bool have_ref = false;
     std::vector<u64> h_ref, h_out;
-    for (u32 p = std::min<u32>(12, ix.p_max); p >= std::min<u32>(8, ix.p_max); --p) {
+    for (u32 p = ix.p_max; p >= std::min<u32>(8, ix.p_max); --p) {
       for (u64 tile : {0ULL, 64ULL, 256ULL, 1024ULL}) {
         for (u32 bps : {2u, 3u, 4u, 6u, 8u}) {
           LaunchConfig c = saved;

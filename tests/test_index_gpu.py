@@ -35,7 +35,7 @@ def test_reads_reproduce_reference_fixture(golden_index, name, per_kmer):
     assert rows == exp
 
 
-@pytest.mark.parametrize("p", [0, 1, 7, 12])
+@pytest.mark.parametrize("p", [0, 1, 7, 12, 14])
 def test_positions_seam_matches_oracle_and_reference(p):
     g, path, sb = synthetic(4, 2, 4000, 31, 1, 0.02)
     idx = S.SbwtIndex.open(path, presearch_letters=p)
@@ -181,3 +181,16 @@ def test_tdbg_without_variant_string(tmp_path):
     a, b = S.SbwtIndex.open(path), S.SbwtIndex.open(tdbg)
     chars, ends = mixed_reads(g, 5, 300)
     assert np.array_equal(a.search_reads(chars, ends), b.search_reads(chars, ends))
+
+
+@pytest.mark.parametrize("p", [13, 14])
+def test_deep_presearch_read_search_matches_oracle(p):
+    # presearch tables deeper than the reference's 12 letters: same results
+    g, path, sb = synthetic(6, 3, 6000, 31, 2, 0.02)
+    chars, ends = mixed_reads(g, 9, 800)
+    exp = oracle_results(oracle_index(path, 8), chars, ends)
+    idx = S.SbwtIndex.open(path, presearch_letters=p)
+    assert idx.presearch_letters == p
+    assert np.array_equal(idx.search_reads(chars, ends), exp)
+    with pytest.raises(S.SbwtError):
+        S.SbwtIndex.open(path, presearch_letters=15)

@@ -113,9 +113,15 @@ __device__ __forceinline__ void add_weighted(uint64_t *planes, uint32_t stride, 
   }
 }
 
-constexpr int kRowsInFlight = 4;  // dense rows loaded before the adds
-constexpr int kWindows = 4;       // windows of 32 k-mers whose lookups overlap
-constexpr int kColorBlocksPerSm = 6;
+#ifndef SBWT_COLORS_ROWS_IN_FLIGHT
+#define SBWT_COLORS_ROWS_IN_FLIGHT 4
+#endif
+#ifndef SBWT_COLORS_BLOCKS_PER_SM
+#define SBWT_COLORS_BLOCKS_PER_SM 6
+#endif
+constexpr int kRowsInFlight = SBWT_COLORS_ROWS_IN_FLIGHT;  // dense rows loaded before the adds
+constexpr int kWindows = 4;  // windows of 32 k-mers whose lookups overlap
+constexpr int kColorBlocksPerSm = SBWT_COLORS_BLOCKS_PER_SM;
 
 // Adds m copies of the sparse color list sparse[start, start + len) to this
 // warp's counters for the row words [wbase, wbase + 32 * WL).  Warp-uniform.

@@ -472,7 +472,7 @@ enum : uint32_t { K_NONE = 0, K_BLOCK = 1, K_PRE = 2, K_SGW = 3 };
 constexpr uint64_t kNarrowLimit = (uint64_t)kBlockBits << kSuperchunkShift;
 
 #ifndef SBWT_SEARCH_MIN_BLOCKS
-#define SBWT_SEARCH_MIN_BLOCKS 4  // 256-thread blocks per SM the register budget targets
+#define SBWT_SEARCH_MIN_BLOCKS 5  // 256-thread blocks per SM the register budget targets
 #endif
 
 // Index arithmetic of the search kernel: all 32-bit (nodes, chunk
@@ -550,6 +550,10 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
   __syncthreads();
   const uint32_t k = s.k;
   const uint32_t L = rv.probe_len;
+  // presearch levels of a new k-mer and of a probe (fixed per launch)
+  const uint32_t probe_lvl = min(L, s.p);
+  const uint64_t pre_off = presearch_level_offset(s.p);
+  const uint64_t probe_off = presearch_level_offset(max(probe_lvl, 1u));
   const uint32_t lane = threadIdx.x & 31;
   const I n_kmers = (I)(rv.n_kmers_dev ? *rv.n_kmers_dev : rv.n_kmers);
   const I tsize = (I)rv.tile;
@@ -671,7 +675,7 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
             mode = M_STREAM;
           } else {
             kind = K_PRE;
-            pre_e = presearch_level_offset(s.p) +
+            pre_e = pre_off +
                     (SMALLK ? cw.prefix(pos, s.p) : chars_prefix(rv.packed, pos, s.p));
           }
         }
@@ -683,10 +687,10 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
         pb = rr + 1;
       } else if (mode == M_SG) {
         kind = K_SGW;
-      } else if (mode == M_PPRE) {  // pu = probe start m, ubit = level
+      } else if (mode == M_PPRE) {  // pu = probe start m
         kind = K_PRE;
-        pre_e = presearch_level_offset(ubit) +
-                (SMALLK ? cw.prefix(pu, ubit) : chars_prefix(rv.packed, pu, ubit));
+        pre_e = probe_off +
+                (SMALLK ? cw.prefix(pu, probe_lvl) : chars_prefix(rv.packed, pu, probe_lvl));
       }
     }
     // ---- known runs (converged): the warp writes each lane's run, 32 slots
@@ -800,7 +804,7 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
           emitted = true;
         }
       } else {
-        const I start = probe ? pu + ubit : pos + s.p;
+        const I start = probe ? pu + probe_lvl : pos + s.p;
         const I end = probe ? probe_end + 1 : pos + k;
         if (start >= end) {  // the presearch covered every char
           if (probe) {
@@ -849,7 +853,6 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
         probe_end = fail_at;
         probe_skip = slot + (m - pos) + 1;  // slots of k-mers starting at pos+1..m
         pu = m;
-        ubit = min(L, s.p);
         mode = M_PPRE;
       } else {
         mode = M_NEW;

@@ -160,6 +160,16 @@ int sbwt_search_reads_noalloc(const sbwt_index_t *index, const char *d_chars,
                               uint64_t results_capacity, uint64_t *n_results,
                               uint32_t flags, void *stream);
 
+/* Builds a plain-matrix SBWT of every k-mer of the sequences on `device`
+ * (chars back to back, seq_ends cumulative; k-mers with a non-ACGT char are
+ * skipped; reverse complements added when add_rc; 2 <= k <= 31) and writes
+ * it to out_path in the format sbwt_index_open reads; *n_nodes (optional)
+ * receives the node count.  The reference loads indexes built elsewhere
+ * (Themisto); this is the project's own builder, on the GPU. */
+int sbwt_build_index(const char *chars, uint64_t n_chars, const uint64_t *seq_ends,
+                     uint64_t n_seqs, uint32_t k, int add_rc, const char *out_path,
+                     int device, uint64_t *n_nodes);
+
 /* ------------------------------------------------------------------------ */
 /* Colors step                                                               */
 /* ------------------------------------------------------------------------ */

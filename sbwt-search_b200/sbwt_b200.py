@@ -106,6 +106,8 @@ def lib():
         L.sbwt_free.argtypes = [vp]
         L.sbwt_fastx_parse.argtypes = [vp, u64, vp, u64, vp, u64, C.POINTER(u64),
                                        C.POINTER(u64), u32, C.c_int, vp]
+        L.sbwt_build_index.argtypes = [vp, u64, vp, u64, u32, C.c_int, C.c_char_p, C.c_int,
+                                       C.POINTER(u64)]
         L.sbwt_format_index_results.argtypes = [vp, vp, u64, u32, C.c_int, vp, u64,
                                                 C.POINTER(u64), u32, C.c_int, vp]
         L.sbwt_format_color_results.argtypes = [vp, vp, u64, u64, C.c_int, vp, u64,
@@ -537,3 +539,18 @@ def format_color_results(ids, ids_offsets, num_colors: int, fmt: int = 0,
     offs = np.ascontiguousarray(ids_offsets, dtype=np.uint64)
     return _format(lib().sbwt_format_color_results, _ptr(ids) if len(ids) else None,
                    _ptr(offs), len(offs) - 1, num_colors, fmt, device=device)
+
+
+def build_index(seqs, k: int, out_path, add_rc: bool = True, device: int = 0) -> int:
+    """SBWT of every k-mer of `seqs` (a list of bytes, or (chars, ends)) built
+    on the GPU and written to out_path; returns the node count."""
+    if isinstance(seqs, tuple):
+        chars, ends = _np_chars(seqs[0]), np.ascontiguousarray(seqs[1], dtype=np.uint64)
+    else:
+        chars = _np_chars(b"".join(seqs))
+        ends = np.cumsum([len(x) for x in seqs]).astype(np.uint64)
+    nn = C.c_uint64()
+    check(lib().sbwt_build_index(_ptr(chars) if len(chars) else None, len(chars),
+                                 _ptr(ends) if len(ends) else None, len(ends), k, int(add_rc),
+                                 str(out_path).encode(), device, C.byref(nn)))
+    return nn.value

@@ -587,6 +587,29 @@ def bench_io(args, S, torch, dev, tmpdir, idx, path, chars, ends, d_out, d_ends,
     return out
 
 
+def bench_build(S, T, g, host_path, tmpdir):
+    """The 100 Mbp index built on the GPU (sbwt_build_index) against the host
+    builder (all host threads), and the two files compared byte for byte."""
+    import torch
+    ends = np.cumsum(g.lens).astype(np.uint64)
+    gpu_path = os.path.join(tmpdir, "cfg2_gpu.sbwt")
+    S.build_index((g.chars, ends), CFG["k"], gpu_path)  # warm (CUDA context, caches)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    nodes = S.build_index((g.chars, ends), CFG["k"], gpu_path)
+    t_gpu = time.perf_counter() - t0
+    host2 = os.path.join(tmpdir, "cfg2_host.sbwt")
+    t0 = time.perf_counter()
+    T.build_sbwt(g, CFG["k"], host2)
+    t_host = time.perf_counter() - t0
+    same = open(gpu_path, "rb").read() == open(host_path, "rb").read()
+    return {"input": f"{len(g.lens)} genomes, {int(ends[-1])} bp, k={CFG['k']}, both strands",
+            "nodes": int(nodes), "gpu_s": t_gpu, "host_s": t_host,
+            "host_threads": os.cpu_count(), "speedup": t_host / t_gpu,
+            "file_identical_to_host_build": bool(same),
+            "note": "wall time incl. host<->device copies and writing the .sbwt file"}
+
+
 def dist_setup(args):
     import replicas as R
     world, rank, local = R.world()
@@ -690,6 +713,9 @@ def main():
         n = idx.search_reads(d_chars, d_ends, out=d_out, stream=stream.cuda_stream)
         assert n == n_kmers
 
+    # launch configuration (presearch depth, tile, blocks per SM) chosen by the
+    # library's autotuner on the first 64 M chars of this batch
+    tune = S.autotune(idx, d_chars, d_ends, sample_chars=64 << 20, use_cache=False)
     # one counting pass (outside the timed region): work per k-mer
     L.sbwt_profile_enable(1, 1)
     step_dev()
@@ -770,6 +796,11 @@ def main():
     if not args.index_only and rank == 0:  # per-GPU sections: rank 0 only
         torch.cuda.empty_cache()
         try:
+            import sbwt_tools as T
+            extra["build"] = bench_build(S, T, g, path, tmp.name)
+        except Exception as e:
+            extra["build"] = {"error": repr(e)}
+        try:
             extra["io"] = bench_io(args, S, torch, dev, tmp.name, idx, path, chars, ends, d_out,
                                    d_ends, n_kmers)
         except Exception as e:
@@ -812,7 +843,7 @@ def main():
                    "reads_per_gpu": args.reads, "kmers_per_gpu": n_kmers,
                    "chars_per_gpu": n_chars, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (no flush needed)",
-                   "presearch_letters": idx.presearch_letters},
+                   "presearch_letters": tune["presearch"], "autotune": tune},
         "gpu_launches": int(launches.value),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,

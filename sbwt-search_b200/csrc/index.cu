@@ -1415,63 +1415,63 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
     }
     return;
   }
-  // host pointers: chunk the reads, double-buffer, overlap H2D/compute/D2H
-  const u64 total_k = count_kmers_host(read_ends, n_reads, k, 0);
-  if (n_results) *n_results = total_k;
-  if (total_k > capacity)
-    throw Error(SBWT_E_CAPACITY, "results_capacity smaller than the k-mer count");
+  // host pointers: chunk the reads, double-buffer, overlap H2D/compute/D2H.
+  // Each chunk is planned (its last read by binary search over the cumulative
+  // ends, its k-mers and the ends' order checked over its own reads) while the
+  // previous one is on the GPU, and its results are only copied back once
+  // they fit the capacity.
   const u64 chunk_chars = cfg.chunk_chars ? cfg.chunk_chars : (64ULL << 20);
   const bool pinned = is_host_pinned(chars) && is_host_pinned(results) &&
                       is_host_pinned(read_ends);
-  struct Chunk {
-    u64 r0, r1, c0, c1, k0, nk;
-  };
-  std::vector<Chunk> chunks;
-  {
-    u64 r = 0, kacc = 0;
-    while (r < n_reads) {
-      Chunk ch{};
-      ch.r0 = r;
-      ch.c0 = r ? read_ends[r - 1] : 0;
-      ch.k0 = kacc;
-      u64 prev = ch.c0;
-      u64 nk = 0;
-      while (r < n_reads && (r == ch.r0 || read_ends[r] - ch.c0 <= chunk_chars)) {
-        const u64 len = read_ends[r] - prev;
-        if (len >= k) nk += len - k + 1;
-        prev = read_ends[r];
-        ++r;
-      }
-      ch.r1 = r;
-      ch.c1 = prev;
-      ch.nk = nk;
-      kacc += nk;
-      chunks.push_back(ch);
+  u64 r = 0, kacc = 0, prev_end = 0;
+  bool over = false, unordered = false;
+  for (size_t i = 0; r < n_reads; ++i) {
+    const u64 r0 = r, c0 = prev_end;
+    u64 r1 = (u64)(std::upper_bound(read_ends + r0, read_ends + n_reads, c0 + chunk_chars) -
+                   read_ends);
+    r1 = std::max(r1, r0 + 1);
+    u64 nk = 0, prev = c0;
+    for (u64 q = r0; q < r1 && !unordered; ++q) {
+      unordered = read_ends[q] < prev;
+      const u64 len = read_ends[q] - prev;
+      if (len >= k) nk += len - k + 1;
+      prev = read_ends[q];
     }
-  }
-  for (size_t i = 0; i < chunks.size(); ++i) {
-    const Chunk &ch = chunks[i];
+    if (unordered) break;  // reported once the chunks in flight are done
+    if (kacc + nk > capacity) {
+      over = true;
+      break;
+    }
     const int b = (int)(i & 1);
     cudaStream_t st = ws.streams[b];
-    const u64 nc = ch.c1 - ch.c0, nr = ch.r1 - ch.r0;
+    const u64 nc = prev - c0, nr = r1 - r0;
     ws.chars[b].ensure(nc + 16);
     ws.ends[b].ensure(nr * 8);
-    ws.results[b].ensure(std::max<u64>(ch.nk, 1) * 8);
-    const ReadsScratch sc = scratch_for(ws, b, nc, nr, ch.nk, tile_size(device, ch.nk, cfg));
-    SBWT_CUDA(cudaMemcpyAsync(ws.chars[b].get(), chars + ch.c0, nc,
+    ws.results[b].ensure(std::max<u64>(nk, 1) * 8);
+    const ReadsScratch sc = scratch_for(ws, b, nc, nr, nk, tile_size(device, nk, cfg));
+    SBWT_CUDA(cudaMemcpyAsync(ws.chars[b].get(), chars + c0, nc, cudaMemcpyHostToDevice, st));
+    SBWT_CUDA(cudaMemcpyAsync(ws.ends[b].get(), read_ends + r0, nr * 8,
                               cudaMemcpyHostToDevice, st));
-    SBWT_CUDA(cudaMemcpyAsync(ws.ends[b].get(), read_ends + ch.r0, nr * 8,
-                              cudaMemcpyHostToDevice, st));
-    launch_prepare(device, k, ws.chars[b].get<char>(), nc, ws.ends[b].get<u64>(), nr, ch.c0,
-                   sc, st);
-    launch_search(*this, nc, ws.ends[b].get<u64>(), nr, ch.c0, ch.nk, ws.results[b].get<u64>(),
-                  ch.nk, flags, cfg, sc, st);
-    if (ch.nk)
-      SBWT_CUDA(cudaMemcpyAsync(results + ch.k0, ws.results[b].get(), ch.nk * 8,
+    launch_prepare(device, k, ws.chars[b].get<char>(), nc, ws.ends[b].get<u64>(), nr, c0, sc,
+                   st);
+    launch_search(*this, nc, ws.ends[b].get<u64>(), nr, c0, nk, ws.results[b].get<u64>(), nk,
+                  flags, cfg, sc, st);
+    if (nk)
+      SBWT_CUDA(cudaMemcpyAsync(results + kacc, ws.results[b].get(), nk * 8,
                                 cudaMemcpyDeviceToHost, st));
     if (!pinned) SBWT_CUDA(cudaStreamSynchronize(st));
+    kacc += nk;
+    r = r1;
+    prev_end = prev;
   }
   for (auto &s : ws.streams) SBWT_CUDA(cudaStreamSynchronize(s));
+  if (unordered) throw Error(SBWT_E_INVALID, "read ends must be non-decreasing");
+  if (over) {
+    const u64 total_k = count_kmers_host(read_ends, n_reads, k, 0);
+    if (n_results) *n_results = total_k;
+    throw Error(SBWT_E_CAPACITY, "results_capacity smaller than the k-mer count");
+  }
+  if (n_results) *n_results = kacc;
   check_err_word(ws, ws.streams[0]);
 }
 

@@ -194,3 +194,32 @@ def test_deep_presearch_read_search_matches_oracle(p):
     assert np.array_equal(idx.search_reads(chars, ends), exp)
     with pytest.raises(S.SbwtError):
         S.SbwtIndex.open(path, presearch_letters=15)
+
+
+def test_host_chunks_capacity_and_order_errors():
+    """Host-pointer calls plan each chunk while the previous one runs: a too
+    small results buffer and out-of-order read ends in a later chunk are
+    still reported (after the chunks in flight finish), with the total k-mer
+    count on E_CAPACITY, and the next call is unaffected."""
+    import ctypes as C
+    g, path, sb = synthetic(4, 2, 4000, 31, 1, 0.02)
+    idx = S.SbwtIndex.open(path)
+    chars, ends = mixed_reads(g, 21, 3000)
+    exp = oracle_results(oracle_index(path, 8), chars, ends)
+    L = S.lib()
+    n_res = C.c_uint64()
+    S.set_launch_config(chunk_chars=4096)  # many chunks
+    try:
+        out = np.zeros(len(exp), np.uint64)
+        rc = L.sbwt_search_reads(idx._h, chars.ctypes.data, len(chars), ends.ctypes.data,
+                                 len(ends), out.ctypes.data, len(exp) - 1, C.byref(n_res), 0,
+                                 None)
+        assert rc == S.E_CAPACITY and n_res.value == len(exp)
+        bad = ends.copy()
+        bad[-5] = bad[-6] - 1  # decreasing near the end: a later chunk
+        rc = L.sbwt_search_reads(idx._h, chars.ctypes.data, len(chars), bad.ctypes.data,
+                                 len(bad), out.ctypes.data, len(out), C.byref(n_res), 0, None)
+        assert rc == S.E_INVALID
+        assert np.array_equal(idx.search_reads(chars, ends), exp)
+    finally:
+        S.set_launch_config()

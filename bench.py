@@ -860,7 +860,7 @@ def main():
                               "kmers_searched": n_searched,
                               "lane_steps_by_path": dict(zip(
                                   ["stream", "presearch", "walk", "group_scan",
-                                   "group_start", "probe"], [int(x) for x in ctr[8:14]])),
+                                   "kmer_table", "probe"], [int(x) for x in ctr[8:14]])),
                               "distinct_paths_per_iteration": int(ctr[14]) / max(n_iter, 1)},
                      "random_sector": rs},
         "cpu_baseline": cpu,

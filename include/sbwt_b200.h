@@ -170,6 +170,17 @@ int sbwt_build_index(const char *chars, uint64_t n_chars, const uint64_t *seq_en
                      uint64_t n_seqs, uint32_t k, int add_rc, const char *out_path,
                      int device, uint64_t *n_nodes);
 
+/* Builds (enable != 0; kept when already built) or drops the index's k-mer
+ * table: every k-mer of the SBWT (k <= 31) -> its node in an open-addressing
+ * hash table (16 bytes per slot, at most half full).  With it, a read k-mer
+ * that is not reached by a stream step from the previous k-mer costs one
+ * table lookup instead of the presearch lookup and the remaining search steps
+ * (src/IndexSearcher/IndexSearcher.cuh:43-59); results are identical.
+ * sbwt_index_open builds it when it fits (<= 32 GiB and a quarter of the
+ * free device memory).  *table_bytes (optional) receives its size, 0 when
+ * absent.  No counterpart in the reference. */
+int sbwt_index_set_kmer_table(sbwt_index_t *index, int enable, uint64_t *table_bytes);
+
 /* ------------------------------------------------------------------------ */
 /* Colors step                                                               */
 /* ------------------------------------------------------------------------ */
@@ -378,7 +389,7 @@ int sbwt_autotune(const sbwt_index_t *index, const char *d_chars,
  * mode): presearch lookups, rank-block sectors, suffix-group words, probe
  * iterations, warp iterations, lane load steps, k-mers written without a
  * search, k-mers searched, lane steps of each search path (stream step,
- * presearch of a new k-mer, walk, group scan, group-start check, probe),
+ * presearch of a new k-mer, walk, group scan, k-mer table lookup, probe),
  * distinct paths per warp iteration (summed), and one unused entry. */
 int sbwt_profile_read(double *search_ms, uint64_t *search_launches,
                       uint64_t *launches, uint64_t counters[16]);

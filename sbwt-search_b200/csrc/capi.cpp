@@ -183,6 +183,24 @@ uint64_t sbwt_colors_num_colors(const sbwt_colors_t *colors) {
   return colors ? colors->impl->num_colors : 0;
 }
 
+int sbwt_index_set_kmer_table(sbwt_index_t *index, int enable, uint64_t *table_bytes) {
+  if (!index) {
+    set_last_error("null index");
+    return SBWT_E_INVALID;
+  }
+  return guarded([&] {
+    IndexImpl &x = *index->impl;
+    if (!enable) {
+      x.drop_kmer_table();
+    } else if (!x.view.kmer_table) {
+      x.build_kmer_table();
+    }
+    x.device_bytes = x.presearch.size() + x.hot.size() + x.key_buf.size() + x.l0_all.size() +
+                     x.kmer_table.size();
+    if (table_bytes) *table_bytes = x.kmer_table.size();
+  });
+}
+
 int sbwt_colors_set_node_table(sbwt_colors_t *colors, int enable, int *built) {
   if (!colors) {
     set_last_error("null color index");

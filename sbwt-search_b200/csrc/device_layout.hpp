@@ -48,6 +48,8 @@ struct SbwtView {
   const uint64_t *presearch;  // pyramid of levels 1..presearch_max
   const uint64_t *suffix_group_starts;  // N bits or nullptr
   const uint64_t *key_marks;            // N bits or nullptr
+  const uint64_t *kmer_table;  // (key, node) slots, or nullptr
+  uint64_t kmer_table_mask;    // slots - 1
   uint64_t num_bits;
   uint32_t k;
   uint32_t p;      // presearch depth used by this call

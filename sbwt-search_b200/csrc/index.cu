@@ -399,7 +399,10 @@ __global__ void tile_reads_kernel(const uint64_t *kmer_off, uint64_t n_reads, ui
 //   M_SG     : suffix-group-start word u (bits <= ubit) below a failed stream
 //              step;
 //   M_PPRE   : probe, presearch entry of x[m..m+lvl);
-//   M_PROBE  : probe walk up to probe_end (nothing is emitted).
+//   M_PROBE  : probe walk up to probe_end (nothing is emitted);
+//   M_HASH   : k-mer table lookup of the k-mer at `slot` (k <= 31, when the
+//              index has the table): one 32-byte sector of two slots per
+//              step, u = the first slot of the pair.
 // Per-lane register window over the packed chars and invalid bits of a read:
 // words wbase and wbase + 1, i.e. chunk positions [32 wbase, 32 wbase + 64).
 // With k <= 33 every char the lane needs for the k-mer at pos (and for a probe
@@ -466,8 +469,9 @@ struct CharWindow {
 // (also the single step of a group start), the stream step from the previous
 // k-mer's node (an empty result sends the lane to the group scan), and the
 // walk of a probe (its end proves k-mers absent or not; nothing is emitted).
-enum : uint32_t { M_NEW = 0, M_SG = 1, M_PPRE = 2, M_WALK = 4, M_STREAM = 5, M_PROBE = 6 };
-enum : uint32_t { K_NONE = 0, K_BLOCK = 1, K_PRE = 2, K_SGW = 3 };
+enum : uint32_t { M_NEW = 0, M_SG = 1, M_PPRE = 2, M_HASH = 3, M_WALK = 4, M_STREAM = 5,
+                  M_PROBE = 6 };
+enum : uint32_t { K_NONE = 0, K_BLOCK = 1, K_PRE = 2, K_SGW = 3, K_HASH = 4 };
 // SBWTs with fewer nodes than this use 32-bit node arithmetic in the search.
 constexpr uint64_t kNarrowLimit = (uint64_t)kBlockBits << kSuperchunkShift;
 
@@ -673,6 +677,9 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
             l = rr = v;
             wi = pos + k - 1;
             mode = M_STREAM;
+          } else if (SMALLK && s.kmer_table) {  // one k-mer table lookup
+            u = (I)kmer_table_bucket(cw.prefix(pos, k), s.kmer_table_mask);
+            mode = M_HASH;
           } else {
             kind = K_PRE;
             pre_e = pre_off +
@@ -687,6 +694,8 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
         pb = rr + 1;
       } else if (mode == M_SG) {
         kind = K_SGW;
+      } else if (mode == M_HASH) {
+        kind = K_HASH;
       } else if (mode == M_PPRE) {  // pu = probe start m
         kind = K_PRE;
         pre_e = probe_off +
@@ -719,6 +728,8 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
       if (bb != ba) addrB = bc + bb;
     } else if (kind == K_PRE) {
       addrA = s.wide ? chunk_of(s.presearch, 2 * pre_e) : chunk_of(s.presearch, pre_e);
+    } else if (kind == K_HASH) {
+      addrA = reinterpret_cast<const Block *>(s.kmer_table + 2 * (uint64_t)u);
     } else if (kind == K_SGW) {
       addrA = chunk_of(s.suffix_group_starts, (uint64_t)u);
     }
@@ -727,19 +738,20 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
     B = A;
     if (addrB) B = load_block(addrB);
     if (COUNT) {
-      n_pre += kind == K_PRE;
+      n_pre += kind == K_PRE || kind == K_HASH;
       n_block += (kind == K_BLOCK) + (addrB != nullptr);
       n_sg += kind == K_SGW;
       n_probe += (mode == M_PPRE || mode == M_PROBE);
       n_iter += lane == 0;
       n_lane += kind != K_NONE;
       // phase-3 paths: stream step, presearch of a new k-mer, walk, group
-      // scan, group-start check, probe (presearch or walk)
+      // scan, k-mer table lookup, probe (presearch or walk)
       const uint32_t path = kind == K_NONE ? 6u
                             : mode == M_STREAM ? 0u
                             : mode == M_NEW ? 1u
                             : mode == M_WALK ? 2u
-                            : mode == M_SG ? 3u : 5u;
+                            : mode == M_SG ? 3u
+                            : mode == M_HASH ? 4u : 5u;
       if (path < 6) ++n_mode[path];
       const uint32_t seen = __reduce_or_sync(0xFFFFFFFFu, path < 6 ? 1u << path : 0u);
       n_distinct += lane == 0 ? __popc(seen) : 0;
@@ -819,6 +831,20 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
           wi = start;
           mode = probe ? M_PROBE : M_WALK;
         }
+      }
+    } else if (kind == K_HASH) {  // slots u, u + 1: (key, node) each
+      const uint64_t key = SMALLK ? cw.prefix(pos, k) : 0;
+      if (A.w0 == key) {
+        emit = (I)A.w1;
+        emitted = true;
+      } else if (A.w2 == key) {
+        emit = (I)A.w3;
+        emitted = true;
+      } else if (A.w0 == ~0ULL || A.w2 == ~0ULL) {  // an empty slot: absent
+        emit = NONE;
+        emitted = true;
+      } else {
+        u = (I)(((uint64_t)u + 2) & s.kmer_table_mask);
       }
     } else {  // M_SG: suffix-group starts at or below v, one word per step
       const uint64_t w = chunk_word(A, (uint64_t)u) & low_mask(ubit + 1);
@@ -1148,7 +1174,9 @@ IndexImpl::IndexImpl(const u64 *const acgt[4], u64 num_bits_, u32 k_,
     SBWT_CUDA(cudaGetLastError());
   }
   SBWT_CUDA(cudaDeviceSynchronize());
-  device_bytes = presearch.size() + hot.size() + key_buf.size() + l0_all.size();
+  build_kmer_table();
+  device_bytes = presearch.size() + hot.size() + key_buf.size() + l0_all.size() +
+                 kmer_table.size();
 }
 
 SbwtView IndexImpl::view_for(u32 p) const {
@@ -1281,7 +1309,7 @@ static void launch_search(const IndexImpl &ix, u64 n_chars, const u64 *d_ends, u
   rv.n_tiles = (n_kmers + rv.tile - 1) / rv.tile;
   rv.out = d_out;
   rv.out_capacity = out_capacity;
-  rv.probe_len = probe_length(ix.num_bits, ix.k, cfg);
+  rv.probe_len = ix.view.kmer_table ? 0 : probe_length(ix.num_bits, ix.k, cfg);
   rv.n_kmers_dev = nullptr;
   rv.queue = sc.queue;
   SBWT_CUDA(cudaMemsetAsync(sc.queue, 0, 8, st));
@@ -1341,7 +1369,7 @@ void enqueue_index_step(const IndexImpl &ix, const char *d_chars, u64 n_chars,
   rv.n_tiles = 0;  // computed on the device from the total
   rv.out = d_out;
   rv.out_capacity = out_capacity;
-  rv.probe_len = probe_length(ix.num_bits, ix.k, cfg);
+  rv.probe_len = ix.view.kmer_table ? 0 : probe_length(ix.num_bits, ix.k, cfg);
   rv.queue = sc.queue;
   tile_reads_kernel<<<grid_for(ix.device, n_reads, 256, 16), 256, 0, st>>>(
       sc.kmer_off, n_reads, rv.tile, sc.tile_read);
@@ -1616,7 +1644,7 @@ void IndexImpl::search_reads_noalloc(const char *d_chars, u64 n_chars, const u64
   rv.n_tiles = (n_k + rv.tile - 1) / rv.tile;
   rv.out = d_results;
   rv.out_capacity = capacity;
-  rv.probe_len = probe_length(num_bits, k, cfg);
+  rv.probe_len = view.kmer_table ? 0 : probe_length(num_bits, k, cfg);
   rv.queue = sc.queue;
   tile_reads_kernel<<<grid_for(device, n_reads, 256, 16), 256, 0, st>>>(sc.kmer_off, n_reads,
                                                                         rv.tile, sc.tile_read);
@@ -1665,7 +1693,7 @@ int sbwt_profile_enable(int enabled, int count_work) {
 // [2] suffix-group words, [3] probe iterations, [4] warp iterations, [5] lane
 // load steps, [6] k-mers written without a search (invalid or proven absent),
 // [7] k-mers searched, [8..13] lane steps of each phase-3 path (stream step,
-// presearch of a new k-mer, walk, group scan, group-start check, probe),
+// presearch of a new k-mer, walk, group scan, k-mer table lookup, probe),
 // [14] distinct paths per warp iteration, summed.  Resets the totals.
 int sbwt_profile_read(double *search_ms, uint64_t *search_launches,
                       uint64_t *launches, uint64_t counters[16]) {

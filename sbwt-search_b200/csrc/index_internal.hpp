@@ -12,6 +12,8 @@ namespace sbwt {
 // Deepest presearch table (4^14 entries: 2 GiB at 8 bytes per entry, 2.9 GB
 // with the shallower levels); the reference fixes 12.
 constexpr uint32_t kPresearchMaxLetters = 14;
+// Largest k-mer table an index builds (16 bytes per slot, <= 2 slots per k-mer).
+constexpr u64 kKmerTableMaxBytes = 32ULL << 30;
 
 struct LaunchConfig {
   uint32_t presearch_letters = 0;  // <= the handle's pyramid depth
@@ -27,6 +29,9 @@ struct IndexImpl {
             const u64 *key_marks, int device, unsigned presearch_letters);
 
   SbwtView view_for(u32 p) const;
+  // k-mer -> node hash table (k <= 31): false when not built
+  bool build_kmer_table();
+  void drop_kmer_table();
 
   void search_positions(const u64 *bit_seqs, u64 n_words, const u64 *positions,
                         u64 n, u64 *results, u32 flags, cudaStream_t st,
@@ -48,7 +53,8 @@ struct IndexImpl {
   u64 device_bytes = 0;
   SbwtView view{};
   DeviceBuffer hot;  // rank blocks of A/C/G/T + suffix-group words, contiguous
-  DeviceBuffer l0_all, presearch, key_buf;
+  DeviceBuffer l0_all, presearch, key_buf, kmer_table;
+  u64 table_kmers = 0;
   u64 window_bytes = 0;   // L2 access-policy window over `hot`
 };
 

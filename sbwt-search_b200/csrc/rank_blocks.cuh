@@ -50,6 +50,16 @@ __device__ __forceinline__ uint64_t block_of(uint64_t i) {
   return (uint64_t)((uint32_t)(i >> 6) / 3u);
 }
 
+// First slot of a key's probe sequence in the k-mer table (an even slot, so
+// that one 32-byte sector holds the first two slots probed); the mixer is the
+// SplitMix64 finalizer (Steele, Lea, Flood 2014).
+__device__ __forceinline__ uint64_t kmer_table_bucket(uint64_t z, uint64_t mask) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  z ^= z >> 31;
+  return z & mask & ~1ULL;
+}
+
 // rank_c(i): ones of vector c in [0, i), i in [0, N].
 __device__ __forceinline__ uint64_t rank_full(const SbwtView &s, uint32_t c,
                                               uint64_t i) {

@@ -68,6 +68,7 @@ def lib():
         L.sbwt_index_free.argtypes = [vp]
         L.sbwt_index_free.restype = None
         L.sbwt_index_get_info.argtypes = [vp, C.POINTER(IndexInfo)]
+        L.sbwt_index_set_kmer_table.argtypes = [vp, C.c_int, C.POINTER(u64)]
         L.sbwt_search_positions.argtypes = [vp, vp, u64, vp, u64, vp, u32, vp]
         L.sbwt_count_kmers.argtypes = [vp, u64, u32]
         L.sbwt_count_kmers.restype = u64
@@ -229,6 +230,16 @@ class SbwtIndex:
     def count_kmers(self, read_ends: np.ndarray) -> int:
         read_ends = np.ascontiguousarray(read_ends, dtype=np.uint64)
         return int(lib().sbwt_count_kmers(_ptr(read_ends), len(read_ends), self.k))
+
+    def set_kmer_table(self, enable: bool) -> int:
+        """Builds (kept when present) or drops the k-mer -> node table (same
+        results either way); returns its size in bytes, 0 when absent."""
+        nb = C.c_uint64(0)
+        check(lib().sbwt_index_set_kmer_table(self._h, int(enable), C.byref(nb)))
+        info = IndexInfo()
+        check(lib().sbwt_index_get_info(self._h, C.byref(info)))
+        self.device_bytes = info.device_bytes
+        return nb.value
 
     def search_reads(self, chars, read_ends, out=None, move_to_key_kmer: bool = False,
                      per_kmer_walk: bool = False, stream: int = 0):

@@ -20,7 +20,9 @@ def golden_index():
 
 @pytest.mark.parametrize("name", FIXTURE_FILES)
 @pytest.mark.parametrize("per_kmer", [False, True])
-def test_reads_reproduce_reference_fixture(golden_index, name, per_kmer):
+@pytest.mark.parametrize("table", [True, False])
+def test_reads_reproduce_reference_fixture(golden_index, name, per_kmer, table):
+    assert (golden_index.set_kmer_table(table) > 0) == table
     reads = O.parse_fastx((GOLDEN / "index_search" / name).read_bytes())
     chars = b"".join(reads)
     ends = np.cumsum([len(r) for r in reads]).astype(np.uint64)
@@ -52,9 +54,11 @@ def test_positions_seam_matches_oracle_and_reference(p):
 
 @pytest.mark.parametrize("per_kmer", [False, True])
 @pytest.mark.parametrize("seed", [11, 12])
-def test_reads_match_oracle(per_kmer, seed):
+@pytest.mark.parametrize("table", [True, False])
+def test_reads_match_oracle(per_kmer, seed, table):
     g, path, sb = synthetic(7, 4, 6000, 31, 2, 0.02)
     idx = S.SbwtIndex.open(path)
+    assert (idx.set_kmer_table(table) > 0) == table
     chars, ends = mixed_reads(g, seed, 2000, median=90, sigma=0.8, len_min=0,
                               len_max=500, sub=0.01, n_rate=0.01)
     got = idx.search_reads(chars, ends, per_kmer_walk=per_kmer)
@@ -75,9 +79,11 @@ def test_reads_small_k_and_no_suffix_groups():
     assert np.array_equal(idx2.search_reads(chars, ends), exp)
 
 
-def test_edge_cases_empty_short_invalid():
+@pytest.mark.parametrize("table", [True, False])
+def test_edge_cases_empty_short_invalid(table):
     g, path, sb = synthetic(4, 2, 4000, 31, 1, 0.02)
     idx = S.SbwtIndex.open(path)
+    idx.set_kmer_table(table)
     gen = g.seq(0)
     reads = [b"", b"ACGT", gen[:31], gen[100:130], b"N" * 40, gen[:31].lower(),
              gen[500:700] + b"X" + gen[700:900], b"", gen[1000:1031]]
@@ -135,6 +141,7 @@ def test_absent_prefix_probe_is_exact(probe):
     for every probe length (0 = automatic, 0xFFFFFFFF = off)."""
     g, path, sb = synthetic(7, 4, 6000, 31, 2, 0.02)
     idx = S.SbwtIndex.open(path)
+    idx.set_kmer_table(False)  # the probe only runs on the search-walk path
     chars, ends = mixed_reads(g, 77, 3000, median=150, sigma=0.5, len_min=20,
                               len_max=600, sub=0.03, n_rate=0.005)
     exp = oracle_results(oracle_index(path, 8), chars, ends)
@@ -148,7 +155,8 @@ def test_absent_prefix_probe_is_exact(probe):
 
 
 @pytest.mark.parametrize("d", [2, 7])
-def test_move_to_key_kmer_matches_oracle_and_reference(d):
+@pytest.mark.parametrize("table", [True, False])
+def test_move_to_key_kmer_matches_oracle_and_reference(d, table):
     """The d > 1 forward walk to the next key k-mer (reference flag -k)."""
     from helpers import key_marks_for
     g, path, sb = synthetic(9, 2, 3000, 31, 1, 0.02)
@@ -156,6 +164,7 @@ def test_move_to_key_kmer_matches_oracle_and_reference(d):
     keys = key_marks_for(oi, d, seed=d)
     idx = S.SbwtIndex.from_arrays(sb.acgt, sb.num_bits, sb.k, sb.suffix_group_starts,
                                   key_kmer_marks=keys)
+    idx.set_kmer_table(table)
     chars, ends = mixed_reads(g, 13, 800, sub=0.01, n_rate=0.003)
     exp = np.concatenate(O.index_search_reads(oi, T.split_reads(chars, ends), keys))
     assert np.array_equal(idx.search_reads(chars, ends, move_to_key_kmer=True), exp)
@@ -223,3 +232,19 @@ def test_host_chunks_capacity_and_order_errors():
         assert np.array_equal(idx.search_reads(chars, ends), exp)
     finally:
         S.set_launch_config()
+
+
+@pytest.mark.parametrize("k", [3, 15, 31])
+def test_kmer_table_on_and_off(k):
+    """The k-mer table (k <= 31) and the search walk give the oracle's results;
+    the table can be dropped and rebuilt."""
+    g, path, sb = synthetic(12, 2, 5000, k, 1, 0.02)
+    idx = S.SbwtIndex.open(path)
+    assert idx.set_kmer_table(True) > 0
+    chars, ends = mixed_reads(g, 14, 600, median=80, sigma=0.5, len_min=0, len_max=300)
+    exp = oracle_results(oracle_index(path, min(8, k)), chars, ends)
+    assert np.array_equal(idx.search_reads(chars, ends), exp)
+    assert idx.set_kmer_table(False) == 0
+    assert np.array_equal(idx.search_reads(chars, ends), exp)
+    assert idx.set_kmer_table(True) > 0
+    assert np.array_equal(idx.search_reads(chars, ends, per_kmer_walk=True), exp)

@@ -371,19 +371,23 @@ def random_sector_peak(S, dev, ws_bytes):
 
 def index_working_sets(idx):
     """Bytes the read search touches at random: the rank blocks of the four
-    vectors plus the suffix-group-start words (every step), and the presearch
-    level it reads (one lookup per full search)."""
+    vectors plus the suffix-group-start words (every step), and the table it
+    starts a k-mer from (one lookup per k-mer not reached by a stream step):
+    the k-mer table when the index has one, else the presearch level."""
     n = idx.num_bits
     hot = 4 * (n // 192 + 1) * 32 + (n + 63) // 64 * 8
+    table = idx.set_kmer_table(True)  # its size (kept when present)
+    if table:
+        return hot, table
     entry = 8 if n < (1 << 32) else 16
-    pre = (4 ** idx.presearch_letters) * entry
-    return hot, pre
+    return hot, (4 ** idx.presearch_letters) * entry
 
 
 def sector_roofline(S, dev, idx, n_hot, n_pre, kernel_s):
     """Random-sector roofline of the read search: the time the kernel's
     sectors take at the measured random-gather rate of their own working set
-    (rank blocks + group words; the presearch level), over the kernel time."""
+    (rank blocks + group words; the k-mer table or presearch level), over the
+    kernel time."""
     hot_b, pre_b = index_working_sets(idx)
     r_hot = random_sector_peak(S, dev, hot_b)
     r_pre = random_sector_peak(S, dev, pre_b)
@@ -392,7 +396,7 @@ def sector_roofline(S, dev, idx, n_hot, n_pre, kernel_s):
             "achieved_gsectors_s": (n_hot + n_pre) / kernel_s / 1e9,
             "hot": {"sectors": int(n_hot), "working_set_bytes": int(hot_b),
                     "peak_gsectors_s": r_hot / 1e9},
-            "presearch": {"sectors": int(n_pre), "working_set_bytes": int(pre_b),
+            "lookup": {"sectors": int(n_pre), "working_set_bytes": int(pre_b),
                           "peak_gsectors_s": r_pre / 1e9},
             "peak_source": "sbwt_measure_random_sectors over buffers of each working set's "
                            "size, best of 4/8 chains"}

@@ -1309,7 +1309,7 @@ static void launch_search(const IndexImpl &ix, u64 n_chars, const u64 *d_ends, u
   rv.n_tiles = (n_kmers + rv.tile - 1) / rv.tile;
   rv.out = d_out;
   rv.out_capacity = out_capacity;
-  rv.probe_len = ix.view.kmer_table ? 0 : probe_length(ix.num_bits, ix.k, cfg);
+  rv.probe_len = probe_length(ix.num_bits, ix.k, cfg);
   rv.n_kmers_dev = nullptr;
   rv.queue = sc.queue;
   SBWT_CUDA(cudaMemsetAsync(sc.queue, 0, 8, st));
@@ -1369,7 +1369,7 @@ void enqueue_index_step(const IndexImpl &ix, const char *d_chars, u64 n_chars,
   rv.n_tiles = 0;  // computed on the device from the total
   rv.out = d_out;
   rv.out_capacity = out_capacity;
-  rv.probe_len = ix.view.kmer_table ? 0 : probe_length(ix.num_bits, ix.k, cfg);
+  rv.probe_len = probe_length(ix.num_bits, ix.k, cfg);
   rv.queue = sc.queue;
   tile_reads_kernel<<<grid_for(ix.device, n_reads, 256, 16), 256, 0, st>>>(
       sc.kmer_off, n_reads, rv.tile, sc.tile_read);
@@ -1644,7 +1644,7 @@ void IndexImpl::search_reads_noalloc(const char *d_chars, u64 n_chars, const u64
   rv.n_tiles = (n_k + rv.tile - 1) / rv.tile;
   rv.out = d_results;
   rv.out_capacity = capacity;
-  rv.probe_len = view.kmer_table ? 0 : probe_length(num_bits, k, cfg);
+  rv.probe_len = probe_length(num_bits, k, cfg);
   rv.queue = sc.queue;
   tile_reads_kernel<<<grid_for(device, n_reads, 256, 16), 256, 0, st>>>(sc.kmer_off, n_reads,
                                                                         rv.tile, sc.tile_read);

@@ -2,9 +2,11 @@
 // in an open-addressing hash table on the device.  It extends the presearch
 // idea (a table lookup replaces the first p search steps) to the whole
 // k-mer: a read k-mer that cannot be reached by a stream step from the
-// previous k-mer costs one table lookup instead of a presearch lookup, k - p
-// backward-search steps and the absent-prefix probe.  Results are identical:
-// the table holds exactly the k-mers of the SBWT with their nodes.
+// previous k-mer costs one table lookup instead of a presearch lookup and
+// k - p backward-search steps.  (A failed stream step still starts the
+// absent-prefix probe, which proves a run of the following k-mers absent
+// with one presearch lookup.)  Results are identical: the table holds exactly
+// the k-mers of the SBWT with their nodes.
 //
 // Labels are recovered from the SBWT itself: the last char of node v is the
 // c with C[c] <= v < C[c + 1] (node 0 is the root, all '$'), and its

@@ -170,6 +170,15 @@ int sbwt_build_index(const char *chars, uint64_t n_chars, const uint64_t *seq_en
                      uint64_t n_seqs, uint32_t k, int add_rc, const char *out_path,
                      int device, uint64_t *n_nodes);
 
+/* Builds a plain-matrix SBWT of every k-mer of the genomes and a Themisto
+ * "sdsl-hybrid-v4" .tcolors color index on `device`: the color set of a k-mer
+ * is the set of genomes holding it (either strand when add_rc), every k-mer is
+ * a key k-mer (d = 1), sets are deduplicated and a set is dense iff its size
+ * exceeds n_genomes / 64.  Both files are byte-identical to the project's
+ * host builder's.  The reference loads these files (built by Themisto). */
+int sbwt_build_colored_index(const char *chars, uint64_t n_chars, const uint64_t *genome_ends,
+                             uint64_t n_genomes, uint32_t k, int add_rc, const char *sbwt_path,
+                             const char *tcolors_path, int device, uint64_t *n_nodes);
 /* Builds (enable != 0; kept when already built) or drops the index's k-mer
  * table: every k-mer of the SBWT (k <= 31) -> its node in an open-addressing
  * hash table (16 bytes per slot, at most half full).  With it, a read k-mer

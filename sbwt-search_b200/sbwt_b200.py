@@ -109,6 +109,8 @@ def lib():
                                        C.POINTER(u64), u32, C.c_int, vp]
         L.sbwt_build_index.argtypes = [vp, u64, vp, u64, u32, C.c_int, C.c_char_p, C.c_int,
                                        C.POINTER(u64)]
+        L.sbwt_build_colored_index.argtypes = [vp, u64, vp, u64, u32, C.c_int, C.c_char_p,
+                                               C.c_char_p, C.c_int, C.POINTER(u64)]
         L.sbwt_format_index_results.argtypes = [vp, vp, u64, u32, C.c_int, vp, u64,
                                                 C.POINTER(u64), u32, C.c_int, vp]
         L.sbwt_format_color_results.argtypes = [vp, vp, u64, u64, C.c_int, vp, u64,
@@ -564,4 +566,18 @@ def build_index(seqs, k: int, out_path, add_rc: bool = True, device: int = 0) ->
     check(lib().sbwt_build_index(_ptr(chars) if len(chars) else None, len(chars),
                                  _ptr(ends) if len(ends) else None, len(ends), k, int(add_rc),
                                  str(out_path).encode(), device, C.byref(nn)))
+    return nn.value
+
+
+def build_colored_index(chars, genome_ends, k: int, sbwt_path, tcolors_path,
+                        add_rc: bool = True, device: int = 0) -> int:
+    """SBWT + .tcolors of genomes (chars back to back, cumulative ends) built
+    on the GPU; returns the node count."""
+    chars = _np_chars(chars)
+    ends = np.ascontiguousarray(genome_ends, dtype=np.uint64)
+    nn = C.c_uint64()
+    check(lib().sbwt_build_colored_index(_ptr(chars) if len(chars) else None, len(chars),
+                                         _ptr(ends), len(ends), k, int(add_rc),
+                                         str(sbwt_path).encode(), str(tcolors_path).encode(),
+                                         device, C.byref(nn)))
     return nn.value

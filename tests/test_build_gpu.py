@@ -53,3 +53,18 @@ def test_gpu_built_index_searches_like_the_oracle(tmp_path):
 def test_k_above_31_is_rejected(tmp_path):
     with pytest.raises(S.SbwtError):
         S.build_index([b"ACGT" * 20], 32, tmp_path / "x.sbwt")
+
+
+@pytest.mark.parametrize("n,length,founders,k,rc", [(12, 3000, 3, 31, True),
+                                                    (150, 800, 6, 31, True),
+                                                    (3000, 120, 12, 21, False)])
+def test_gpu_colored_builder_matches_host_builder(n, length, founders, k, rc, tmp_path):
+    # sets of every kind: singletons, sparse lists, dense rows (n > 64)
+    g = T.gen_genomes(n + k, n, length, founders, 0.01, 0.05, 0.001)
+    hs, hc = tmp_path / "h.sbwt", tmp_path / "h.tcolors"
+    ds, dc = tmp_path / "d.sbwt", tmp_path / "d.tcolors"
+    nh = T.build_colored(g, k, str(hs), str(hc), add_rc=rc)
+    nd = S.build_colored_index(g.chars, np.cumsum(g.lens).astype(np.uint64), k, ds, dc, rc)
+    assert nd == nh
+    assert ds.read_bytes() == hs.read_bytes()
+    assert dc.read_bytes() == hc.read_bytes()

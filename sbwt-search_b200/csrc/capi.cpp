@@ -271,13 +271,14 @@ int sbwt_search_reads_noalloc(const sbwt_index_t *index, const char *d_chars,
 int sbwt_set_launch_config(uint32_t presearch_letters, uint32_t blocks_per_sm,
                            uint64_t tile, uint64_t chunk_chars) {
   LaunchConfig &c = default_launch_config();
-  const uint32_t probe = c.probe_len, l2w = c.l2_window;
+  const uint32_t probe = c.probe_len, l2w = c.l2_window, tk = c.table_kernel;
   c.presearch_letters = presearch_letters;
   c.blocks_per_sm = blocks_per_sm ? blocks_per_sm : 8;
   c.tile = tile;
   c.chunk_chars = chunk_chars;
   c.probe_len = probe;
   c.l2_window = l2w;
+  c.table_kernel = tk;
   return SBWT_OK;
 }
 
@@ -292,6 +293,13 @@ int sbwt_set_l2_window(int enabled) {
 // (0 = automatic, 0xFFFFFFFF = off).  Results do not depend on it.
 int sbwt_set_probe_length(uint32_t probe_len) {
   default_launch_config().probe_len = probe_len;
+  return SBWT_OK;
+}
+
+// Tuning hook: 1 runs the read search of an index with a k-mer table on the
+// table kernel, 0 on the general kernel.  Results do not depend on it.
+int sbwt_set_table_kernel(int enabled) {
+  default_launch_config().table_kernel = enabled ? 1u : 0u;
   return SBWT_OK;
 }
 

@@ -902,6 +902,251 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
   }
 }
 
+// Read search for the common configuration: the index has its k-mer table
+// (k <= 31) and suffix-group words, fewer than 192 * 2^24 nodes (32-bit node
+// arithmetic), no key-k-mer walk.  The same tiles, work queue and result
+// rules as search_reads_kernel, with three single-sector operations only:
+//   T_STREAM : the k-mer follows a found k-mer v: bit c of v (c = the new
+//              last char).  Set: the node is C[c] + rank_c(v) (v starts its
+//              suffix group, where edge bits live).  Clear: the group scan.
+//   T_SG     : highest suffix-group start g <= v, one 64-bit word per load;
+//              g == v means no edge c (not found), else T_STEP at g.
+//   T_STEP   : bit c of g: C[c] + rank_c(g), or not found.
+//   T_HASH   : any other k-mer: its k-mer table pair of slots.
+// A step on the single-node interval [x, x] is nonempty iff bit c of x is
+// set (rank_c(x + 1) - rank_c(x) = bit), so one rank block answers it.  No
+// presearch walk and no absent-prefix probe: every k-mer the stream cannot
+// reach is one table lookup.  Keeping the lane state to these four modes
+// keeps the per-iteration instruction count low (the general kernel is
+// issue-bound on its state machine).
+enum : uint32_t { T_NEW = 0, T_STREAM = 1, T_STEP = 2, T_SG = 3, T_HASH = 4 };
+
+#ifndef SBWT_TABLE_MIN_BLOCKS
+#define SBWT_TABLE_MIN_BLOCKS 5  // 256-thread blocks per SM the register budget targets
+#endif
+
+template <bool COUNT>
+__global__ void __launch_bounds__(256, SBWT_TABLE_MIN_BLOCKS)
+    search_table_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
+                        unsigned long long *counters) {
+  using I = uint32_t;
+  constexpr I NONE = ~I(0);
+  __shared__ uint32_t sh_cmap[4];
+  if (threadIdx.x < 4) sh_cmap[threadIdx.x] = (uint32_t)s.c_map[threadIdx.x];
+  __syncthreads();
+  const uint32_t k = s.k;
+  const uint32_t lane = threadIdx.x & 31;
+  const I n_kmers = (I)(rv.n_kmers_dev ? *rv.n_kmers_dev : rv.n_kmers);
+  const I tsize = (I)rv.tile;
+  const I n_tiles = (n_kmers + tsize - 1) / tsize;
+  const I base = (I)rv.base;
+  const I out_cap = (I)min(rv.out_capacity, (uint64_t)NONE);
+  uint64_t n_table = 0, n_block = 0, n_sg = 0, n_iter = 0, n_lane = 0, n_known = 0,
+           n_searched = 0, n_distinct = 0, n_stream = 0, n_step = 0;
+  bool exhausted = false;  // the work queue is empty for this lane
+  bool done = false;
+  I slot = 0, slot_end = 0, r = 0, r_next = 0, pos = 0;
+  I last_inv1 = 0;  // 1 + last invalid char position (0 = none)
+  I v = NONE;       // node of the previous k-mer of this read
+  I x = 0;          // node of a step, or the word of the group scan
+  uint32_t mode = T_NEW, ubit = 63;
+  uint64_t key = 0, hslot = 0;
+  CharWin<I> cw;
+  cw.init();
+  while (true) {
+    // ---- work queue (warp-collective), as in search_reads_kernel
+    __syncwarp();
+    const bool need = !exhausted && mode == T_NEW && slot >= slot_end;
+    const unsigned need_mask = __ballot_sync(0xFFFFFFFFu, need);
+    I new_tile = NONE;
+    if (need_mask) {
+      const int leader = __ffs(need_mask) - 1;
+      unsigned long long qb = 0;
+      if ((int)lane == leader) qb = atomicAdd(rv.queue, (unsigned long long)__popc(need_mask));
+      qb = __shfl_sync(0xFFFFFFFFu, qb, leader);
+      if (need) {
+        const unsigned long long t = qb + __popc(need_mask & ((1u << lane) - 1u));
+        if (t >= (unsigned long long)n_tiles) {
+          exhausted = true;
+        } else {
+          new_tile = (I)t;
+        }
+      }
+    }
+    // ---- phase 1 (per lane): the next k-mer and its load address
+    I run_slot = 0;
+    uint32_t run_n = 0;
+    const Block *addr = nullptr;
+    uint32_t c = 0;
+    if (!done) {
+      if (mode == T_NEW) {
+        bool ready = false;
+        while (true) {
+          if (slot >= slot_end) {  // next tile
+            if (new_tile == NONE) {
+              done = exhausted;
+              break;
+            }
+            slot = new_tile * tsize;
+            new_tile = NONE;
+            slot_end = min(slot + tsize, n_kmers);
+            r = (I)__ldg(tile_read + slot / tsize);
+            r_next = (I)__ldg(rv.kmer_off + r + 1);
+            pos = (r ? (I)__ldg(rv.ends + r - 1) : base) - base +
+                  (slot - (I)__ldg(rv.kmer_off + r));
+            cw.move_to(rv.packed, rv.invalid, pos);
+            last_inv1 = cw.last_invalid1(pos, pos + k - 1);
+            v = NONE;
+          } else if (slot == r_next) {  // next read
+            do {
+              r_next = (I)__ldg(rv.kmer_off + (++r) + 1);
+            } while (r_next == slot);
+            pos = (I)__ldg(rv.ends + r - 1) - base;
+            cw.move_to(rv.packed, rv.invalid, pos);
+            last_inv1 = cw.last_invalid1(pos, pos + k - 1);
+            v = NONE;
+          }
+          const I newc = pos + k - 1;
+          cw.move_to(rv.packed, rv.invalid, pos);
+          if (cw.invalid_at(newc)) last_inv1 = newc + 1;
+          if (last_inv1 <= pos) {
+            ready = true;
+            break;
+          }
+          if (run_n) break;  // one run per iteration
+          // k-mers pos .. last_inv1 - 1 all hold the invalid char at
+          // last_inv1 - 1: a run of -2 up to the read / tile end, written
+          // by the warp below
+          const I n = min(last_inv1 - pos, min(r_next, slot_end) - slot);
+          run_slot = slot;
+          run_n = (uint32_t)n;
+          if (COUNT) n_known += n;
+          v = NONE;
+          slot += n;
+          pos += n;
+          if (slot < min(r_next, slot_end)) {
+            cw.move_to(rv.packed, rv.invalid, pos);
+            last_inv1 = cw.last_invalid1(pos, pos + k - 1);
+          }
+        }
+        if (ready) {
+          if (v != NONE) {
+            x = v;
+            mode = T_STREAM;
+          } else {
+            key = cw.prefix(pos, k);
+            hslot = kmer_table_bucket(key, s.kmer_table_mask);
+            mode = T_HASH;
+          }
+        }
+      }
+      if (mode == T_STREAM || mode == T_STEP) {
+        c = cw.char_at(pos + k - 1);
+        addr = s.blocks0 + (uint64_t)c * s.block_stride + block_idx(x);
+      } else if (mode == T_HASH) {
+        addr = reinterpret_cast<const Block *>(s.kmer_table + 2 * hslot);
+      } else if (mode == T_SG) {
+        addr = chunk_of(s.suffix_group_starts, (uint64_t)x);
+      }
+    }
+    // ---- runs of -2 (converged): the warp writes each lane's run
+    for (unsigned runs = __ballot_sync(0xFFFFFFFFu, run_n != 0); runs; runs &= runs - 1) {
+      const int q = __ffs(runs) - 1;
+      const I q_slot = __shfl_sync(0xFFFFFFFFu, run_slot, q);
+      const uint32_t q_n = __shfl_sync(0xFFFFFFFFu, run_n, q);
+      for (uint32_t j = lane; j < q_n; j += 32)
+        if (q_slot + j < out_cap) __stcs(rv.out + q_slot + j, (unsigned long long)SBWT_INVALID);
+    }
+    if (__all_sync(0xFFFFFFFFu, done)) break;
+    // ---- phase 2 (converged): one 32-byte load per active lane
+    Block A = Block{0, 0, 0, 0};
+    if (addr) A = load_block(addr);
+    if (COUNT) {
+      n_iter += lane == 0;
+      n_lane += addr != nullptr;
+      const uint32_t path = addr == nullptr ? 0u : 1u << mode;
+      if (addr) {
+        n_table += mode == T_HASH;
+        n_block += mode == T_STREAM || mode == T_STEP;
+        n_sg += mode == T_SG;
+        n_stream += mode == T_STREAM;
+        n_step += mode == T_STEP;
+      }
+      const uint32_t seen = __reduce_or_sync(0xFFFFFFFFu, path);
+      n_distinct += lane == 0 ? __popc(seen) : 0;
+    }
+    if (addr == nullptr) continue;
+    // ---- phase 3 (per lane)
+    I emit = NONE;
+    bool emitted = false;
+    if (mode == T_HASH) {  // slots hslot, hslot + 1: (key, node) each
+      if (A.w0 == key) {
+        emit = (I)A.w1;
+        emitted = true;
+      } else if (A.w2 == key) {
+        emit = (I)A.w3;
+        emitted = true;
+      } else if (A.w0 == ~0ULL || A.w2 == ~0ULL) {  // an empty slot: absent
+        emitted = true;
+      } else {
+        hslot = (hslot + 2) & s.kmer_table_mask;
+      }
+    } else if (mode == T_SG) {  // group starts at or below v in word x
+      const uint64_t w = chunk_word(A, (uint64_t)x) & low_mask(ubit + 1);
+      if (w) {
+        const I g = x * 64 + 63 - (I)__clzll(w);
+        if (g == v) {
+          emitted = true;  // v starts its group and has no edge c
+        } else {
+          x = g;
+          mode = T_STEP;
+        }
+      } else if (x == 0) {
+        emitted = true;  // no group start below v: malformed SBWT
+      } else {
+        --x;
+        ubit = 63;
+      }
+    } else {  // a step on [x, x] with the k-mer's last char
+      const uint32_t q = x - block_idx(x) * kBlockBits;
+      if (block_bit(A, q)) {
+        emit = sh_cmap[c] + (I)block_rank(A, q);
+        emitted = true;
+      } else if (mode == T_STREAM) {  // no edge at v itself: v's group start
+        ubit = x & 63;
+        x >>= 6;
+        mode = T_SG;
+      } else {
+        emitted = true;
+      }
+    }
+    if (emitted) {
+      if (COUNT) ++n_searched;
+      v = emit;
+      if (slot < out_cap)
+        __stcs(rv.out + slot,
+               (unsigned long long)(emit == NONE ? SBWT_NOT_FOUND : (uint64_t)emit));
+      ++slot;
+      ++pos;
+      mode = T_NEW;
+    }
+  }
+  if (COUNT) {
+    atomicAdd(counters + 0, (unsigned long long)n_table);
+    atomicAdd(counters + 1, (unsigned long long)n_block);
+    atomicAdd(counters + 2, (unsigned long long)n_sg);
+    atomicAdd(counters + 4, (unsigned long long)n_iter);
+    atomicAdd(counters + 5, (unsigned long long)n_lane);
+    atomicAdd(counters + 6, (unsigned long long)n_known);
+    atomicAdd(counters + 7, (unsigned long long)n_searched);
+    atomicAdd(counters + 8, (unsigned long long)n_stream);   // stream steps
+    atomicAdd(counters + 10, (unsigned long long)n_step);    // steps at a group start
+    atomicAdd(counters + 11, (unsigned long long)n_sg);      // group scan words
+    atomicAdd(counters + 12, (unsigned long long)n_table);   // table lookups
+    atomicAdd(counters + 14, (unsigned long long)n_distinct);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -966,7 +1211,7 @@ static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStrea
 static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsView &rv,
                                  const uint64_t *tile_read, uint32_t mtk, uint32_t *d_err,
                                  int grid, int threads, cudaStream_t st,
-                                 const LaunchAttrs &la) {
+                                 const LaunchAttrs &la, bool table_kernel) {
   Profile &p = profile();
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -988,6 +1233,8 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
   }
   const bool small = sv.k <= 33;
   const bool narrow = sv.num_bits < kNarrowLimit && rv.n_kmers_bound < (1ULL << 32);
+  const bool table = table_kernel && stream && narrow && sv.kmer_table && sv.k <= 31 &&
+                     mtk == 0 && sv.suffix_group_starts;
 #define SBWT_LAUNCH(S_, C_, K_)                                                          \
   do {                                                                                   \
     if (narrow)                                                                          \
@@ -997,7 +1244,12 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
       launch_ex(search_reads_kernel<S_, C_, K_, uint64_t>, grid, threads, st, la, sv, rv, \
                 tile_read, mtk, d_err, ctr);                                             \
   } while (0)
-  if (ctr) {
+  if (table) {
+    if (ctr)
+      launch_ex(search_table_kernel<true>, grid, threads, st, la, sv, rv, tile_read, ctr);
+    else
+      launch_ex(search_table_kernel<false>, grid, threads, st, la, sv, rv, tile_read, ctr);
+  } else if (ctr) {
     if (stream) {
       if (small) SBWT_LAUNCH(true, true, true); else SBWT_LAUNCH(true, true, false);
     } else {
@@ -1336,7 +1588,8 @@ static void launch_search(const IndexImpl &ix, u64 n_chars, const u64 *d_ends, u
   }
   launch_search_kernel(stream, sv, rv, sc.tile_read, mtk, sc.err, grid, threads, st,
                        persist ? search_attrs(ix.hot.get(), ix.window_bytes, persist)
-                               : LaunchAttrs{});
+                               : LaunchAttrs{},
+                       cfg.table_kernel != 0);
 }
 
 // The index step of one device-resident batch without any host
@@ -1378,7 +1631,7 @@ void enqueue_index_step(const IndexImpl &ix, const char *d_chars, u64 n_chars,
   const bool stream = !(flags & SBWT_PER_KMER_WALK) && ix.view.suffix_group_starts;
   const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
   launch_search_kernel(stream, sv, rv, sc.tile_read, mtk, sc.err, grid, 256, st,
-                       LaunchAttrs{});
+                       LaunchAttrs{}, cfg.table_kernel != 0);
   note_launches(1);
 }
 

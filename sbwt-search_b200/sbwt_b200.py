@@ -152,6 +152,12 @@ def set_probe_length(probe_len: int = 0) -> None:
     check(lib().sbwt_set_probe_length(probe_len))
 
 
+def set_table_kernel(enabled: bool = True) -> None:
+    """True: an index with a k-mer table runs the read search on the table
+    kernel; False: on the general kernel.  Results never depend on it."""
+    check(lib().sbwt_set_table_kernel(int(enabled)))
+
+
 def set_l2_window(enabled: bool = True) -> None:
     check(lib().sbwt_set_l2_window(int(enabled)))
 

@@ -12,6 +12,9 @@ from helpers import FIXTURE_FILES, GOLDEN, golden_sbwt_path, synthetic, oracle_i
 
 pytestmark = pytest.mark.gpu
 
+# the library's default choice of read search kernel for indexes with a k-mer table
+DEFAULT_TABLE_KERNEL = False
+
 
 @pytest.fixture(scope="module")
 def golden_index():
@@ -248,3 +251,50 @@ def test_kmer_table_on_and_off(k):
     assert np.array_equal(idx.search_reads(chars, ends), exp)
     assert idx.set_kmer_table(True) > 0
     assert np.array_equal(idx.search_reads(chars, ends, per_kmer_walk=True), exp)
+
+
+@pytest.mark.parametrize("kernel", [True, False])
+@pytest.mark.parametrize("seed", [21, 22])
+@pytest.mark.parametrize("k", [3, 15, 31])
+def test_table_kernel_and_general_kernel_match_oracle(kernel, seed, k):
+    """With a k-mer table the read search runs on the table kernel (stream
+    steps, group scans and table lookups only) or on the general kernel;
+    both give the oracle's results on reads with errors, N, empty and short
+    reads, at several tile sizes (k-mers of one read split across tiles)."""
+    g, path, sb = synthetic(30 + seed, 3, 5000, k, 2, 0.02)
+    idx = S.SbwtIndex.open(path)
+    assert idx.set_kmer_table(True) > 0
+    chars, ends = mixed_reads(g, seed, 1500, median=70, sigma=0.8, len_min=0, len_max=400,
+                              sub=0.01, n_rate=0.01)
+    exp = oracle_results(oracle_index(path, min(8, k)), chars, ends)
+    S.set_table_kernel(kernel)
+    try:
+        for tile in (0, 16, 100, 5000):
+            S.set_launch_config(tile=tile)
+            assert np.array_equal(idx.search_reads(chars, ends), exp), tile
+    finally:
+        S.set_table_kernel(DEFAULT_TABLE_KERNEL)
+        S.set_launch_config()
+
+
+def test_table_kernel_device_pointers_and_capacity():
+    """The table kernel through device pointers: exact, and it writes no slot
+    past the k-mer count (the guard slots keep their fill)."""
+    import torch
+    g, path, sb = synthetic(31, 3, 5000, 31, 2, 0.02)
+    idx = S.SbwtIndex.open(path)
+    assert idx.set_kmer_table(True) > 0
+    chars, ends = mixed_reads(g, 23, 3000, median=120, sigma=0.6, len_min=0, len_max=600,
+                              sub=0.005, n_rate=0.002)
+    exp = oracle_results(oracle_index(path, 8), chars, ends)
+    d_chars = torch.from_numpy(chars.copy()).cuda()
+    d_ends = torch.from_numpy(ends.view(np.int64).copy()).cuda()
+    out = torch.full((len(exp) + 64,), -7, dtype=torch.int64, device="cuda")
+    S.set_table_kernel(True)
+    try:
+        assert idx.search_reads(d_chars, d_ends, out=out) == len(exp)
+    finally:
+        S.set_table_kernel(DEFAULT_TABLE_KERNEL)
+    got = out.cpu().numpy()
+    assert np.array_equal(got[:len(exp)].view(np.uint64), exp)
+    assert (got[len(exp):] == -7).all()

@@ -285,11 +285,16 @@ def parse():
     return ap.parse_args()
 
 
-def profiled_traffic_per_kmer():
+def profile_file(kernel: str) -> Path:
+    """The committed ncu summary of `kernel` on the 1 M-read case."""
+    return REPO / "profiles" / f"{kernel}_100Mbp_1Mreads_full.md"
+
+
+def profiled_traffic_per_kmer(kernel: str):
     """DRAM bytes (read + write) per k-mer of the search kernel from the
     committed ncu capture of the 1 M-read case; traffic grows with the k-mers
     processed, so it scales to a full launch by the k-mer count."""
-    p = REPO / "profiles" / "search_reads_kernel_100Mbp_1Mreads_full.md"
+    p = profile_file(kernel)
     try:
         for ln in p.read_text().splitlines():
             if ln.startswith("traffic_bytes_per_kmer:"):
@@ -795,12 +800,15 @@ def main():
     peak, peak_kind = load_peaks()
     kern_ms = search_ms.value / max(1, search_launches.value)
     # algorithmic bytes per launch (what this kernel's algorithm must move):
-    # one 32-byte sector per presearch entry, per rank block and per
-    # suffix-group word the search reads; 8 B result per k-mer; 2 bits of
+    # one 32-byte sector per k-mer-table or presearch lookup, per rank block
+    # and per suffix-group word the search reads; 8 B result per k-mer; 2 bits of
     # packed input + 1 invalid bit per char.
     alg_bytes = ((n_pre + n_block + n_sg) * 32 + n_kmers * 8 + n_chars / 4 + n_chars / 8)
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9
-    traffic_pk = profiled_traffic_per_kmer()
+    # the read search runs on the table kernel when the index has its k-mer
+    # table (k <= 31, the library default), else on the general kernel
+    kernel = "search_table_kernel" if idx.set_kmer_table(True) else "search_reads_kernel"
+    traffic_pk = profiled_traffic_per_kmer(kernel)
     try:
         rs = sector_roofline(S, dev, idx, n_block + n_sg, n_pre, kern_ms / 1e3)
     except Exception as e:  # reported as unmeasured, never hides the headline
@@ -865,10 +873,11 @@ def main():
                      "frac": achieved / peak,
                      "traffic": (None if traffic_pk is None else traffic_pk * n_kmers),
                      "traffic_source": "ncu capture of the 1 M-read case scaled by k-mers "
-                                       "(profiles/search_reads_kernel_100Mbp_1Mreads_full.md)",
-                     "peak_kind": peak_kind, "kernel": "search_reads_kernel",
+                                       f"({profile_file(kernel).relative_to(REPO)})",
+                     "peak_kind": peak_kind, "kernel": kernel,
                      "kernel_ms": kern_ms,
-                     "work": {"presearch_lookups": n_pre, "rank_block_sectors": n_block,
+                     "work": {"table_or_presearch_lookups": n_pre,
+                              "rank_block_sectors": n_block,
                               "suffix_group_words": n_sg, "probe_iterations": n_probe,
                               "bytes_per_kmer": alg_bytes / n_kmers,
                               "warp_iterations": n_iter,

@@ -371,8 +371,9 @@ int sbwt_set_launch_config(uint32_t presearch_letters, uint32_t blocks_per_sm,
  * 0xFFFFFFFF = off).  Results never depend on it. */
 int sbwt_set_probe_length(uint32_t probe_len);
 /* Read search kernel of an index with a k-mer table (k <= 31, fewer than
- * 192 * 2^24 nodes, no SBWT_MOVE_TO_KEY_KMER): 1 = the table kernel (stream
- * steps, group scans and table lookups only), 0 = the general kernel (table
+ * 192 * 2^24 nodes, no SBWT_MOVE_TO_KEY_KMER): 1 = the table kernel (the
+ * default: stream steps, group scans and table lookups only, with L2
+ * eviction priorities on its loads), 0 = the general kernel (table
  * lookups plus presearch walks and absent-prefix probes).  Results never
  * depend on it. */
 int sbwt_set_table_kernel(int enabled);

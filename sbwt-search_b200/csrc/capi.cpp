@@ -296,8 +296,9 @@ int sbwt_set_probe_length(uint32_t probe_len) {
   return SBWT_OK;
 }
 
-// Tuning hook: 1 runs the read search of an index with a k-mer table on the
-// table kernel, 0 on the general kernel.  Results do not depend on it.
+// Tuning hook: 1 (the default) runs the read search of an index with a k-mer
+// table on the table kernel, 0 on the general kernel.  Results do not depend
+// on it.
 int sbwt_set_table_kernel(int enabled) {
   default_launch_config().table_kernel = enabled ? 1u : 0u;
   return SBWT_OK;

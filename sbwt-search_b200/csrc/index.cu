@@ -918,7 +918,9 @@ __global__ void __launch_bounds__(256, SBWT_SEARCH_MIN_BLOCKS)
 // presearch walk and no absent-prefix probe: every k-mer the stream cannot
 // reach is one table lookup.  Keeping the lane state to these four modes
 // keeps the per-iteration instruction count low (the general kernel is
-// issue-bound on its state machine).
+// issue-bound on its state machine); the kernel then waits on its sectors,
+// so the loads carry L2 eviction priorities that keep the rank blocks and
+// group words resident against the table lookups and the result stream.
 enum : uint32_t { T_NEW = 0, T_STREAM = 1, T_STEP = 2, T_SG = 3, T_HASH = 4 };
 
 #ifndef SBWT_TABLE_MIN_BLOCKS
@@ -951,6 +953,9 @@ __global__ void __launch_bounds__(256, SBWT_TABLE_MIN_BLOCKS)
   I x = 0;          // node of a step, or the word of the group scan
   uint32_t mode = T_NEW, ubit = 63;
   uint64_t key = 0, hslot = 0;
+  // rank blocks and group words (every step, ~32 bytes per 192 nodes per
+  // char) stay in L2; table lines (one random lookup each) leave first
+  const uint64_t pol_last = l2_policy_evict_last(), pol_first = l2_policy_evict_first();
   CharWin<I> cw;
   cw.init();
   while (true) {
@@ -1060,7 +1065,7 @@ __global__ void __launch_bounds__(256, SBWT_TABLE_MIN_BLOCKS)
     if (__all_sync(0xFFFFFFFFu, done)) break;
     // ---- phase 2 (converged): one 32-byte load per active lane
     Block A = Block{0, 0, 0, 0};
-    if (addr) A = load_block(addr);
+    if (addr) A = load_block_hint(addr, mode == T_HASH ? pol_first : pol_last);
     if (COUNT) {
       n_iter += lane == 0;
       n_lane += addr != nullptr;

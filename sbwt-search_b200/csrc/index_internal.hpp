@@ -22,7 +22,7 @@ struct LaunchConfig {
   uint64_t chunk_chars = 0;        // host-pointer path: chars per chunk
   uint32_t probe_len = 0;          // absent-prefix probe length (0 = auto, ~0u = off)
   uint32_t l2_window = 0;          // persisting L2 window over the index's hot data
-  uint32_t table_kernel = 0;       // k-mer-table read search kernel where it applies
+  uint32_t table_kernel = 1;       // k-mer-table read search kernel where it applies
 };
 
 struct IndexImpl {

@@ -16,6 +16,32 @@ __device__ __forceinline__ Block load_block(const Block *p) {
   return b;
 }
 
+// L2 eviction-priority policies (createpolicy, sm_80+) for loads that give
+// one: evict_last keeps a small working set that every step hits resident in
+// L2 while large random or streaming traffic passes through; evict_first
+// marks lines that are read once (random lookups in a table much larger
+// than L2).
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+// load_block with an L2 eviction policy and no L1 allocation (random sectors
+// see no L1 reuse).
+__device__ __forceinline__ Block load_block_hint(const Block *p, uint64_t policy) {
+  Block b;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u64 {%0,%1,%2,%3}, [%4], %5;"
+      : "=l"(b.w0), "=l"(b.w1), "=l"(b.w2), "=l"(b.w3)
+      : "l"(p), "l"(policy));
+  return b;
+}
+
 __device__ __forceinline__ unsigned long long low_mask(uint32_t t) {
   // bits [0, t) set, t in [0, 64]
   return t >= 64 ? ~0ULL : ((1ULL << t) - 1ULL);

@@ -153,8 +153,9 @@ def set_probe_length(probe_len: int = 0) -> None:
 
 
 def set_table_kernel(enabled: bool = True) -> None:
-    """True: an index with a k-mer table runs the read search on the table
-    kernel; False: on the general kernel.  Results never depend on it."""
+    """True (the default): an index with a k-mer table runs the read search
+    on the table kernel; False: on the general kernel.  Results never depend
+    on it."""
     check(lib().sbwt_set_table_kernel(int(enabled)))
 
 

@@ -13,7 +13,7 @@ from helpers import FIXTURE_FILES, GOLDEN, golden_sbwt_path, synthetic, oracle_i
 pytestmark = pytest.mark.gpu
 
 # the library's default choice of read search kernel for indexes with a k-mer table
-DEFAULT_TABLE_KERNEL = False
+DEFAULT_TABLE_KERNEL = True
 
 
 @pytest.fixture(scope="module")

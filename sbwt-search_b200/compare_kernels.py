@@ -1,7 +1,7 @@
 """Times the two read search kernels on the index workload and checks that
 their outputs are equal.
 
-    python sbwt-search_b200/compare_kernels.py [--reads N]
+    python sbwt-search_b200/compare_kernels.py [--reads N] [--lib PATH]
 
 Builds the 100 Mbp index workload of bench.py (first N reads, default 10 M),
 opens the index (k-mer table included), and for the general kernel and then
@@ -26,11 +26,15 @@ sys.path.insert(0, str(HERE))
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reads", type=int, default=10_000_000)
+    ap.add_argument("--lib", default=None,
+                    help="another build of libsbwt_b200.so (default: _build/)")
     args = ap.parse_args()
     import numpy as np
     import torch
     import bench
     import sbwt_b200 as S
+    if args.lib:
+        S.LIB_PATH = Path(args.lib).resolve()
     L = S.lib()
     L.sbwt_profile_enable.argtypes = [C.c_int, C.c_int]
     L.sbwt_profile_read.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -40,7 +44,7 @@ def main() -> None:
     n_k = idx.count_kmers(ends)
     d_chars = torch.from_numpy(chars).cuda()
     d_ends = torch.from_numpy(ends.view(np.int64)).cuda()
-    outs, res = {}, {"kmers": n_k}
+    outs, res = {}, {"kmers": n_k, "lib": str(S.LIB_PATH)}
     for name, tk in (("general", False), ("table", True)):
         S.set_table_kernel(tk)
         out = torch.empty(n_k, dtype=torch.int64, device="cuda")

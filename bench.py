@@ -866,8 +866,9 @@ def main():
                    "chars_per_gpu": n_chars, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (no flush needed)",
                    "presearch_letters": idx.presearch_letters,
-                   "launch": "library defaults (an autotuned sample of 64 M chars picked "
-                             "tile 64, 6% slower on the whole batch)"},
+                   "launch": "library defaults: the k-mer table kernel (k <= 31), grid of "
+                             "8 x 256-thread blocks per SM (5 resident), tiles of "
+                             "k-mers / (resident threads x 8)"},
         "gpu_launches": int(launches.value),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,

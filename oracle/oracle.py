@@ -81,7 +81,8 @@ def lib():
 
 
 def ref_lib():
-    """SBWT-Search's own index kernels compiled for the host (or None)."""
+    """SBWT-Search's own index and colors kernels compiled for the host (or
+    None when oracle/_ref was not built)."""
     global _ref
     if _ref is None:
         if not REF_SO.exists():
@@ -96,6 +97,11 @@ def ref_lib():
                                  U64P, U64P, U64P, U64P, C.c_void_p, C.c_uint64,
                                  U64P, C.c_int]
         L.ref_max_threads.restype = C.c_int
+        L.ref_color_counts.argtypes = [
+            U64P, C.c_uint64, U64P, U64P, U64P, U64P, C.c_uint32, U64P, U64P, U64P,
+            U64P, U64P, C.c_uint32, U64P, C.c_uint32, U64P, C.c_uint32, C.c_uint64,
+            U64P, C.c_uint64, U64P, C.c_int]
+        L.ref_color_counts.restype = C.c_int
         _ref = L
     return _ref
 
@@ -488,6 +494,92 @@ class OracleColors:
             return rows, counts[:n_reads * self.tc.num_colors].reshape(
                 n_reads, self.tc.num_colors)
         return rows
+
+
+class RefColors:
+    """A parsed .tcolors index (see ColorsFile) prepared for the reference's
+    own colors kernels built for the host (oracle/ref_colors.cpp): Poppy
+    layers from the reference's PoppyBuilder, arrays padded as the
+    reference's GpuColorIndexContainer pads them (one extra word)."""
+
+    def __init__(self, tc):
+        L = ref_lib()
+        if L is None:
+            raise RuntimeError("reference CPU build missing: run `make -C oracle ref`")
+        self.tc = tc
+        self.keep = []
+
+        def poppy(bits, nbits):
+            n0, n12 = C.c_uint64(), C.c_uint64()
+            L.ref_poppy_sizes(nbits, C.byref(n0), C.byref(n12))
+            b = np.zeros(((nbits + 255) // 256) * 4 + 4, np.uint64)
+            b[:len(bits)] = bits
+            l0 = np.zeros(n0.value, np.uint64)
+            l12 = np.zeros(n12.value, np.uint64)
+            L.ref_poppy_build(_p(b), nbits, _p(l0), _p(l12))
+            self.keep += [b, l0, l12]
+            return b, l0, l12
+
+        self.is_dense = poppy(tc.is_dense_marks, tc.is_dense_bits)
+        self.key = poppy(tc.key_kmer_marks, tc.key_kmer_bits)
+        self.dense_arrays, self.dense_intervals, self.sparse_arrays, \
+            self.sparse_intervals, self.color_set_idxs = (
+                _pad(tc.dense_arrays), _pad(tc.dense_intervals), _pad(tc.sparse_arrays),
+                _pad(tc.sparse_intervals), _pad(tc.color_set_idxs))
+
+    def color_counts(self, warped: np.ndarray, warp_intervals: np.ndarray,
+                     threads: int | None = None) -> np.ndarray:
+        """Counts of the reference's d_color_search + d_post_process over one
+        batch: warped indexes (found indexes only, each read's count a
+        multiple of 32) and the warps before each read (n_reads + 1 entries).
+        Returns a (n_reads, num_colors) u64 array."""
+        L = ref_lib()
+        tc = self.tc
+        warped = np.ascontiguousarray(warped, np.uint64)
+        wi = np.ascontiguousarray(warp_intervals, np.uint64)
+        n_reads = len(wi) - 1
+        counts = np.zeros(max(1, n_reads * tc.num_colors), np.uint64)
+        if len(warped) == 0:
+            return counts[:0].reshape(0, tc.num_colors)
+        rc = L.ref_color_counts(
+            _p(warped), len(warped), _p(self.key[0]), _p(self.key[1]), _p(self.key[2]),
+            _p(self.color_set_idxs), tc.color_set_idxs_width, _p(self.is_dense[0]),
+            _p(self.is_dense[1]), _p(self.is_dense[2]), _p(self.dense_arrays),
+            _p(self.dense_intervals), tc.dense_intervals_width, _p(self.sparse_arrays),
+            tc.sparse_arrays_width, _p(self.sparse_intervals), tc.sparse_intervals_width,
+            tc.num_colors, _p(wi), n_reads, _p(counts), threads or L.ref_max_threads())
+        if rc != 0:
+            raise ValueError("reference color kernel: a warp held padding lanes")
+        return counts[:n_reads * tc.num_colors].reshape(n_reads, tc.num_colors)
+
+
+def padding_free_batch(found_lists, batch_multiple: int = 1024):
+    """Trims per-read found-index lists so that the reference's colors kernel
+    sees no padding lane: every kept read keeps a positive multiple of 32 of
+    its found indexes (reads with fewer than 32 are dropped), and the batch
+    total is a multiple of batch_multiple (the reference pads its batch to
+    1024 with -1, ColorSearcher.cpp:68-78).  Returns (kept read numbers,
+    trimmed lists, warped indexes, warp intervals)."""
+    lists = [np.asarray(x, np.uint64)[: (len(x) // 32) * 32] for x in found_lists]
+    keep = [i for i, x in enumerate(lists) if len(x) >= 32]
+    lists = [lists[i] for i in keep]
+    total = sum(len(x) for x in lists)
+    excess = total % batch_multiple
+    j = len(lists) - 1
+    while excess and j >= 0:  # take whole warps off the longest-tail reads
+        can = min(excess, len(lists[j]) - 32)
+        if can > 0:
+            lists[j] = lists[j][:len(lists[j]) - can]
+            excess -= can
+        j -= 1
+    while excess and lists:  # drop whole reads from the end
+        excess = (excess - len(lists[-1])) % batch_multiple
+        lists.pop()
+        keep.pop()
+    warped = np.concatenate(lists) if lists else np.zeros(0, np.uint64)
+    wi = np.zeros(len(lists) + 1, np.uint64)
+    wi[1:] = np.cumsum([len(x) // 32 for x in lists])
+    return keep, lists, warped, wi
 
 
 def threshold_minimum(seq_size: int, tau: float) -> int:

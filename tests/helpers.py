@@ -157,3 +157,49 @@ def host_fastx(text: bytes, path) -> tuple[bytes, np.ndarray]:
     L.sbwt_free(ch)
     L.sbwt_free(en)
     return chars, ends
+
+
+def small_sbwt(seqs: list[bytes], k: int, add_rc: bool = True):
+    """A plain-matrix SBWT of the k-mers of seqs (any k), built by brute force
+    from the definition, for indexes the project's builder does not make
+    (k > 31).  Nodes are the k-mers plus, for every k-mer x without a
+    predecessor, the dummies $^(k-i) x[0..i) (i < k); nodes are in colex
+    order ($ < A < C < G < T, last char first); the first node of each suffix
+    group (nodes sharing their last k-1 chars) carries bit c iff its last
+    k-1 chars followed by c is a node.  Returns (acgt words, suffix-group-start
+    words, number of nodes, number of k-mers)."""
+    comp = bytes.maketrans(b"ACGT", b"TGCA")
+    kmers = set()
+    for s in seqs:
+        s = s.upper()
+        strands = [s, s.translate(comp)[::-1]] if add_rc else [s]
+        for t in strands:
+            for i in range(len(t) - k + 1):
+                x = t[i:i + k]
+                if all(ch in b"ACGT" for ch in x):
+                    kmers.add(x.decode())
+    nodes = set(kmers)
+    for x in kmers:
+        if not any(c + x[:-1] in kmers for c in "ACGT"):
+            for i in range(k):
+                nodes.add("$" * (k - i) + x[:i])
+    order = str.maketrans("$ACGT", "01234")
+    ordered = sorted(nodes, key=lambda x: x.translate(order)[::-1])
+    n = len(ordered)
+    bits = np.zeros((4, n), np.uint8)
+    sg = np.zeros(n, np.uint8)
+    prev = None
+    for i, x in enumerate(ordered):
+        if x[1:] != prev:
+            sg[i] = 1
+            prev = x[1:]
+            for ci, c in enumerate("ACGT"):
+                if x[1:] + c in nodes:
+                    bits[ci, i] = 1
+
+    def words(b):
+        w = np.packbits(b, bitorder="little")
+        w = np.concatenate([w, np.zeros((-len(w)) % 8, np.uint8)])
+        return w.view(np.uint64).copy()
+
+    return [words(bits[c]) for c in range(4)], words(sg), n, len(kmers)

@@ -277,11 +277,13 @@ def parse():
     ap.add_argument("--reads", type=int, default=CFG["n_reads"])
     ap.add_argument("--presearch", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--cpu-sample-reads", type=int, default=60_000)
+    ap.add_argument("--cpu-sample-reads", type=int, default=500_000)
     ap.add_argument("--index-only", action="store_true",
                     help="skip the batched, colors and serving sections")
     ap.add_argument("--colors-reads", type=int, default=CFG3["n_reads"])
     ap.add_argument("--serve-seconds", type=float, default=3.0)
+    ap.add_argument("--write-workload", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--seed-reads", type=int, default=1000, help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -369,6 +371,48 @@ def make_workload(seed_reads: int, n_reads: int, tmpdir: str):
                               c["len_sigma"], c["len_min"], c["len_max"],
                               c["read_sub"], c["n_rate"])
     return g, path, nodes, chars, ends
+
+
+def kmer_count(ends: np.ndarray, k: int) -> int:
+    lens = np.diff(np.concatenate([[0], ends.astype(np.int64)]))
+    return int(np.maximum(lens - k + 1, 0).sum())
+
+
+def index_config(args, world: int, nodes: int, n_kmers: int, n_chars: int) -> dict:
+    """The `config` of the index-search line, the same for both arms."""
+    return {"workload": "index search: 100 Mbp reference (40 x 2.5 Mbp genomes "
+                        "from 4 founders, 2% subs, 0.1% indels), k=31, both strands; "
+                        f"{args.reads} reads log-normal length (median 150, 31-1000), "
+                        "0.5% subs, 0.1% N", "k": CFG["k"], "nodes": int(nodes),
+            "reads_per_gpu": args.reads, "kmers_per_gpu": int(n_kmers),
+            "chars_per_gpu": int(n_chars), "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (no flush needed)"}
+
+
+def workload_files(seed_reads: int, n_reads: int, sample_reads: int, tmpdir: str):
+    """The index workload for the reference arm, made in a child process (the
+    project's generator and builder stay out of the reference arm's process):
+    the .sbwt path and the first `sample_reads` reads (chars, ends)."""
+    subprocess.run([sys.executable, str(Path(__file__).resolve()), "--write-workload", tmpdir,
+                    "--reads", str(n_reads), "--cpu-sample-reads", str(sample_reads),
+                    "--seed-reads", str(seed_reads)], check=True)
+    chars = np.load(os.path.join(tmpdir, "sample_chars.npy"))
+    ends = np.load(os.path.join(tmpdir, "sample_ends.npy"))
+    with open(os.path.join(tmpdir, "meta.json")) as f:
+        meta = json.load(f)
+    return os.path.join(tmpdir, "cfg2.sbwt"), chars, ends, meta
+
+
+def write_workload(args):
+    """Child side of workload_files."""
+    g, path, nodes, chars, ends = make_workload(args.seed_reads, args.reads,
+                                                args.write_workload)
+    n = min(args.cpu_sample_reads, len(ends))
+    np.save(os.path.join(args.write_workload, "sample_chars.npy"), chars[:int(ends[n - 1])])
+    np.save(os.path.join(args.write_workload, "sample_ends.npy"), ends[:n])
+    with open(os.path.join(args.write_workload, "meta.json"), "w") as f:
+        json.dump({"nodes": int(nodes), "kmers": kmer_count(ends, CFG["k"]),
+                   "chars": int(ends[-1])}, f)
 
 
 def random_sector_peak(S, dev, ws_bytes):
@@ -672,7 +716,8 @@ def run_reference(args, world, rank, local, pg):
     if rank != 0:
         return
     with tempfile.TemporaryDirectory() as d:
-        g, path, nodes, chars, ends = make_workload(1000 + rank, args.reads, d)
+        path, chars, ends, meta = workload_files(1000 + rank, args.reads,
+                                                 args.cpu_sample_reads, d)
         times, last = [], None
         for i in range(args.warmup + args.steps):
             r = cpu_reference_rate(path, chars, ends, CFG["k"], args.cpu_sample_reads)
@@ -689,10 +734,9 @@ def run_reference(args, world, rank, local, pg):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": med * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "u64", "data": "synthetic (seeded)", "impl": "reference",
-                "config": {"workload": "index search, 100 Mbp reference x 10M reads "
-                           "(bounded sample per step)", "k": CFG["k"],
-                           "sample_reads": args.cpu_sample_reads},
+                "dtype": "u64", "data": "synthetic (seeded; generated at start-up)", "impl": "reference",
+                "config": index_config(args, world, meta["nodes"], meta["kmers"],
+                                       meta["chars"]),
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
                                  "kind": "reference",
                                  "sample": f"first {args.cpu_sample_reads} reads "
@@ -704,6 +748,9 @@ def run_reference(args, world, rank, local, pg):
 
 def main():
     args = parse()
+    if args.write_workload:
+        write_workload(args)
+        return
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank, local, pg)
@@ -858,17 +905,11 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u64", "data": "synthetic (seeded; generated at start-up)",
-        "config": {"workload": "index search: 100 Mbp reference (40 x 2.5 Mbp genomes "
-                   "from 4 founders, 2% subs, 0.1% indels), k=31, both strands; "
-                   f"{args.reads} reads log-normal length (median 150, 31-1000), "
-                   "0.5% subs, 0.1% N", "k": CFG["k"], "nodes": nodes,
-                   "reads_per_gpu": args.reads, "kmers_per_gpu": n_kmers,
-                   "chars_per_gpu": n_chars, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (no flush needed)",
-                   "presearch_letters": idx.presearch_letters,
-                   "launch": "library defaults: the k-mer table kernel (k <= 31), grid of "
-                             "8 x 256-thread blocks per SM (5 resident), tiles of "
-                             "k-mers / (resident threads x 8)"},
+        "config": index_config(args, world, nodes, n_kmers, n_chars),
+        "launch": {"presearch_letters": idx.presearch_letters,
+                   "kernels": "library defaults: the k-mer table kernel (k <= 31), grid of "
+                              "8 x 256-thread blocks per SM (5 resident), tiles of "
+                              "k-mers / (resident threads x 8)"},
         "gpu_launches": int(launches.value),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,

@@ -277,11 +277,15 @@ def parse():
     ap.add_argument("--reads", type=int, default=CFG["n_reads"])
     ap.add_argument("--presearch", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--cpu-sample-reads", type=int, default=500_000)
     ap.add_argument("--index-only", action="store_true",
                     help="skip the batched, colors and serving sections")
     ap.add_argument("--colors-reads", type=int, default=CFG3["n_reads"])
     ap.add_argument("--serve-seconds", type=float, default=3.0)
+    ap.add_argument("--kernel", type=int, default=-1,
+                    help="read search kernel with a k-mer table (sbwt_set_table_kernel): "
+                         "0 general, 1 table, 2..5 walks variants, -1 library default")
     ap.add_argument("--write-workload", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--seed-reads", type=int, default=1000, help=argparse.SUPPRESS)
     return ap.parse_args()
@@ -431,37 +435,55 @@ def random_sector_peak(S, dev, ws_bytes):
     return best
 
 
+KERNELS = {0: "search_reads_kernel", 1: "search_table_kernel", 2: "search_walks_kernel",
+           3: "search_walks_kernel", 4: "search_walks_kernel", 5: "search_walks_kernel"}
+DEFAULT_KERNEL_MODE = 3
+
+
+def search_kernel_name(idx, mode: int) -> str:
+    """The read search kernel that runs for `mode` (sbwt_set_table_kernel) on
+    an index: without a k-mer table always the general kernel."""
+    mode = DEFAULT_KERNEL_MODE if mode < 0 else mode
+    return KERNELS[mode] if idx.set_kmer_table(True) else KERNELS[0]
+
+
 def index_working_sets(idx):
     """Bytes the read search touches at random: the rank blocks of the four
-    vectors plus the suffix-group-start words (every step), and the table it
+    vectors plus the suffix-group-start words (every step); the table it
     starts a k-mer from (one lookup per k-mer not reached by a stream step):
-    the k-mer table when the index has one, else the presearch level."""
+    the k-mer table when the index has one, else the presearch level; and
+    the k-mer filter in front of the table (10 bits per k-mer)."""
     n = idx.num_bits
     hot = 4 * (n // 192 + 1) * 32 + (n + 63) // 64 * 8
     table = idx.set_kmer_table(True)  # its size (kept when present)
     if table:
-        return hot, table
+        return hot, table, idx.filter_bytes()
     entry = 8 if n < (1 << 32) else 16
-    return hot, (4 ** idx.presearch_letters) * entry
+    return hot, (4 ** idx.presearch_letters) * entry, 0
 
 
-def sector_roofline(S, dev, idx, n_hot, n_pre, kernel_s):
+def sector_roofline(S, dev, idx, n_hot, n_pre, kernel_s, n_filter=0):
     """Random-sector roofline of the read search: the time the kernel's
     sectors take at the measured random-gather rate of their own working set
-    (rank blocks + group words; the k-mer table or presearch level), over the
-    kernel time."""
-    hot_b, pre_b = index_working_sets(idx)
+    (rank blocks + group words; the k-mer table or presearch level; the
+    k-mer filter), over the kernel time."""
+    hot_b, pre_b, filt_b = index_working_sets(idx)
     r_hot = random_sector_peak(S, dev, hot_b)
     r_pre = random_sector_peak(S, dev, pre_b)
-    t_min = n_hot / r_hot + n_pre / r_pre
-    return {"frac": t_min / kernel_s, "t_min_ms": t_min * 1e3, "kernel_ms": kernel_s * 1e3,
-            "achieved_gsectors_s": (n_hot + n_pre) / kernel_s / 1e9,
-            "hot": {"sectors": int(n_hot), "working_set_bytes": int(hot_b),
-                    "peak_gsectors_s": r_hot / 1e9},
-            "lookup": {"sectors": int(n_pre), "working_set_bytes": int(pre_b),
-                          "peak_gsectors_s": r_pre / 1e9},
-            "peak_source": "sbwt_measure_random_sectors over buffers of each working set's "
-                           "size, best of 4/8 chains"}
+    r_filt = random_sector_peak(S, dev, filt_b) if (filt_b and n_filter) else 0.0
+    t_min = n_hot / r_hot + n_pre / r_pre + (n_filter / r_filt if r_filt else 0.0)
+    out = {"frac": t_min / kernel_s, "t_min_ms": t_min * 1e3, "kernel_ms": kernel_s * 1e3,
+           "achieved_gsectors_s": (n_hot + n_pre + n_filter) / kernel_s / 1e9,
+           "hot": {"sectors": int(n_hot), "working_set_bytes": int(hot_b),
+                   "peak_gsectors_s": r_hot / 1e9},
+           "lookup": {"sectors": int(n_pre), "working_set_bytes": int(pre_b),
+                      "peak_gsectors_s": r_pre / 1e9},
+           "peak_source": "sbwt_measure_random_sectors over buffers of each working set's "
+                          "size, best of 4/8 chains"}
+    if n_filter:
+        out["filter"] = {"sectors": int(n_filter), "working_set_bytes": int(filt_b),
+                         "peak_gsectors_s": r_filt / 1e9}
+    return out
 
 
 def bench_cfg1(args, S, torch, dev, tmpdir):
@@ -493,7 +515,9 @@ def bench_cfg1(args, S, torch, dev, tmpdir):
     ctr = (C.c_uint64 * 16)()
     L.sbwt_profile_read(None, None, None, ctr)
     L.sbwt_profile_enable(0, 0)
-    sectors = int(ctr[0]) + int(ctr[1]) + int(ctr[2])
+    kernel = search_kernel_name(idx, args.kernel)
+    n_filter = int(ctr[3]) if kernel == "search_walks_kernel" else 0
+    sectors = int(ctr[0]) + int(ctr[1]) + int(ctr[2]) + n_filter
     for _ in range(max(3, args.warmup)):
         step()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
@@ -518,8 +542,9 @@ def bench_cfg1(args, S, torch, dev, tmpdir):
            "found_frac": float((out_h >= 0).mean()),
            "kmers_per_s": nk / (total_ms / n_steps / 1e3), "ms_per_step": total_ms / n_steps,
            "l2": "flushed (256 MB write) before every timed step",
+           "kernel": kernel,
            "random_sector": dict(sector_roofline(S, dev, idx, int(ctr[1]) + int(ctr[2]),
-                                                 int(ctr[0]), kern_s),
+                                                 int(ctr[0]), kern_s, n_filter),
                                  sectors_per_kmer=sectors / nk)}
     r = cpu_reference_rate(path, chars, ends, 31, len(ends))
     if r is not None:
@@ -762,6 +787,7 @@ def main():
     import sbwt_b200 as S
     torch.cuda.set_device(local)
     dev = local
+    S.set_table_kernel(args.kernel)
     L = S.lib()
     L.sbwt_profile_enable.argtypes = [C.c_int, C.c_int]
     L.sbwt_profile_read.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -846,18 +872,22 @@ def main():
     # roofline of the dominant kernel (the read search kernel)
     peak, peak_kind = load_peaks()
     kern_ms = search_ms.value / max(1, search_launches.value)
+    # the kernel that ran: with the k-mer table (k <= 31) the walks kernel by
+    # default, else the general kernel
+    kernel = search_kernel_name(idx, args.kernel)
+    n_filter = n_probe if kernel == "search_walks_kernel" else 0
+    if n_filter:
+        n_probe = 0
     # algorithmic bytes per launch (what this kernel's algorithm must move):
-    # one 32-byte sector per k-mer-table or presearch lookup, per rank block
-    # and per suffix-group word the search reads; 8 B result per k-mer; 2 bits of
-    # packed input + 1 invalid bit per char.
-    alg_bytes = ((n_pre + n_block + n_sg) * 32 + n_kmers * 8 + n_chars / 4 + n_chars / 8)
+    # one 32-byte sector per k-mer-table or presearch lookup, per k-mer filter
+    # word, per rank block and per suffix-group word the search reads; 8 B
+    # result per k-mer; 2 bits of packed input + 1 invalid bit per char.
+    alg_bytes = ((n_pre + n_block + n_sg + n_filter) * 32 + n_kmers * 8 + n_chars / 4 +
+                 n_chars / 8)
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9
-    # the read search runs on the table kernel when the index has its k-mer
-    # table (k <= 31, the library default), else on the general kernel
-    kernel = "search_table_kernel" if idx.set_kmer_table(True) else "search_reads_kernel"
     traffic_pk = profiled_traffic_per_kmer(kernel)
     try:
-        rs = sector_roofline(S, dev, idx, n_block + n_sg, n_pre, kern_ms / 1e3)
+        rs = sector_roofline(S, dev, idx, n_block + n_sg, n_pre, kern_ms / 1e3, n_filter)
     except Exception as e:  # reported as unmeasured, never hides the headline
         rs = {"error": repr(e)}
 
@@ -890,7 +920,7 @@ def main():
             extra["colors"] = {"error": repr(e)}
 
     cpu = None
-    if rank == 0:
+    if rank == 0 and not args.no_cpu:
         r = cpu_reference_rate(path, chars, ends, CFG["k"], args.cpu_sample_reads)
         if r is not None:
             rate, nk, dt, threads, (bits, pos, res) = r
@@ -921,14 +951,16 @@ def main():
                      "work": {"table_or_presearch_lookups": n_pre,
                               "rank_block_sectors": n_block,
                               "suffix_group_words": n_sg, "probe_iterations": n_probe,
+                              "filter_words": n_filter,
                               "bytes_per_kmer": alg_bytes / n_kmers,
                               "warp_iterations": n_iter,
                               "lanes_loading_per_iteration": n_lane / max(n_iter, 1),
                               "kmers_written_without_search": n_known,
                               "kmers_searched": n_searched,
                               "lane_steps_by_path": dict(zip(
-                                  ["stream", "presearch", "walk", "group_scan",
-                                   "kmer_table", "probe"], [int(x) for x in ctr[8:14]])),
+                                  ["stream", "filter" if n_filter else "presearch", "walk",
+                                   "group_scan", "kmer_table", "probe"],
+                                  [int(x) for x in ctr[8:14]])),
                               "distinct_paths_per_iteration": int(ctr[14]) / max(n_iter, 1)},
                      "random_sector": rs},
         "cpu_baseline": cpu,

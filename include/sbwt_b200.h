@@ -66,6 +66,8 @@ typedef struct {
   uint64_t device_bytes;      /* device memory held by the handle */
   int device;
   int has_key_kmer_marks;
+  uint64_t kmer_table_bytes;  /* k-mer -> node table (0 when absent) */
+  uint64_t kmer_filter_bytes; /* k-mer filter in front of the table (0 when absent) */
 } sbwt_index_info_t;
 
 /* Loads a .sbwt / .tdbg file (and, when colors_path is not NULL, the key
@@ -153,7 +155,8 @@ int sbwt_search_reads(const sbwt_index_t *index, const char *chars,
  *     that first call before any stream capture on that device.
  *   - Every call shares the array: calls that overlap on the GPU (several host
  *     threads or streams at once) race and must be serialized by the caller.
- * Results are identical to sbwt_search_reads. */
+ * Results are identical to sbwt_search_reads; the call runs the same read
+ * search kernel (the one sbwt_set_table_kernel selects). */
 int sbwt_search_reads_noalloc(const sbwt_index_t *index, const char *d_chars,
                               uint64_t n_chars, const uint64_t *d_read_ends,
                               uint64_t n_reads, uint64_t *d_results,
@@ -371,12 +374,19 @@ int sbwt_set_launch_config(uint32_t presearch_letters, uint32_t blocks_per_sm,
  * 0xFFFFFFFF = off).  Results never depend on it. */
 int sbwt_set_probe_length(uint32_t probe_len);
 /* Read search kernel of an index with a k-mer table (k <= 31, fewer than
- * 192 * 2^24 nodes, no SBWT_MOVE_TO_KEY_KMER): 1 = the table kernel (the
- * default: stream steps, group scans and table lookups only, with L2
- * eviction priorities on its loads), 0 = the general kernel (table
- * lookups plus presearch walks and absent-prefix probes).  Results never
- * depend on it. */
-int sbwt_set_table_kernel(int enabled);
+ * 192 * 2^24 nodes, no SBWT_MOVE_TO_KEY_KMER):
+ *   0 = the general kernel (table lookups plus presearch walks and
+ *       absent-prefix probes);
+ *   1 = the table kernel (stream steps, group scans and table lookups only,
+ *       with L2 eviction priorities on its loads);
+ *   2..5 = the walks kernel (the table kernel's steps, plus the k-mer
+ *       filter in front of the table, several tiles per lane with their
+ *       loads in flight together, and 32-byte result stores) with
+ *       (walks per lane, 256-thread blocks per SM) = (1, 5), (2, 4),
+ *       (2, 3), (4, 2); 3 is the default;
+ *   negative = the default.
+ * Results never depend on it.  Returns SBWT_E_INVALID above 5. */
+int sbwt_set_table_kernel(int mode);
 /* Persisting-L2 access-policy window over the index's rank blocks on the
  * search launches (0 = off, the default; 1 = on: sets this context's
  * persisting-L2 size). */

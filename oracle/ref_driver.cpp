@@ -65,6 +65,8 @@ void ref_presearch(const u64 *c_map, const u64 *const *acgt,
   const long n = 1L << (sbwt_search::presearch_letters * 2);
 #pragma omp parallel for schedule(static) num_threads(threads)
   for (long i = 0; i < n; ++i) {
+    blockIdx.x = 0;
+    blockDim.x = 1;
     threadIdx.x = (unsigned)i;
     sbwt_search::d_presearch(c_map, acgt, l0, l12, left, right);
   }
@@ -79,6 +81,10 @@ void ref_search(unsigned kmer_size, const u64 *c_map, const u64 *const *acgt,
                 const u64 *key_kmer_marks, u64 n, u64 *out, int threads) {
 #pragma omp parallel for schedule(dynamic, 4096) num_threads(threads)
   for (long i = 0; i < (long)n; ++i) {
+    /* every launch sets the whole index: OpenMP threads are shared with the
+     * colors driver, which launches with other block shapes */
+    blockIdx.x = 0;
+    blockDim.x = 1;
     threadIdx.x = (unsigned)i;
     if (key_kmer_marks)
       sbwt_search::d_search<true>(kmer_size, c_map, acgt, l0, l12, pre_left,

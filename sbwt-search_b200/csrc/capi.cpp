@@ -102,6 +102,8 @@ int sbwt_index_get_info(const sbwt_index_t *index, sbwt_index_info_t *info) {
   info->device_bytes = x.device_bytes;
   info->device = x.device;
   info->has_key_kmer_marks = x.view.key_marks != nullptr;
+  info->kmer_table_bytes = x.kmer_table.size();
+  info->kmer_filter_bytes = x.kmer_filter.size();
   return SBWT_OK;
 }
 
@@ -196,7 +198,7 @@ int sbwt_index_set_kmer_table(sbwt_index_t *index, int enable, uint64_t *table_b
       x.build_kmer_table();
     }
     x.device_bytes = x.presearch.size() + x.hot.size() + x.key_buf.size() + x.l0_all.size() +
-                     x.kmer_table.size();
+                     x.kmer_table.size() + x.kmer_filter.size();
     if (table_bytes) *table_bytes = x.kmer_table.size();
   });
 }
@@ -296,11 +298,15 @@ int sbwt_set_probe_length(uint32_t probe_len) {
   return SBWT_OK;
 }
 
-// Tuning hook: 1 (the default) runs the read search of an index with a k-mer
-// table on the table kernel, 0 on the general kernel.  Results do not depend
-// on it.
-int sbwt_set_table_kernel(int enabled) {
-  default_launch_config().table_kernel = enabled ? 1u : 0u;
+// Tuning hook: the read search kernel of an index with a k-mer table (see
+// launch_search_kernel in index.cu): 0 general, 1 table, 2..5 walks kernel
+// variants, negative = the library default.  Results do not depend on it.
+int sbwt_set_table_kernel(int mode) {
+  if (mode > 5) {
+    set_last_error("table kernel mode must be 0..5 (or negative for the default)");
+    return SBWT_E_INVALID;
+  }
+  default_launch_config().table_kernel = mode < 0 ? kDefaultTableKernel : (uint32_t)mode;
   return SBWT_OK;
 }
 

@@ -50,6 +50,8 @@ struct SbwtView {
   const uint64_t *key_marks;            // N bits or nullptr
   const uint64_t *kmer_table;  // (key, node) slots, or nullptr
   uint64_t kmer_table_mask;    // slots - 1
+  const uint64_t *kmer_filter; // blocked Bloom filter of the table's keys, or nullptr
+  uint64_t filter_words;       // 64-bit words of kmer_filter
   uint64_t num_bits;
   uint32_t k;
   uint32_t p;      // presearch depth used by this call

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -1152,6 +1153,370 @@ __global__ void __launch_bounds__(256, SBWT_TABLE_MIN_BLOCKS)
   }
 }
 
+// Read search with the k-mer table and its filter, W walks per lane (a walk
+// = one work tile being searched).  The same tiles, work queue and result
+// rules as search_table_kernel.  Each iteration first issues the loads of all
+// W walks of the lane and then uses them, so a lane keeps W independent
+// loads in flight (up to 4 W while its walks read filter words).  Walk modes:
+//   WK_STREAM, WK_SG, WK_STEP : T_STREAM, T_SG and T_STEP of search_table_kernel;
+//   WK_FILTER : the walk has no previous node (tile or read start, after an
+//              absent k-mer or an invalid char): the filter words of the
+//              next nb <= 4 k-mers of the read, loaded together.  K-mers the
+//              filter rejects are absent (-1); the first one it passes goes
+//              to WK_HASH.
+//   WK_HASH   : the k-mer table pair of slots of that k-mer.
+// The filter answers most k-mers a stream step cannot reach (those around
+// read errors) from a structure 25x smaller than the table; a rejection is
+// exact, so results equal the table kernel's.  Results pass through 4 slots
+// per walk in shared memory and leave as one 32-byte store per 4 consecutive
+// k-mer slots (tiles are multiples of 4 slots) when the output is 32-byte
+// aligned.
+enum : uint32_t { WK_NEW = 0, WK_STREAM = 1, WK_STEP = 2, WK_SG = 3, WK_FILTER = 4, WK_HASH = 5,
+                  WK_DONE = 6 };
+constexpr uint32_t kFilterBatch = 4;
+
+__device__ __forceinline__ uint64_t load_u64_nc(const uint64_t *p) {
+  uint64_t v;
+  asm("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
+}
+
+__device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_t b,
+                                                uint64_t c, uint64_t d) {
+  asm volatile("st.global.cs.v4.u64 [%0], {%1,%2,%3,%4};" ::"l"(p), "l"(a), "l"(b), "l"(c),
+               "l"(d)
+               : "memory");
+}
+
+// W walks per lane; MINB = 256-thread blocks per SM the register budget
+// targets (W = 1: 5, W = 2: 4 or 3, W = 4: 2).
+template <int W, int MINB, bool COUNT>
+__global__ void __launch_bounds__(256, MINB)
+    search_walks_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
+                        unsigned long long *counters) {
+  using I = uint32_t;
+  constexpr I NONE = ~I(0);
+  __shared__ uint32_t sh_cmap[4];
+  __shared__ unsigned long long sh_out[4][W][256];  // staged results, slot & 3 first
+  if (threadIdx.x < 4) sh_cmap[threadIdx.x] = (uint32_t)s.c_map[threadIdx.x];
+  __syncthreads();
+  const uint32_t k = s.k;
+  const uint32_t lane = threadIdx.x & 31;
+  const I n_kmers = (I)(rv.n_kmers_dev ? *rv.n_kmers_dev : rv.n_kmers);
+  const I tsize = (I)rv.tile;
+  const I n_tiles = (n_kmers + tsize - 1) / tsize;
+  const I base = (I)rv.base;
+  const I out_cap = (I)min(rv.out_capacity, (uint64_t)NONE);
+  const bool vec_out = ((uintptr_t)rv.out & 31) == 0;
+  uint64_t n_table = 0, n_block = 0, n_sg = 0, n_filter = 0, n_iter = 0, n_lane = 0,
+           n_known = 0, n_searched = 0, n_stream = 0, n_step = 0, n_distinct = 0;
+  I slot[W], slot_end[W], r[W], r_next[W], pos[W], last_inv1[W], v[W], x[W], hslot[W];
+  I obase[W];
+  uint32_t mode[W], ubit[W], nb[W], omask[W];
+  CharWin<I> cw[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    slot[w] = slot_end[w] = r[w] = r_next[w] = pos[w] = last_inv1[w] = x[w] = hslot[w] = 0;
+    v[w] = NONE;
+    obase[w] = 0;
+    mode[w] = WK_NEW;
+    ubit[w] = 63;
+    nb[w] = 0;
+    omask[w] = 0;
+    cw[w].init();
+  }
+  const uint64_t pol_last = l2_policy_evict_last(), pol_first = l2_policy_evict_first();
+
+  auto flush = [&](int w) {  // the staged slots of walk w's open group
+    const I g = obase[w];
+    const uint32_t t = threadIdx.x;
+    if (omask[w] == 15u && vec_out && g + 4 <= out_cap) {
+      store_sector_cs(rv.out + g, sh_out[0][w][t], sh_out[1][w][t], sh_out[2][w][t],
+                      sh_out[3][w][t]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (((omask[w] >> q) & 1u) && g + q < out_cap) __stcs(rv.out + g + q, sh_out[q][w][t]);
+    }
+    omask[w] = 0;
+  };
+  auto emit = [&](int w, I sl, I node) {
+    const I g = sl & ~I(3);
+    if (omask[w] && g != obase[w]) flush(w);
+    obase[w] = g;
+    sh_out[sl & 3][w][threadIdx.x] =
+        node == NONE ? (unsigned long long)SBWT_NOT_FOUND : (unsigned long long)node;
+    omask[w] |= 1u << (sl & 3);
+    if (omask[w] == 15u) flush(w);
+  };
+
+  while (true) {
+    // ---- work queue (warp-collective): one tile per walk that needs one
+    uint32_t need = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) need += (mode[w] == WK_NEW && slot[w] >= slot_end[w]);
+    uint32_t incl = need;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if ((int)lane >= o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    I new_tile[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) new_tile[w] = NONE;
+    if (total) {
+      unsigned long long qb = 0;
+      if (lane == 31) qb = atomicAdd(rv.queue, (unsigned long long)total);
+      qb = __shfl_sync(0xFFFFFFFFu, qb, 31);
+      unsigned long long t = qb + incl - need;
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        if (mode[w] == WK_NEW && slot[w] >= slot_end[w]) {
+          if (t < (unsigned long long)n_tiles)
+            new_tile[w] = (I)t;
+          else
+            mode[w] = WK_DONE;
+          ++t;
+        }
+      }
+    }
+    // ---- phase 1 (per walk): the next k-mer, runs of -2, the walk's mode
+    I run_slot[W];
+    uint32_t run_n[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      run_slot[w] = 0;
+      run_n[w] = 0;
+      if (mode[w] != WK_NEW) continue;
+      bool ready = false;
+      while (true) {
+        if (slot[w] >= slot_end[w]) {  // next tile
+          if (new_tile[w] == NONE) break;
+          slot[w] = new_tile[w] * tsize;
+          new_tile[w] = NONE;
+          slot_end[w] = min(slot[w] + tsize, n_kmers);
+          r[w] = (I)__ldg(tile_read + slot[w] / tsize);
+          r_next[w] = (I)__ldg(rv.kmer_off + r[w] + 1);
+          pos[w] = (r[w] ? (I)__ldg(rv.ends + r[w] - 1) : base) - base +
+                   (slot[w] - (I)__ldg(rv.kmer_off + r[w]));
+          cw[w].move_to(rv.packed, rv.invalid, pos[w]);
+          last_inv1[w] = cw[w].last_invalid1(pos[w], pos[w] + k - 1);
+          v[w] = NONE;
+        } else if (slot[w] == r_next[w]) {  // next read
+          do {
+            r_next[w] = (I)__ldg(rv.kmer_off + (++r[w]) + 1);
+          } while (r_next[w] == slot[w]);
+          pos[w] = (I)__ldg(rv.ends + r[w] - 1) - base;
+          cw[w].move_to(rv.packed, rv.invalid, pos[w]);
+          last_inv1[w] = cw[w].last_invalid1(pos[w], pos[w] + k - 1);
+          v[w] = NONE;
+        }
+        const I newc = pos[w] + k - 1;
+        cw[w].move_to(rv.packed, rv.invalid, pos[w]);
+        if (cw[w].invalid_at(newc)) last_inv1[w] = newc + 1;
+        if (last_inv1[w] <= pos[w]) {
+          ready = true;
+          break;
+        }
+        if (run_n[w]) break;  // one run per walk per iteration
+        // k-mers pos .. last_inv1 - 1 all hold the invalid char at
+        // last_inv1 - 1: a run of -2 up to the read / tile end
+        const I n = min(last_inv1[w] - pos[w], min(r_next[w], slot_end[w]) - slot[w]);
+        run_slot[w] = slot[w];
+        run_n[w] = (uint32_t)n;
+        if (COUNT) n_known += n;
+        v[w] = NONE;
+        slot[w] += n;
+        pos[w] += n;
+        if (slot[w] < min(r_next[w], slot_end[w])) {
+          cw[w].move_to(rv.packed, rv.invalid, pos[w]);
+          last_inv1[w] = cw[w].last_invalid1(pos[w], pos[w] + k - 1);
+        }
+      }
+      if (ready) {
+        if (v[w] != NONE) {
+          x[w] = v[w];
+          mode[w] = WK_STREAM;
+        } else {
+          // k-mers pos .. pos + nb - 1 of this read and tile, in the char
+          // window, whose chars after newc are valid
+          const uint32_t off = pos[w] - 32 * cw[w].wbase;
+          uint32_t lim = min(min(r_next[w], slot_end[w]) - slot[w], 65u - k - off);
+          lim = min(lim, kFilterBatch);
+          const uint32_t o1 = off + k;  // window offset of newc + 1
+          const uint64_t m = (cw[w].inv >> o1) & low_mask(lim - 1);
+          if (m) lim = min(lim, (uint32_t)__ffsll((long long)m));
+          nb[w] = lim;
+          mode[w] = WK_FILTER;
+        }
+      }
+    }
+    // ---- runs of -2 (converged): the warp writes each walk's run
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      for (unsigned runs = __ballot_sync(0xFFFFFFFFu, run_n[w] != 0); runs; runs &= runs - 1) {
+        const int q = __ffs(runs) - 1;
+        const I q_slot = __shfl_sync(0xFFFFFFFFu, run_slot[w], q);
+        const uint32_t q_n = __shfl_sync(0xFFFFFFFFu, run_n[w], q);
+        for (uint32_t j = lane; j < q_n; j += 32)
+          if (q_slot + j < out_cap) __stcs(rv.out + q_slot + j, (unsigned long long)SBWT_INVALID);
+      }
+    }
+    bool all_done = true;
+#pragma unroll
+    for (int w = 0; w < W; ++w) all_done &= mode[w] == WK_DONE;
+    if (__all_sync(0xFFFFFFFFu, all_done)) break;
+    // ---- phase 2: the loads of every walk, issued before any is used
+    Block A[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      A[w] = Block{0, 0, 0, 0};
+      if (mode[w] == WK_STREAM || mode[w] == WK_STEP) {
+        const uint32_t c = cw[w].char_at(pos[w] + k - 1);
+        A[w] = load_block_hint(s.blocks0 + (uint64_t)c * s.block_stride + block_idx(x[w]),
+                               pol_last);
+      } else if (mode[w] == WK_SG) {
+        A[w] = load_block_hint(chunk_of(s.suffix_group_starts, (uint64_t)x[w]), pol_last);
+      } else if (mode[w] == WK_HASH) {
+        A[w] = load_block_hint(reinterpret_cast<const Block *>(s.kmer_table + 2 * (uint64_t)hslot[w]),
+                               pol_first);
+      } else if (mode[w] == WK_FILTER) {
+        uint64_t z = kmer_mix(cw[w].prefix(pos[w], k));
+        A[w].w0 = load_u64_nc(s.kmer_filter + kmer_filter_word(z, s.filter_words));
+        if (nb[w] > 1) {
+          z = kmer_mix(cw[w].prefix(pos[w] + 1, k));
+          A[w].w1 = load_u64_nc(s.kmer_filter + kmer_filter_word(z, s.filter_words));
+        }
+        if (nb[w] > 2) {
+          z = kmer_mix(cw[w].prefix(pos[w] + 2, k));
+          A[w].w2 = load_u64_nc(s.kmer_filter + kmer_filter_word(z, s.filter_words));
+        }
+        if (nb[w] > 3) {
+          z = kmer_mix(cw[w].prefix(pos[w] + 3, k));
+          A[w].w3 = load_u64_nc(s.kmer_filter + kmer_filter_word(z, s.filter_words));
+        }
+      }
+    }
+    if (COUNT) {
+      n_iter += lane == 0;
+      uint32_t path = 0;
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        const uint32_t md = mode[w];
+        n_lane += md >= WK_STREAM && md <= WK_HASH;
+        path |= (md >= WK_STREAM && md <= WK_HASH) ? 1u << md : 0u;
+        n_table += md == WK_HASH;
+        n_block += md == WK_STREAM || md == WK_STEP;
+        n_sg += md == WK_SG;
+        n_filter += md == WK_FILTER ? nb[w] : 0;
+        n_stream += md == WK_STREAM;
+        n_step += md == WK_STEP;
+      }
+      const uint32_t seen = __reduce_or_sync(0xFFFFFFFFu, path);
+      n_distinct += lane == 0 ? __popc(seen) : 0;
+    }
+    // ---- phase 3 (per walk)
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      const uint32_t md = mode[w];
+      if (md == WK_FILTER) {
+        // k-mers the filter rejects are absent; the first it passes is looked up
+        uint32_t j = 0;
+        for (; j < nb[w]; ++j) {
+          const uint64_t z = kmer_mix(cw[w].prefix(pos[w], k));
+          const uint64_t word = j == 0 ? A[w].w0 : (j == 1 ? A[w].w1 : (j == 2 ? A[w].w2 : A[w].w3));
+          const uint64_t bits = kmer_filter_bits(z);
+          if ((word & bits) == bits) {
+            hslot[w] = (I)kmer_table_slot(z, s.kmer_table_mask);
+            mode[w] = WK_HASH;
+            break;
+          }
+          if (COUNT) ++n_searched;
+          emit(w, slot[w], NONE);
+          ++slot[w];
+          ++pos[w];
+        }
+        if (j == nb[w]) mode[w] = WK_NEW;  // v stays NONE
+        continue;
+      }
+      if (md != WK_STREAM && md != WK_STEP && md != WK_SG && md != WK_HASH) continue;
+      I res = NONE;
+      bool emitted = false;
+      if (md == WK_HASH) {  // slots hslot, hslot + 1: (key, node) each
+        const uint64_t key = cw[w].prefix(pos[w], k);
+        if (A[w].w0 == key) {
+          res = (I)A[w].w1;
+          emitted = true;
+        } else if (A[w].w2 == key) {
+          res = (I)A[w].w3;
+          emitted = true;
+        } else if (A[w].w0 == ~0ULL || A[w].w2 == ~0ULL) {  // an empty slot: absent
+          emitted = true;
+        } else {
+          hslot[w] = (I)(((uint64_t)hslot[w] + 2) & s.kmer_table_mask);
+        }
+      } else if (md == WK_SG) {  // group starts at or below v in word x
+        const uint64_t wd = chunk_word(A[w], (uint64_t)x[w]) & low_mask(ubit[w] + 1);
+        if (wd) {
+          const I g = x[w] * 64 + 63 - (I)__clzll(wd);
+          if (g == v[w]) {
+            emitted = true;  // v starts its group and has no edge c
+          } else {
+            x[w] = g;
+            mode[w] = WK_STEP;
+          }
+        } else if (x[w] == 0) {
+          emitted = true;  // no group start below v: malformed SBWT
+        } else {
+          --x[w];
+          ubit[w] = 63;
+        }
+      } else {  // a step on [x, x] with the k-mer's last char
+        const uint32_t c = cw[w].char_at(pos[w] + k - 1);
+        const uint32_t q = x[w] - block_idx(x[w]) * kBlockBits;
+        if (block_bit(A[w], q)) {
+          res = sh_cmap[c] + (I)block_rank(A[w], q);
+          emitted = true;
+        } else if (md == WK_STREAM) {  // no edge at v itself: v's group start
+          ubit[w] = x[w] & 63;
+          x[w] >>= 6;
+          mode[w] = WK_SG;
+        } else {
+          emitted = true;
+        }
+      }
+      if (emitted) {
+        if (COUNT) ++n_searched;
+        v[w] = res;
+        emit(w, slot[w], res);
+        ++slot[w];
+        ++pos[w];
+        mode[w] = WK_NEW;
+      }
+    }
+  }
+#pragma unroll
+  for (int w = 0; w < W; ++w)
+    if (omask[w]) flush(w);
+  if (COUNT) {
+    atomicAdd(counters + 0, (unsigned long long)n_table);
+    atomicAdd(counters + 1, (unsigned long long)n_block);
+    atomicAdd(counters + 2, (unsigned long long)n_sg);
+    atomicAdd(counters + 3, (unsigned long long)n_filter);
+    atomicAdd(counters + 4, (unsigned long long)n_iter);
+    atomicAdd(counters + 5, (unsigned long long)n_lane);
+    atomicAdd(counters + 6, (unsigned long long)n_known);
+    atomicAdd(counters + 7, (unsigned long long)n_searched);
+    atomicAdd(counters + 8, (unsigned long long)n_stream);   // stream steps
+    atomicAdd(counters + 9, (unsigned long long)n_filter);   // filter words
+    atomicAdd(counters + 10, (unsigned long long)n_step);    // steps at a group start
+    atomicAdd(counters + 11, (unsigned long long)n_sg);      // group scan words
+    atomicAdd(counters + 12, (unsigned long long)n_table);   // table lookups
+    atomicAdd(counters + 14, (unsigned long long)n_distinct);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -1213,15 +1578,22 @@ static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStrea
   SBWT_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
 }
 
+// kernel_mode: 0 = the general kernel; 1 = the table kernel; 2..5 = the
+// walks kernel with (walks per lane, blocks per SM) = (1, 5), (2, 4), (2, 3),
+// (4, 2) (the table kernel when the index has no k-mer filter).  Results
+// never depend on it.
+// instrument = false keeps the launch free of the profiler's events and
+// counter buffer (the allocation-free entry point).
 static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsView &rv,
                                  const uint64_t *tile_read, uint32_t mtk, uint32_t *d_err,
                                  int grid, int threads, cudaStream_t st,
-                                 const LaunchAttrs &la, bool table_kernel) {
+                                 const LaunchAttrs &la, uint32_t kernel_mode,
+                                 bool instrument = true) {
   Profile &p = profile();
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(st, &cap);
-  const bool timed = p.enabled && cap == cudaStreamCaptureStatusNone;
+  const bool timed = instrument && p.enabled && cap == cudaStreamCaptureStatusNone;
   if (timed) {
     SBWT_CUDA(cudaEventCreate(&e0));
     SBWT_CUDA(cudaEventCreate(&e1));
@@ -1238,8 +1610,9 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
   }
   const bool small = sv.k <= 33;
   const bool narrow = sv.num_bits < kNarrowLimit && rv.n_kmers_bound < (1ULL << 32);
-  const bool table = table_kernel && stream && narrow && sv.kmer_table && sv.k <= 31 &&
+  const bool table = kernel_mode != 0 && stream && narrow && sv.kmer_table && sv.k <= 31 &&
                      mtk == 0 && sv.suffix_group_starts;
+  const bool walks = table && kernel_mode >= 2 && sv.kmer_filter;
 #define SBWT_LAUNCH(S_, C_, K_)                                                          \
   do {                                                                                   \
     if (narrow)                                                                          \
@@ -1249,7 +1622,22 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
       launch_ex(search_reads_kernel<S_, C_, K_, uint64_t>, grid, threads, st, la, sv, rv, \
                 tile_read, mtk, d_err, ctr);                                             \
   } while (0)
-  if (table) {
+  if (walks) {
+#define SBWT_WALKS(W_, B_)                                                                 \
+  do {                                                                                     \
+    if (ctr)                                                                               \
+      launch_ex(search_walks_kernel<W_, B_, true>, grid, threads, st, la, sv, rv, tile_read, \
+                ctr);                                                                      \
+    else                                                                                   \
+      launch_ex(search_walks_kernel<W_, B_, false>, grid, threads, st, la, sv, rv, tile_read, \
+                ctr);                                                                      \
+  } while (0)
+    if (kernel_mode == 2) SBWT_WALKS(1, 5);
+    else if (kernel_mode == 3) SBWT_WALKS(2, 4);
+    else if (kernel_mode == 4) SBWT_WALKS(2, 3);
+    else SBWT_WALKS(4, 2);
+#undef SBWT_WALKS
+  } else if (table) {
     if (ctr)
       launch_ex(search_table_kernel<true>, grid, threads, st, la, sv, rv, tile_read, ctr);
     else
@@ -1433,7 +1821,7 @@ IndexImpl::IndexImpl(const u64 *const acgt[4], u64 num_bits_, u32 k_,
   SBWT_CUDA(cudaDeviceSynchronize());
   build_kmer_table();
   device_bytes = presearch.size() + hot.size() + key_buf.size() + l0_all.size() +
-                 kmer_table.size();
+                 kmer_table.size() + kmer_filter.size();
 }
 
 SbwtView IndexImpl::view_for(u32 p) const {
@@ -1522,7 +1910,8 @@ static u64 tile_size(int device, u64 n_kmers, const LaunchConfig &cfg) {
   if (cfg.tile) return cfg.tile;
   const u64 resident = (u64)sm_count(device) * cfg.blocks_per_sm * 256;
   u64 tile = n_kmers / (resident * 8);
-  return std::min<u64>(std::max<u64>(tile, 16), 1024);
+  // a multiple of 4 slots: the walks kernel stores 4 results per 32 bytes
+  return (std::min<u64>(std::max<u64>(tile, 16), 1024) + 3) & ~3ULL;
 }
 
 // Scan of per-read k-mer counts and the packing of the chars (device-resident
@@ -1594,7 +1983,7 @@ static void launch_search(const IndexImpl &ix, u64 n_chars, const u64 *d_ends, u
   launch_search_kernel(stream, sv, rv, sc.tile_read, mtk, sc.err, grid, threads, st,
                        persist ? search_attrs(ix.hot.get(), ix.window_bytes, persist)
                                : LaunchAttrs{},
-                       cfg.table_kernel != 0);
+                       cfg.table_kernel);
 }
 
 // The index step of one device-resident batch without any host
@@ -1636,7 +2025,7 @@ void enqueue_index_step(const IndexImpl &ix, const char *d_chars, u64 n_chars,
   const bool stream = !(flags & SBWT_PER_KMER_WALK) && ix.view.suffix_group_starts;
   const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
   launch_search_kernel(stream, sv, rv, sc.tile_read, mtk, sc.err, grid, 256, st,
-                       LaunchAttrs{}, cfg.table_kernel != 0);
+                       LaunchAttrs{}, cfg.table_kernel);
   note_launches(1);
 }
 
@@ -1832,21 +2221,35 @@ constexpr u64 kNoAllocBytes =
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 // Device address of g_noalloc_scratch on `device`, looked up once per device
-// (with that device current) on the first call there.
+// (with that device current) on the first call there; later calls read it
+// without a lock.
 static unsigned char *noalloc_scratch_address(int device) {
+  static const int n_dev = [] {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+      cudaGetLastError();
+      n = 0;
+    }
+    return n;
+  }();
+  static std::unique_ptr<std::atomic<unsigned char *>[]> addr(
+      new std::atomic<unsigned char *>[std::max(n_dev, 1)]());
   static std::mutex mu;
-  static unsigned char *addr[64] = {};
-  if (device < 0 || device >= 64) throw Error(SBWT_E_INVALID, "device id out of range");
+  if (device < 0 || device >= n_dev) throw Error(SBWT_E_INVALID, "device id out of range");
+  unsigned char *a = addr[device].load(std::memory_order_acquire);
+  if (a) return a;
   std::lock_guard<std::mutex> g(mu);
-  if (!addr[device]) {
+  a = addr[device].load(std::memory_order_relaxed);
+  if (!a) {
     void *p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess)
       throw Error(SBWT_E_CUDA, std::string("cudaGetSymbolAddress(no-alloc scratch): ") +
                                    cudaGetErrorString(e));
-    addr[device] = static_cast<unsigned char *>(p);
+    a = static_cast<unsigned char *>(p);
+    addr[device].store(a, std::memory_order_release);
   }
-  return addr[device];
+  return a;
 }
 
 void IndexImpl::search_reads_noalloc(const char *d_chars, u64 n_chars, const u64 *d_ends,
@@ -1910,23 +2313,9 @@ void IndexImpl::search_reads_noalloc(const char *d_chars, u64 n_chars, const u64
   const SbwtView sv = view_for(cfg.presearch_letters);
   const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
   const bool stream = !(flags & SBWT_PER_KMER_WALK) && view.suffix_group_starts;
-  const bool narrow = sv.num_bits < kNarrowLimit && rv.n_kmers_bound < (1ULL << 32);
-#define SBWT_NA_LAUNCH(S_, K_)                                                          \
-  do {                                                                                  \
-    if (narrow)                                                                         \
-      search_reads_kernel<S_, false, K_, uint32_t>                                      \
-          <<<grid, 256, 0, st>>>(sv, rv, sc.tile_read, mtk, sc.err, nullptr);           \
-    else                                                                                \
-      search_reads_kernel<S_, false, K_, uint64_t>                                      \
-          <<<grid, 256, 0, st>>>(sv, rv, sc.tile_read, mtk, sc.err, nullptr);           \
-  } while (0)
-  if (sv.k <= 33) {
-    if (stream) SBWT_NA_LAUNCH(true, true); else SBWT_NA_LAUNCH(false, true);
-  } else {
-    if (stream) SBWT_NA_LAUNCH(true, false); else SBWT_NA_LAUNCH(false, false);
-  }
-#undef SBWT_NA_LAUNCH
-  SBWT_CUDA(cudaGetLastError());
+  // the same kernel choice as sbwt_search_reads, without the profiler
+  launch_search_kernel(stream, sv, rv, sc.tile_read, mtk, sc.err, grid, 256, st,
+                       LaunchAttrs{}, cfg.table_kernel, /*instrument=*/false);
   SBWT_CUDA(cudaMemcpyAsync(&err, sc.err, 4, cudaMemcpyDeviceToHost, st));
   SBWT_CUDA(cudaStreamSynchronize(st));
   if (err)

@@ -14,6 +14,12 @@ namespace sbwt {
 constexpr uint32_t kPresearchMaxLetters = 14;
 // Largest k-mer table an index builds (16 bytes per slot, <= 2 slots per k-mer).
 constexpr u64 kKmerTableMaxBytes = 32ULL << 30;
+// Bits per k-mer of the k-mer filter built with the table.
+constexpr u64 kFilterBitsPerKmer = 10;
+
+// Read search kernel of an index with a k-mer table and filter by default
+// (LaunchConfig::table_kernel): the walks kernel with 2 walks per lane.
+constexpr uint32_t kDefaultTableKernel = 3;
 
 struct LaunchConfig {
   uint32_t presearch_letters = 0;  // <= the handle's pyramid depth
@@ -22,7 +28,8 @@ struct LaunchConfig {
   uint64_t chunk_chars = 0;        // host-pointer path: chars per chunk
   uint32_t probe_len = 0;          // absent-prefix probe length (0 = auto, ~0u = off)
   uint32_t l2_window = 0;          // persisting L2 window over the index's hot data
-  uint32_t table_kernel = 1;       // k-mer-table read search kernel where it applies
+  uint32_t table_kernel = kDefaultTableKernel;  // read search kernel with a k-mer table
+                                               // (0 general, 1 table, 2-4 walks)
 };
 
 struct IndexImpl {
@@ -30,7 +37,8 @@ struct IndexImpl {
             const u64 *key_marks, int device, unsigned presearch_letters);
 
   SbwtView view_for(u32 p) const;
-  // k-mer -> node hash table (k <= 31): false when not built
+  // k-mer -> node hash table (k <= 31) and its k-mer filter: false when not
+  // built
   bool build_kmer_table();
   void drop_kmer_table();
 
@@ -54,7 +62,7 @@ struct IndexImpl {
   u64 device_bytes = 0;
   SbwtView view{};
   DeviceBuffer hot;  // rank blocks of A/C/G/T + suffix-group words, contiguous
-  DeviceBuffer l0_all, presearch, key_buf, kmer_table;
+  DeviceBuffer l0_all, presearch, key_buf, kmer_table, kmer_filter;
   u64 table_kmers = 0;
   u64 window_bytes = 0;   // L2 access-policy window over `hot`
 };

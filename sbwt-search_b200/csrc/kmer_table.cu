@@ -19,6 +19,15 @@
 // char on top (2 bits each), empty = ~0; a key's probe sequence starts at an
 // even slot (so a 32-byte sector holds the first two slots it probes) and
 // moves one slot at a time; at most half of the slots are used.
+//
+// Filter: beside the table, a blocked Bloom filter of the same keys, 10 bits
+// per k-mer, one 64-bit word per key with four of its bits set
+// (kmer_filter_word / kmer_filter_bits).  It is 25x smaller than the table
+// (144 MB for 115 M k-mers against 4 GiB), so a read k-mer that is absent
+// -- most k-mers that a stream step cannot reach -- is answered from a
+// structure inside the GPU's address-translation reach and mostly in L2,
+// and only k-mers the filter passes pay a table lookup.  A filter answer of
+// "absent" is exact (no false negatives), so results do not change.
 #include <cuda_runtime.h>
 
 #include <cub/cub.cuh>
@@ -117,6 +126,16 @@ __global__ void table_insert_kernel(const uint64_t *key, const uint8_t *alive, u
   }
 }
 
+__global__ void filter_insert_kernel(const uint64_t *key, const uint8_t *alive, uint64_t n,
+                                     unsigned long long *filter, uint64_t n_words) {
+  const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += step) {
+    if (!alive[v]) continue;
+    const uint64_t z = kmer_mix(key[v]);
+    atomicOr(filter + kmer_filter_word(z, n_words), (unsigned long long)kmer_filter_bits(z));
+  }
+}
+
 unsigned grid_of(uint64_t n) {
   return (unsigned)std::max<uint64_t>(std::min<uint64_t>((n + 255) / 256, 148 * 32), 1);
 }
@@ -128,9 +147,7 @@ unsigned grid_of(uint64_t n) {
 // quarter of the free device memory.
 bool IndexImpl::build_kmer_table() {
   DeviceGuard g(device);
-  kmer_table.release();
-  view.kmer_table = nullptr;
-  view.kmer_table_mask = 0;
+  drop_kmer_table();
   if (k > 31 || k < 2) return false;
   const u64 n = num_bits, nw = (num_bits + 63) / 64;
   // predecessor tables: positions of the ones of each vector
@@ -175,7 +192,9 @@ bool IndexImpl::build_kmer_table() {
   while (slots < 2 * n_kmers) slots <<= 1;
   size_t free_b = 0, total_b = 0;
   SBWT_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  if (slots > (1ULL << 32) || slots * 16 > kKmerTableMaxBytes || slots * 16 > free_b / 4)
+  const u64 filter_words = std::max<u64>((n_kmers * kFilterBitsPerKmer + 63) / 64, 1);
+  if (slots > (1ULL << 32) || slots * 16 > kKmerTableMaxBytes ||
+      slots * 16 + filter_words * 8 > free_b / 4)
     return false;
   kmer_table.resize(slots * 16);
   SBWT_CUDA(cudaMemset(kmer_table.get(), 0xFF, slots * 16));
@@ -191,8 +210,16 @@ bool IndexImpl::build_kmer_table() {
     kmer_table.release();
     throw Error(SBWT_E_FORMAT, "an SBWT k-mer occurs twice");
   }
+  kmer_filter.resize(filter_words * 8);
+  SBWT_CUDA(cudaMemset(kmer_filter.get(), 0, filter_words * 8));
+  filter_insert_kernel<<<grid_of(n), 256>>>(key.get<u64>(), alive.get<uint8_t>(), n,
+                                            kmer_filter.get<unsigned long long>(),
+                                            filter_words);
+  SBWT_CUDA(cudaGetLastError());
   view.kmer_table = kmer_table.get<u64>();
   view.kmer_table_mask = slots - 1;
+  view.kmer_filter = kmer_filter.get<u64>();
+  view.filter_words = filter_words;
   table_kmers = n_kmers;
   return true;
 }
@@ -200,8 +227,11 @@ bool IndexImpl::build_kmer_table() {
 void IndexImpl::drop_kmer_table() {
   DeviceGuard g(device);
   kmer_table.release();
+  kmer_filter.release();
   view.kmer_table = nullptr;
   view.kmer_table_mask = 0;
+  view.kmer_filter = nullptr;
+  view.filter_words = 0;
   table_kmers = 0;
 }
 

@@ -76,14 +76,36 @@ __device__ __forceinline__ uint64_t block_of(uint64_t i) {
   return (uint64_t)((uint32_t)(i >> 6) / 3u);
 }
 
-// First slot of a key's probe sequence in the k-mer table (an even slot, so
-// that one 32-byte sector holds the first two slots probed); the mixer is the
-// SplitMix64 finalizer (Steele, Lea, Flood 2014).
-__device__ __forceinline__ uint64_t kmer_table_bucket(uint64_t z, uint64_t mask) {
+// Hash of a k-mer key: the SplitMix64 finalizer (Steele, Lea, Flood 2014).
+// The k-mer table takes its bucket from the low bits, the k-mer filter its
+// word from the high bits and its four bit positions from bits 0..23.
+__device__ __forceinline__ uint64_t kmer_mix(uint64_t z) {
   z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
   z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
-  z ^= z >> 31;
+  return z ^ (z >> 31);
+}
+
+// First slot of a key's probe sequence in the k-mer table (an even slot, so
+// that one 32-byte sector holds the first two slots probed), from its hash.
+__device__ __forceinline__ uint64_t kmer_table_slot(uint64_t z, uint64_t mask) {
   return z & mask & ~1ULL;
+}
+
+__device__ __forceinline__ uint64_t kmer_table_bucket(uint64_t key, uint64_t mask) {
+  return kmer_table_slot(kmer_mix(key), mask);
+}
+
+// k-mer filter (a blocked Bloom filter with one 64-bit word per key): the
+// word of a hash (multiply-shift range reduction of its high bits) and the
+// four bits the key sets in it.  A key is absent when any of its bits is
+// clear; a key whose bits are all set may be present (false positives at
+// about 1.5 % with 10 bits per key).
+__device__ __forceinline__ uint64_t kmer_filter_word(uint64_t z, uint64_t n_words) {
+  return __umul64hi(z, n_words);
+}
+__device__ __forceinline__ uint64_t kmer_filter_bits(uint64_t z) {
+  return (1ULL << (z & 63)) | (1ULL << ((z >> 6) & 63)) | (1ULL << ((z >> 12) & 63)) |
+         (1ULL << ((z >> 18) & 63));
 }
 
 // rank_c(i): ones of vector c in [0, i), i in [0, N].

@@ -45,7 +45,8 @@ class IndexInfo(C.Structure):
     _fields_ = [("num_bits", C.c_uint64), ("k", C.c_uint32),
                 ("presearch_letters", C.c_uint32), ("c_map", C.c_uint64 * 5),
                 ("device_bytes", C.c_uint64), ("device", C.c_int),
-                ("has_key_kmer_marks", C.c_int)]
+                ("has_key_kmer_marks", C.c_int), ("kmer_table_bytes", C.c_uint64),
+                ("kmer_filter_bytes", C.c_uint64)]
 
 
 _L = None
@@ -152,11 +153,15 @@ def set_probe_length(probe_len: int = 0) -> None:
     check(lib().sbwt_set_probe_length(probe_len))
 
 
-def set_table_kernel(enabled: bool = True) -> None:
-    """True (the default): an index with a k-mer table runs the read search
-    on the table kernel; False: on the general kernel.  Results never depend
+TABLE_KERNEL_DEFAULT = -1
+
+
+def set_table_kernel(mode: int = TABLE_KERNEL_DEFAULT) -> None:
+    """Read search kernel of an index with a k-mer table: 0 general, 1 table
+    (True), 2..5 walks kernel with (walks per lane, blocks per SM) = (1, 5),
+    (2, 4), (2, 3), (4, 2), -1 the library default.  Results never depend
     on it."""
-    check(lib().sbwt_set_table_kernel(int(enabled)))
+    check(lib().sbwt_set_table_kernel(int(mode)))
 
 
 def set_l2_window(enabled: bool = True) -> None:
@@ -249,6 +254,12 @@ class SbwtIndex:
         check(lib().sbwt_index_get_info(self._h, C.byref(info)))
         self.device_bytes = info.device_bytes
         return nb.value
+
+    def filter_bytes(self) -> int:
+        """Size of the k-mer filter in front of the k-mer table (0 when absent)."""
+        info = IndexInfo()
+        check(lib().sbwt_index_get_info(self._h, C.byref(info)))
+        return int(info.kmer_filter_bytes)
 
     def search_reads(self, chars, read_ends, out=None, move_to_key_kmer: bool = False,
                      per_kmer_walk: bool = False, stream: int = 0):

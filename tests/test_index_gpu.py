@@ -13,7 +13,10 @@ from helpers import FIXTURE_FILES, GOLDEN, golden_sbwt_path, synthetic, oracle_i
 pytestmark = pytest.mark.gpu
 
 # the library's default choice of read search kernel for indexes with a k-mer table
-DEFAULT_TABLE_KERNEL = True
+DEFAULT_TABLE_KERNEL = S.TABLE_KERNEL_DEFAULT
+# read search kernels of an index with a k-mer table: general, table, and the
+# walks kernel as (walks per lane, blocks per SM) = (1, 5), (2, 4), (2, 3), (4, 2)
+KERNEL_MODES = [0, 1, 2, 3, 4, 5]
 
 
 @pytest.fixture(scope="module")
@@ -253,14 +256,16 @@ def test_kmer_table_on_and_off(k):
     assert np.array_equal(idx.search_reads(chars, ends, per_kmer_walk=True), exp)
 
 
-@pytest.mark.parametrize("kernel", [True, False])
+@pytest.mark.parametrize("kernel", KERNEL_MODES)
 @pytest.mark.parametrize("seed", [21, 22])
 @pytest.mark.parametrize("k", [3, 15, 31])
 def test_table_kernel_and_general_kernel_match_oracle(kernel, seed, k):
-    """With a k-mer table the read search runs on the table kernel (stream
-    steps, group scans and table lookups only) or on the general kernel;
-    both give the oracle's results on reads with errors, N, empty and short
-    reads, at several tile sizes (k-mers of one read split across tiles)."""
+    """With a k-mer table the read search runs on the general kernel, the
+    table kernel (stream steps, group scans and table lookups only) or the
+    walks kernel (the same steps behind the k-mer filter, several tiles per
+    lane, 32-byte result stores); all give the oracle's results on reads
+    with errors, N, empty and short reads, at several tile sizes (k-mers of
+    one read split across tiles, tiles that are not multiples of 4)."""
     g, path, sb = synthetic(30 + seed, 3, 5000, k, 2, 0.02)
     idx = S.SbwtIndex.open(path)
     assert idx.set_kmer_table(True) > 0
@@ -269,7 +274,7 @@ def test_table_kernel_and_general_kernel_match_oracle(kernel, seed, k):
     exp = oracle_results(oracle_index(path, min(8, k)), chars, ends)
     S.set_table_kernel(kernel)
     try:
-        for tile in (0, 16, 100, 5000):
+        for tile in (0, 16, 37, 100, 5000):
             S.set_launch_config(tile=tile)
             assert np.array_equal(idx.search_reads(chars, ends), exp), tile
     finally:
@@ -277,9 +282,12 @@ def test_table_kernel_and_general_kernel_match_oracle(kernel, seed, k):
         S.set_launch_config()
 
 
-def test_table_kernel_device_pointers_and_capacity():
-    """The table kernel through device pointers: exact, and it writes no slot
-    past the k-mer count (the guard slots keep their fill)."""
+@pytest.mark.parametrize("kernel", KERNEL_MODES[1:])
+@pytest.mark.parametrize("shift", [0, 1, 3])
+def test_table_kernel_device_pointers_and_capacity(kernel, shift):
+    """The table and walks kernels through device pointers: exact, they write
+    no slot past the k-mer count (the guard slots keep their fill), also
+    when the output is not 32-byte aligned (shift: 8-byte elements)."""
     import torch
     g, path, sb = synthetic(31, 3, 5000, 31, 2, 0.02)
     idx = S.SbwtIndex.open(path)
@@ -289,12 +297,14 @@ def test_table_kernel_device_pointers_and_capacity():
     exp = oracle_results(oracle_index(path, 8), chars, ends)
     d_chars = torch.from_numpy(chars.copy()).cuda()
     d_ends = torch.from_numpy(ends.view(np.int64).copy()).cuda()
-    out = torch.full((len(exp) + 64,), -7, dtype=torch.int64, device="cuda")
-    S.set_table_kernel(True)
+    buf = torch.full((len(exp) + 64 + shift,), -7, dtype=torch.int64, device="cuda")
+    out = buf[shift:]
+    S.set_table_kernel(kernel)
     try:
         assert idx.search_reads(d_chars, d_ends, out=out) == len(exp)
     finally:
         S.set_table_kernel(DEFAULT_TABLE_KERNEL)
-    got = out.cpu().numpy()
-    assert np.array_equal(got[:len(exp)].view(np.uint64), exp)
-    assert (got[len(exp):] == -7).all()
+    got = buf.cpu().numpy()
+    assert (got[:shift] == -7).all()
+    assert np.array_equal(got[shift:shift + len(exp)].view(np.uint64), exp)
+    assert (got[shift + len(exp):] == -7).all()

@@ -198,3 +198,102 @@ def test_stream_rule_reaches_every_branch(k, monkeypatch):
                               len_max=250, sub=0.03, n_rate=0.01)
     _check(path, chars, ends)
     assert all(seen.values()), seen
+
+
+# ---------------------------------------------------------------------------
+# The k-mer filter in front of the table (csrc/kmer_table.cu, used by
+# search_walks_kernel): a blocked Bloom filter, 10 bits per k-mer, one 64-bit
+# word per key (word = the high bits of the key's SplitMix64 hash times the
+# word count, >> 64), four bits per key (hash bits 0-5, 6-11, 12-17, 18-23).
+# ---------------------------------------------------------------------------
+M64 = (1 << 64) - 1
+
+
+def kmer_mix(z: int) -> int:
+    z = ((z ^ (z >> 30)) * 0xbf58476d1ce4e5b9) & M64
+    z = ((z ^ (z >> 27)) * 0x94d049bb133111eb) & M64
+    return z ^ (z >> 31)
+
+
+def filter_word_bits(key: int, n_words: int):
+    z = kmer_mix(key)
+    bits = 0
+    for sh in (0, 6, 12, 18):
+        bits |= 1 << ((z >> sh) & 63)
+    return (z * n_words) >> 64, bits
+
+
+def build_filter(keys, bits_per_kmer: int = 10):
+    n_words = max((len(keys) * bits_per_kmer + 63) // 64, 1)
+    words = [0] * n_words
+    for key in keys:
+        w, b = filter_word_bits(key, n_words)
+        words[w] |= b
+    return words
+
+
+def filter_passes(words, key: int) -> bool:
+    w, b = filter_word_bits(key, len(words))
+    return (words[w] & b) == b
+
+
+def walks_rule_search(bv: BitVectors, table: dict, words, read: bytes, stats) -> list:
+    """table_rule_search with the filter in front of every table lookup: a
+    key the filter rejects is not found without a lookup."""
+    k, out, v = bv.k, [], None
+    codes = [CODE.get(ch) for ch in read]
+    for pos in range(len(read) - k + 1):
+        window = codes[pos:pos + k]
+        if any(x is None for x in window):
+            out.append(O.INVALID)
+            v = None
+            continue
+        if v is not None:
+            v = stream_step(bv, v, window[-1])
+        else:
+            key = 0
+            for x in window:
+                key = (key << 2) | x
+            if filter_passes(words, key):
+                stats["lookups"] += 1
+                v = table.get(key)
+                stats["false_pass"] += v is None
+            else:
+                stats["rejected"] += 1
+                v = None
+        out.append(O.NOT_FOUND if v is None else v)
+    return out
+
+
+@pytest.mark.parametrize("k", [15, 31])
+def test_filter_rule_matches_oracle(k):
+    """The filter has no false negatives (every table key passes), so the
+    walks kernel's rule gives the oracle's results; it rejects most absent
+    k-mers before a table lookup."""
+    g, path, sb = synthetic(80 + k, 3, 3000, k, 2, 0.02)
+    bv = BitVectors(sb)
+    table = kmer_table(bv)
+    words = build_filter(list(table))
+    assert all(filter_passes(words, key) for key in table)
+    chars, ends = mixed_reads(g, 90 + k, 300, median=90, sigma=0.6, len_min=0,
+                              len_max=300, sub=0.02, n_rate=0.005, frac=0.5)
+    exp = oracle_results(oracle_index(path, 8), chars, ends)
+    stats = {"lookups": 0, "false_pass": 0, "rejected": 0}
+    got = []
+    for r in T.split_reads(chars, ends):
+        got.extend(walks_rule_search(bv, table, words, bytes(r), stats))
+    assert np.array_equal(np.array(got, dtype=np.uint64), exp)
+    absent = stats["rejected"] + stats["false_pass"]
+    assert absent > 1000
+    assert stats["false_pass"] / absent < 0.04  # about 1.5 % at 10 bits per k-mer
+
+
+def test_filter_false_positive_rate():
+    """On random keys the filter passes about 1-2 % (10 bits per key, 4 bits
+    in one 64-bit word)."""
+    rng = np.random.default_rng(5)
+    keys = [int(x) for x in rng.integers(0, 1 << 62, 40000, dtype=np.int64)]
+    words = build_filter(keys)
+    probes = [int(x) for x in rng.integers(0, 1 << 62, 40000, dtype=np.int64)]
+    fp = sum(filter_passes(words, p) for p in probes) / len(probes)
+    assert 0.005 < fp < 0.03, fp

@@ -114,6 +114,7 @@ def bench_batched(args, idx, S, torch, dev, scratch):
     t_batch = e0.elapsed_time(e1) / 3 / 1e3
     exact = bool(torch.equal(d_out, d_plain))
     S.set_launch_config()
+    S.set_table_kernel(args.kernel)
     return {"workload": "256 files vs the 100 Mbp index, reads/file log-uniform [50, 1e5] "
                         "(full-size range [1e3, 2e6] scaled 1/20), 10% files of 1-10 kbp "
                         "reads, 5% substitutions", "files": len(files),
@@ -122,7 +123,177 @@ def bench_batched(args, idx, S, torch, dev, scratch):
             "speedup": t_plain / t_batch, "bit_exact": exact, "autotune": tune}
 
 
-def bench_colors_and_serving(args, S, torch, dev, tmpdir, rank):
+# batched mixed workload at its full size: 256 files, reads/file log-uniform in
+# [1e3, 2e6], 10 % of the files with 1-10 kbp reads, the rest 100 bp, 5 %
+# substitutions (about 4.5e10 chars in all).
+CFG4_FULL = dict(n_files=256, reads_lo=1_000, reads_hi=2_000_000, long_frac=0.1,
+                 short_len=100, long_lo=1000, long_hi=10_000, sub=0.05,
+                 short_pool=2_000_000, long_pool=100_000, wave_chars=6_000_000_000)
+
+
+def _wave_checksum(torch, out, n):
+    """Position-weighted wrapping sum of the first n results (chunked)."""
+    total = torch.zeros((), dtype=torch.int64, device=out.device)
+    step = 1 << 27
+    for lo in range(0, n, step):
+        hi = min(n, lo + step)
+        w = torch.arange(2 * lo + 1, 2 * hi + 1, 2, dtype=torch.int64, device=out.device)
+        total += (out[lo:hi] * w).sum()
+    return int(total.item())
+
+
+def bench_batched_full(args, idx, S, torch, dev):
+    """The batched workload at its stated size, streamed in waves of files
+    that fit the device: the files' reads are cyclic runs of two seeded read
+    pools kept on the device (2 M short reads, 100 k long reads), so a wave
+    is assembled by device copies.  Per wave: plain = one sbwt_search_reads
+    call per file (each synchronous, the library defaults); batched = one
+    call over the whole wave (one persistent launch), with the library
+    defaults and with the autotuner's choice.  Bit-exact: equal
+    position-weighted checksums of all results and equal first 1 M results
+    of every wave."""
+    import sbwt_tools as T
+    c = CFG4_FULL
+    rng = np.random.default_rng(17)
+    g = T.gen_genomes(20240601, CFG["n_genomes"], CFG["genome_len"], CFG["n_founders"],
+                      CFG["sub"], CFG["sub"], CFG["indel"])
+    pools = {}
+    for kind, n, med, sig, lo, hi in (("short", c["short_pool"], c["short_len"], 0.0,
+                                       c["short_len"], c["short_len"]),
+                                      ("long", c["long_pool"], 3000, 0.6, c["long_lo"],
+                                       c["long_hi"])):
+        ch, en = T.gen_reads(4242 + len(pools), g, n, 1.0, med, sig, lo, hi, c["sub"], 0.0)
+        lens = np.diff(np.concatenate([[0], en.astype(np.int64)]))
+        pools[kind] = (torch.from_numpy(ch).to(f"cuda:{dev}"), lens,
+                       np.concatenate([[0], np.cumsum(lens)]))
+    files = []
+    for f in range(c["n_files"]):
+        n = int(np.exp(rng.uniform(np.log(c["reads_lo"]), np.log(c["reads_hi"]))))
+        kind = "long" if rng.random() < c["long_frac"] else "short"
+        files.append((kind, int(rng.integers(0, len(pools[kind][1]))), n))
+
+    def file_arrays(kind, start, n):
+        d_ch, lens, cum = pools[kind]
+        P = len(lens)
+        segs, lsegs, left, s0 = [], [], n, start
+        while left:
+            take = min(left, P - s0)
+            segs.append(d_ch[int(cum[s0]):int(cum[s0 + take])])
+            lsegs.append(lens[s0:s0 + take])
+            left -= take
+            s0 = 0
+        return segs, np.concatenate(lsegs)
+
+    def file_chars(f):
+        kind, start, n = files[f]
+        lens = pools[kind][1]
+        P = len(lens)
+        full, rem = divmod(n, P)
+        cum = pools[kind][2]
+        tot = full * int(cum[P]) + (int(cum[min(start + rem, P)] - cum[start]) +
+                                    (int(cum[start + rem - P]) if start + rem > P else 0))
+        return tot
+
+    # waves of consecutive files up to wave_chars (a larger file is a wave)
+    waves, cur, cur_c = [], [], 0
+    for f in range(len(files)):
+        fc = file_chars(f)
+        if cur and cur_c + fc > c["wave_chars"]:
+            waves.append(cur)
+            cur, cur_c = [], 0
+        cur.append(f)
+        cur_c += fc
+    waves.append(cur)
+    stream = torch.cuda.current_stream(dev)
+    tot = {"plain": 0.0, "batched": 0.0, "batched_tuned": 0.0, "plain_tuned": 0.0}
+    n_kmers = n_chars = n_reads = 0
+    exact = True
+    tune = None
+    for wi, wave in enumerate(waves):
+        segs, lens, fk, fr = [], [], [], []
+        for f in wave:
+            s_, l_ = file_arrays(*files[f])
+            segs += s_
+            lens.append(l_)
+            fr.append(len(l_))
+        d_chars = torch.cat(segs)
+        lens = np.concatenate(lens)
+        ends = np.cumsum(lens).astype(np.uint64)
+        d_ends = torch.from_numpy(ends.view(np.int64)).to(f"cuda:{dev}")
+        n_k = idx.count_kmers(ends)
+        # per file: its chars, its ends (file-relative), its k-mer slots
+        rb = np.concatenate([[0], np.cumsum(fr)])
+        per_file = []
+        for i in range(len(wave)):
+            c0 = int(ends[rb[i] - 1]) if rb[i] else 0
+            c1 = int(ends[rb[i + 1] - 1])
+            e = torch.from_numpy((ends[rb[i]:rb[i + 1]] - c0).view(np.int64)).to(f"cuda:{dev}")
+            per_file.append((d_chars[c0:c1], e, idx.count_kmers(ends[rb[i]:rb[i + 1]] - c0)))
+        koff = np.concatenate([[0], np.cumsum([x[2] for x in per_file])])
+        d_out = torch.empty(n_k, dtype=torch.int64, device=f"cuda:{dev}")
+
+        def plain():
+            for i, (dc, de, k_) in enumerate(per_file):
+                if k_:
+                    idx.search_reads(dc, de, out=d_out[int(koff[i]):int(koff[i + 1])])
+            torch.cuda.synchronize()
+
+        def batched():
+            idx.search_reads(d_chars, d_ends, out=d_out)
+            torch.cuda.synchronize()
+
+        def timed(fn):
+            fn()  # warm (per-call workspaces grown)
+            t0 = time.perf_counter()
+            fn()
+            return time.perf_counter() - t0
+
+        S.set_launch_config()
+        tot["plain"] += timed(plain)
+        ref_ck = _wave_checksum(torch, d_out, n_k)
+        ref_head = d_out[:1 << 20].clone()
+        tot["batched"] += timed(batched)
+        exact &= _wave_checksum(torch, d_out, n_k) == ref_ck
+        exact &= bool(torch.equal(d_out[:1 << 20], ref_head))
+        if tune is None:  # the autotuner on the first wave, kept for the rest
+            tune = S.autotune(idx, d_chars, d_ends, sample_chars=256 << 20, use_cache=False)
+        else:
+            S.set_launch_config(presearch_letters=tune["presearch"],
+                                blocks_per_sm=tune["blocks_per_sm"], tile=tune["tile"])
+            S.set_table_kernel(tune["table_kernel"])
+        tot["batched_tuned"] += timed(batched)
+        exact &= _wave_checksum(torch, d_out, n_k) == ref_ck
+        tot["plain_tuned"] += timed(plain)
+        exact &= _wave_checksum(torch, d_out, n_k) == ref_ck
+        S.set_launch_config()
+        S.set_table_kernel(args.kernel)
+        n_kmers += n_k
+        n_chars += int(ends[-1])
+        n_reads += len(ends)
+        del d_out, d_chars, d_ends, per_file, segs
+        torch.cuda.empty_cache()
+    del pools
+    torch.cuda.empty_cache()
+    return {"workload": "256 files vs the 100 Mbp index at the stated size: reads/file "
+                        "log-uniform [1e3, 2e6], 10% files of 1-10 kbp reads (log-normal, "
+                        "median 3 kbp), the rest 100 bp, 5% substitutions; reads are cyclic "
+                        "runs of two seeded pools (2 M short, 100 k long reads) on the "
+                        "device; processed in waves of <= 6e9 chars",
+            "files": len(files), "waves": len(waves), "reads": int(n_reads),
+            "chars": int(n_chars), "kmers": int(n_kmers),
+            "plain_kmers_per_s": n_kmers / tot["plain"],
+            "batched_kmers_per_s": n_kmers / tot["batched"],
+            "plain_autotuned_kmers_per_s": n_kmers / tot["plain_tuned"],
+            "batched_autotuned_kmers_per_s": n_kmers / tot["batched_tuned"],
+            "speedup_same_launch_config": tot["plain"] / tot["batched"],
+            "speedup_autotuned": tot["plain_tuned"] / tot["batched_tuned"],
+            "speedup": tot["plain"] / tot["batched_tuned"],
+            "bit_exact": bool(exact), "autotune": tune,
+            "timing": "wall time around device-resident calls, each wave synchronised; "
+                      "chars assembled on the device outside the timed calls"}
+
+
+def bench_colors_and_serving(args, S, torch, dev, tmpdir, rank, resident_index=None):
     """Pseudoalignment reads/s (colors step, device-resident), the fused
     reads -> colors pipeline (host in, host out), the CPU oracle on a sample,
     and the serving loop's p50 / p99 latency at Poisson offered loads."""
@@ -191,10 +362,63 @@ def bench_colors_and_serving(args, S, torch, dev, tmpdir, rank):
     ids_h = d_ids[:int(ids_off_h[-1])].cpu().numpy()
     got = [ids_h[ids_off_h[r]:ids_off_h[r + 1]].tolist() for r in range(chk)]
     oc = O.OracleColors(O.ColorsFile.read(cp))
-    t1 = time.perf_counter()
     exp = oc.pseudoalign([found_h[offs_h[r]:offs_h[r + 1]] for r in range(chk)], [0] * chk,
                          [0] * chk, c["tau"])
+    # CPU baseline: the restatement on all host threads (OpenMP over reads),
+    # on a bounded sample; agreement = per-read id count and id checksum
+    n_cpu = min(args.colors_cpu_reads, n_reads)
+    offs_c = d_offs[:n_cpu + 1].cpu().numpy().view(np.uint64)
+    found_c = d_found[:int(offs_c[-1])].cpu().numpy().view(np.uint64)
+    zeros = np.zeros(n_cpu, np.uint64)
+    threads = os.cpu_count()
+    t1 = time.perf_counter()
+    cpu_n, cpu_ck = oc.pseudoalign_mt(found_c, offs_c, zeros, zeros, c["tau"], threads=threads)
     t_cpu = time.perf_counter() - t1
+    gio = d_ids_off[:n_cpu + 1].cpu().numpy()
+    gids = d_ids[:int(gio[-1])].cpu().numpy().astype(np.uint64)
+    gn = np.diff(gio).astype(np.uint64)
+    rank_in_read = np.arange(len(gids), dtype=np.uint64) - np.repeat(gio[:-1], gn.astype(np.int64)).astype(np.uint64) + 1
+    gck = np.zeros(n_cpu, np.uint64)
+    np.add.at(gck, np.repeat(np.arange(n_cpu), gn.astype(np.int64)), (gids + 1) * rank_in_read)
+    cpu_agree = bool(np.array_equal(cpu_n, gn) and np.array_equal(cpu_ck, gck))
+    # plain colors flow (the reference's ColorSearcher + printer): per batch
+    # the R x C counts to the host, then the threshold on the host
+    # (ceil((double) size * tau)); timed on a bounded sample
+    n_plain = min(args.colors_plain_reads, n_reads)
+    pb = min(n_plain, 100_000)
+    d_cnt = torch.empty((pb, ci.num_colors), dtype=torch.int32, device=f"cuda:{dev}")
+    h_cnt = torch.empty((pb, ci.num_colors), dtype=torch.int32).pin_memory()
+    sizes = (d_offs[1:] - d_offs[:-1])[:n_plain].cpu().numpy()
+    minimum = np.ceil(sizes.astype(np.float64) * c["tau"]).astype(np.int64)
+
+    def plain_colors():
+        n_plain_ids = 0
+        for lo in range(0, n_plain, pb):
+            m = min(pb, n_plain - lo)
+            offs_b = (d_offs[lo:lo + m + 1] - d_offs[lo]).contiguous()
+            S.check(L.sbwt_color_counts(ci._h, d_found[int(d_offs[lo].item()):].data_ptr(),
+                                        offs_b.data_ptr(), m, d_cnt.data_ptr(),
+                                        S.DEVICE_POINTERS, stream.cuda_stream))
+            h_cnt[:m].copy_(d_cnt[:m], non_blocking=True)
+            torch.cuda.synchronize()
+            cnt = h_cnt[:m].numpy()
+            mins = minimum[lo:lo + m]
+            n_plain_ids += int(((cnt >= mins[:, None]) & (mins[:, None] > 0)).sum())
+        return n_plain_ids
+
+    plain_colors()
+    t1 = time.perf_counter()
+    n_plain_ids = plain_colors()
+    t_plain = time.perf_counter() - t1
+    e0.record(stream)
+    S.check(L.sbwt_pseudoalign(ci._h, d_found.data_ptr(), d_offs.data_ptr(), None, None,
+                               n_plain, c["tau"], S.DEVICE_POINTERS, d_ids.data_ptr(), cap,
+                               d_ids_off.data_ptr(), stream.cuda_stream))
+    fused_ids_h = d_ids_off[n_plain].item()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_fused = e0.elapsed_time(e1) / 1e3
+    del d_cnt, h_cnt
     colors = {"workload": "2000 genomes x 100 kbp from 8 founders (1-5% divergence), k=31, "
                           f"{n_reads} reads x 150 bp, 0.5% substitutions, tau 0.7",
               "nodes": nodes, "reads": n_reads, "kmers": int(n_k), "ids": n_ids,
@@ -205,8 +429,20 @@ def bench_colors_and_serving(args, S, torch, dev, tmpdir, rank):
                                 "files_identical_to_host_build": bool(build_same),
                                 "note": "first GPU call of the process, incl. CUDA start-up "
                                         "costs and writing both files"},
-              "cpu_baseline": {"value": chk / t_cpu, "unit": "reads/s", "cores": 1,
-                               "kind": "port", "sample": f"first {chk} reads"}}
+              "cpu_baseline": {"value": n_cpu / t_cpu, "unit": "reads/s", "cores": threads,
+                               "kind": "port", "sample": f"first {n_cpu} reads (OpenMP "
+                               "restatement of d_color_search + d_post_process + the "
+                               "threshold, oracle/sbwt_oracle.c)",
+                               "agrees_with_gpu": cpu_agree},
+              "plain_vs_fused": {
+                  "sample_reads": n_plain,
+                  "plain_reads_per_s": n_plain / t_plain,
+                  "fused_reads_per_s": n_plain / t_fused,
+                  "speedup": t_plain / t_fused,
+                  "same_id_count": int(n_plain_ids) == int(fused_ids_h),
+                  "plain": "the reference's flow: per batch of 100000 reads the R x C counts "
+                           "(sbwt_color_counts) copied to the host, threshold on the host",
+                  "fused": "sbwt_pseudoalign: counts and threshold on the device, sorted ids"}}
     del d_res, d_found, d_ids, found_mask, res2
     torch.cuda.empty_cache()
     # fused reads -> colors pipeline from host memory (CUDA graph per batch)
@@ -225,7 +461,13 @@ def bench_colors_and_serving(args, S, torch, dev, tmpdir, rank):
     # serving loop: Poisson arrivals, log-uniform request sizes in [1, 1e5]
     srv = S.Server(idx, ci, batch_chars=32 << 20, batch_reads=1 << 18, slots=3, tau=c["tau"])
     rng = np.random.default_rng(11)
-    serving = {"offline_reads_per_s": colors["fused_pipeline_reads_per_s"], "loads": []}
+    serving = {"offline_reads_per_s": colors["fused_pipeline_reads_per_s"], "loads": [],
+               "resident": {"colors_workload_sbwt_bytes": int(idx.device_bytes),
+                            "index_workload_sbwt_bytes":
+                            int(resident_index.device_bytes) if resident_index else 0,
+                            "color_index": "resident (sbwt_colors_open)"},
+               "admission": "slots open on demand while the device has a slot's bytes free "
+                            "above an eighth of its memory (sbwt_server_create)"}
     for offered in (1e5, 1e6, 1e7, 0.8 * colors["fused_pipeline_reads_per_s"]):
         mean_size = (1e5 - 1) / np.log(1e5)
         rate = offered / mean_size
@@ -259,7 +501,7 @@ def bench_colors_and_serving(args, S, torch, dev, tmpdir, rank):
         stop.set()
         th.join()
         st = srv.stats()
-        serving["loads"].append({"offered_reads_per_s": offered,
+        serving["loads"].append({"slots": srv.slots(), "offered_reads_per_s": offered,
                                  "achieved_reads_per_s": st["reads"] / max(st["elapsed_s"], 1e-9),
                                  "arrival_window_s": t_window, "drain_s": st["elapsed_s"] - t_window,
                                  "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3,
@@ -283,6 +525,10 @@ def parse():
                     help="skip the batched, colors and serving sections")
     ap.add_argument("--colors-reads", type=int, default=CFG3["n_reads"])
     ap.add_argument("--serve-seconds", type=float, default=3.0)
+    ap.add_argument("--colors-cpu-reads", type=int, default=200_000)
+    ap.add_argument("--no-full-batched", action="store_true",
+                    help="skip the full-size batched workload")
+    ap.add_argument("--colors-plain-reads", type=int, default=500_000)
     ap.add_argument("--kernel", type=int, default=-1,
                     help="read search kernel with a k-mer table (sbwt_set_table_kernel): "
                          "0 general, 1 table, 2..5 walks variants, -1 library default")
@@ -909,13 +1155,20 @@ def main():
         except Exception as e:
             extra["cfg1"] = {"error": repr(e)}
         try:
-            extra["batched"] = bench_batched(args, idx, S, torch, dev, d_out)
+            extra["batched_small_files"] = bench_batched(args, idx, S, torch, dev, d_out)
         except Exception as e:  # reported, never hides the headline
-            extra["batched"] = {"error": repr(e)}
+            extra["batched_small_files"] = {"error": repr(e)}
         del d_out, d_chars, d_ends
         torch.cuda.empty_cache()
+        if not args.no_full_batched:
+            try:
+                extra["batched"] = bench_batched_full(args, idx, S, torch, dev)
+            except Exception as e:  # reported, never hides the headline
+                extra["batched"] = {"error": repr(e)}
+            torch.cuda.empty_cache()
         try:
-            extra.update(bench_colors_and_serving(args, S, torch, dev, tmp.name, rank))
+            extra.update(bench_colors_and_serving(args, S, torch, dev, tmp.name, rank,
+                                                  resident_index=idx))
         except Exception as e:
             extra["colors"] = {"error": repr(e)}
 

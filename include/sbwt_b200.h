@@ -269,13 +269,18 @@ int sbwt_pipeline_run(sbwt_pipeline_t *p, const char *chars, uint64_t n_chars,
                       uint64_t *n_results, uint32_t *ids, uint64_t ids_capacity,
                       uint64_t *ids_offsets);
 
-/* A serving loop over resident indexes: `slots` pipelines of batch_chars /
- * batch_reads (shrunk at creation until they fit in half of the free device
- * memory).  Requests of any size are accepted from any thread; a background
- * thread keeps every free slot busy with the pending requests in arrival
- * order (continuous batching: a request arriving while batches run joins the
- * next free slot and runs concurrently with them; a large request is split
- * over several batches).  Results are identical to the single calls. */
+/* A serving loop over resident indexes: up to `slots` pipelines of
+ * batch_chars / batch_reads (shrunk at creation until one fits in half of the
+ * free device memory).  Requests of any size are accepted from any thread; a
+ * background thread keeps every open slot busy with the pending requests in
+ * arrival order (continuous batching: a request arriving while batches run
+ * joins the next free slot and runs concurrently with them; a large request
+ * is split over several batches).  Admission by free device memory: one slot
+ * opens at creation; another opens only when batches wait, every open slot
+ * is busy and the device has a slot's bytes free above a reserve of an eighth
+ * of its memory (so other tenants of the GPU keep their headroom); otherwise
+ * the batch waits for a running slot.  Results are identical to the single
+ * calls. */
 int sbwt_server_create(const sbwt_index_t *index, const sbwt_colors_t *colors,
                        uint64_t batch_chars, uint64_t batch_reads, int slots,
                        uint32_t flags, double tau, sbwt_server_t **out);
@@ -296,6 +301,10 @@ int sbwt_server_wait(sbwt_server_t *s, uint64_t request_id, double timeout_ms,
 int sbwt_server_stats(sbwt_server_t *s, double *p50_s, double *p99_s,
                       uint64_t *requests_done, uint64_t *reads_done,
                       uint64_t *batches, double *elapsed_s, int reset);
+/* Slots open now, the device bytes one slot holds, and how many times a
+ * waiting batch found too little free device memory to open a slot. */
+int sbwt_server_slots(sbwt_server_t *s, int *open_slots, uint64_t *slot_bytes,
+                      uint64_t *denied);
 
 /* ------------------------------------------------------------------------ */
 /* Host I/O in the reference's file formats (no GPU involved)               */
@@ -387,6 +396,10 @@ int sbwt_set_probe_length(uint32_t probe_len);
  *   negative = the default.
  * Results never depend on it.  Returns SBWT_E_INVALID above 5. */
 int sbwt_set_table_kernel(int mode);
+/* The process-wide launch configuration (set by sbwt_set_launch_config,
+ * sbwt_set_table_kernel, sbwt_autotune); any pointer may be NULL. */
+int sbwt_get_launch_config(uint32_t *presearch_letters, uint32_t *blocks_per_sm,
+                           uint64_t *tile, uint64_t *chunk_chars, int *table_kernel);
 /* Persisting-L2 access-policy window over the index's rank blocks on the
  * search launches (0 = off, the default; 1 = on: sets this context's
  * persisting-L2 size). */
@@ -402,10 +415,14 @@ int sbwt_profile_enable(int enabled, int count_work);
 int sbwt_measure_random_sectors(int device, uint64_t bytes, int chains,
                                 double *gbs, double *sectors_per_s);
 /* Autotuner: times the read search on the first sample_chars chars of a
- * device-resident batch over presearch depth 8..12, tile size (k-mers per
- * lane work unit) {auto, 64, 256, 1024} and blocks per SM {2, 3, 4, 6, 8},
- * checks that every configuration gives the same results, and makes the
- * fastest the process-wide launch configuration. */
+ * device-resident batch over a first axis, tile size (k-mers per walk work
+ * unit) {auto, 64, 256, 1024} and 256-thread blocks per SM in the grid
+ * {2, 3, 4, 6, 8}, checks that every configuration gives the same results,
+ * and makes the fastest the process-wide launch configuration.  The first
+ * axis is the read search kernel (sbwt_set_table_kernel 1..5: the table
+ * kernel, or the walks kernel with 1, 2 or 4 walks per lane) when the index
+ * has its k-mer table, else the presearch depth (8 up to the index's).
+ * sbwt_get_launch_config reads the choice back. */
 int sbwt_autotune(const sbwt_index_t *index, const char *d_chars,
                   uint64_t n_chars, const uint64_t *d_read_ends,
                   uint64_t n_reads, uint64_t sample_chars,

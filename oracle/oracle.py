@@ -76,6 +76,10 @@ def lib():
                                          C.c_uint64, C.c_double, C.c_int, C.c_int,
                                          C.c_void_p, U64P, C.c_void_p]
         L.oracle_pseudoalign.restype = C.c_uint64
+        L.oracle_pseudoalign_mt.argtypes = [C.c_void_p, U64P, U64P, U64P, U64P,
+                                            C.c_uint64, C.c_double, C.c_int, C.c_int,
+                                            U64P, U64P, C.c_int]
+        L.oracle_pseudoalign_mt.restype = C.c_uint64
         _lib = L
     return _lib
 
@@ -462,6 +466,24 @@ class OracleColors:
             _p(isd), _p(isd0), _p(isd12), _p(km), _p(km0), _p(km12), _p(arrs[4]),
             tc.color_set_idxs_width, tc.num_colors)
 
+    def pseudoalign_mt(self, flat_idx, idx_offsets, not_found, invalid, tau=0.7,
+                       include_not_found=False, include_invalid=False, threads=None):
+        """The same per read, on `threads` host threads: (number of ids,
+        ids checksum) per read."""
+        idx = np.concatenate([np.ascontiguousarray(flat_idx, np.uint64),
+                              np.zeros(1, np.uint64)])
+        offs = np.ascontiguousarray(idx_offsets, np.uint64)
+        n_reads = len(offs) - 1
+        nf = np.ascontiguousarray(not_found, np.uint64)
+        inv = np.ascontiguousarray(invalid, np.uint64)
+        n_ids = np.zeros(max(1, n_reads), np.uint64)
+        ck = np.zeros(max(1, n_reads), np.uint64)
+        lib().oracle_pseudoalign_mt(C.byref(self.s), _p(idx), _p(offs), _p(nf), _p(inv),
+                                    n_reads, tau, int(include_not_found),
+                                    int(include_invalid), _p(n_ids), _p(ck),
+                                    threads or os.cpu_count())
+        return n_ids[:n_reads], ck[:n_reads]
+
     def pseudoalign(self, found_lists, not_found, invalid, tau=0.7,
                     include_not_found=False, include_invalid=False,
                     want_counts=False):
@@ -580,6 +602,13 @@ def padding_free_batch(found_lists, batch_multiple: int = 1024):
     wi = np.zeros(len(lists) + 1, np.uint64)
     wi[1:] = np.cumsum([len(x) // 32 for x in lists])
     return keep, lists, warped, wi
+
+
+def ids_checksum(rows) -> np.ndarray:
+    """Per read, the checksum oracle_pseudoalign_mt reports: sum over the
+    read's ascending ids c of (c + 1) * (position in the list, from 1)."""
+    return np.array([sum((c + 1) * (i + 1) for i, c in enumerate(r)) for r in rows],
+                    dtype=np.uint64)
 
 
 def threshold_minimum(seq_size: int, tau: float) -> int:

@@ -344,6 +344,44 @@ u64 oracle_pseudoalign(const oracle_colors_index *ci, const u64 *idx,
   return n_ids;
 }
 
+/* oracle_pseudoalign over reads on `threads` host threads (OpenMP), for the
+ * colors CPU baseline: per read only the number of passing colors and a
+ * checksum of their ids (sum over passing c of (c + 1) * (index in the read's
+ * list + 1)), so that no R x C count matrix is kept.  Returns the total. */
+u64 oracle_pseudoalign_mt(const oracle_colors_index *ci, const u64 *idx,
+                          const u64 *idx_offsets, const u64 *not_found,
+                          const u64 *invalid, u64 n_reads, double tau,
+                          int include_not_found, int include_invalid,
+                          u64 *n_ids_out, u64 *checksum_out, int threads) {
+  u64 total = 0;
+#pragma omp parallel num_threads(threads) reduction(+ : total)
+  {
+    u64 *counts = (u64 *)malloc(ci->num_colors * sizeof(u64));
+#pragma omp for schedule(dynamic, 256)
+    for (long rr = 0; rr < (long)n_reads; ++rr) {
+      const u64 r = (u64)rr;
+      memset(counts, 0, ci->num_colors * sizeof(u64));
+      u64 found = idx_offsets[r + 1] - idx_offsets[r];
+      for (u64 t = idx_offsets[r]; t < idx_offsets[r + 1]; ++t)
+        add_color_set(ci, idx[t], counts);
+      u64 seq_size = found + (include_not_found ? not_found[r] : 0) +
+                     (include_invalid ? invalid[r] : 0);
+      u64 minimum = (u64)ceil((double)seq_size * tau);
+      u64 n = 0, h = 0;
+      for (u64 c = 0; minimum > 0 && c < ci->num_colors; ++c)
+        if (counts[c] >= minimum) {
+          ++n;
+          h += (c + 1) * n;
+        }
+      n_ids_out[r] = n;
+      checksum_out[r] = h;
+      total += n;
+    }
+    free(counts);
+  }
+  return total;
+}
+
 /* Sectors-touched instrumentation for the index walk: counts, per k-mer, the
  * distinct 32-byte sectors of the A/C/G/T bitvectors that the reference walk
  * (steps p..k-1, stopping at the first empty interval) reads.  Used only to

@@ -284,6 +284,19 @@ int sbwt_set_launch_config(uint32_t presearch_letters, uint32_t blocks_per_sm,
   return SBWT_OK;
 }
 
+// The process-wide launch configuration (what sbwt_set_launch_config,
+// sbwt_set_table_kernel and sbwt_autotune set); any pointer may be NULL.
+int sbwt_get_launch_config(uint32_t *presearch_letters, uint32_t *blocks_per_sm,
+                           uint64_t *tile, uint64_t *chunk_chars, int *table_kernel) {
+  const LaunchConfig &c = default_launch_config();
+  if (presearch_letters) *presearch_letters = c.presearch_letters;
+  if (blocks_per_sm) *blocks_per_sm = c.blocks_per_sm;
+  if (tile) *tile = c.tile;
+  if (chunk_chars) *chunk_chars = c.chunk_chars;
+  if (table_kernel) *table_kernel = (int)c.table_kernel;
+  return SBWT_OK;
+}
+
 // Tuning hook: persisting-L2 access-policy window over the index's rank
 // blocks on the search launches (0 = off, the default; 1 = on).
 int sbwt_set_l2_window(int enabled) {

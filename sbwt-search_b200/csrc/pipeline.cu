@@ -301,27 +301,72 @@ struct ServerImpl {
   std::thread worker;
   Clock::time_point t0 = Clock::now();
 
+  // Admission by free device memory.  A slot (one pipeline: its device
+  // buffers and CUDA graph) holds about slot_bytes.  The server opens its
+  // first slot at creation (shrunk until it fits in half of the free
+  // memory) and opens more, up to max_slots, only while batches are waiting
+  // and the device still has slot_bytes free above a reserve of an eighth of
+  // its memory; otherwise waiting batches queue for a running slot.
+  u64 slot_chars_ = 0, slot_reads_ = 0, slot_bytes = 0;
+  u32 flags_ = 0;
+  double tau_ = 0;
+  int max_slots = 1;
+  u64 denied = 0;  // times a waiting batch found no free memory for a slot
+
+  static double slot_size(const ColorsImpl *ci, u64 chars, u64 reads) {
+    const double per_char = 1 + 8 + 0.375 + 1.0 / 16 + 1;  // chars, results, packing, tiles
+    const double per_read = 8 * 2 + (ci ? (ci->num_colors / 8.0 + 4 + 8 + 64 * 4) : 0);
+    return chars * per_char + reads * per_read;
+  }
+
   ServerImpl(const IndexImpl *ix_, const ColorsImpl *ci_, u64 slot_chars, u64 slot_reads,
              int n_slots, u32 flags, double tau)
       : ix(ix_), ci(ci_) {
     if (n_slots < 1 || n_slots > 8) throw Error(SBWT_E_INVALID, "slots must be 1..8");
     DeviceGuard g(ix->device);
-    // admission by free device memory: shrink the slots until they fit in
-    // half of the free memory
     size_t free_b = 0, total_b = 0;
     SBWT_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const double per_char = 1 + 8 + 0.375 + 1.0 / 16 + 1;  // chars, results, packing, tiles
-    const double per_read = 8 * 2 + (ci ? (ci->num_colors / 8.0 + 4 + 8 + 64 * 4) : 0);
-    while ((slot_chars * per_char + slot_reads * per_read) * n_slots > 0.5 * (double)free_b &&
+    while (slot_size(ci, slot_chars, slot_reads) > 0.5 * (double)free_b &&
            slot_chars > (1u << 20)) {
       slot_chars /= 2;
       slot_reads = std::max<u64>(slot_reads / 2, 1024);
     }
-    for (int i = 0; i < n_slots; ++i)
-      slots.emplace_back(std::make_unique<PipelineImpl>(ix, ci, slot_chars, slot_reads, flags, tau));
-    slot_pieces.resize(n_slots);
-    busy.assign(n_slots, false);
+    slot_chars_ = slot_chars;
+    slot_reads_ = slot_reads;
+    slot_bytes = (u64)slot_size(ci, slot_chars, slot_reads);
+    flags_ = flags;
+    tau_ = tau;
+    max_slots = n_slots;
+    slots.emplace_back(std::make_unique<PipelineImpl>(ix, ci, slot_chars, slot_reads, flags, tau));
+    slot_pieces.resize(1);
+    busy.assign(1, false);
     worker = std::thread([this] { run(); });
+  }
+
+  // Opens one more slot when batches wait, every slot is busy and the
+  // device has room for it; called by the worker thread only.
+  bool admit_slot() {
+    if ((int)slots.size() >= max_slots) return false;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    if ((double)free_b < (double)slot_bytes + (double)total_b / 8) {
+      ++denied;
+      return false;
+    }
+    try {
+      auto p = std::make_unique<PipelineImpl>(ix, ci, slot_chars_, slot_reads_, flags_, tau_);
+      std::lock_guard<std::mutex> lk(mu);
+      slots.push_back(std::move(p));
+      slot_pieces.emplace_back();
+      busy.push_back(false);
+    } catch (const Error &) {
+      ++denied;  // the allocation failed after all: keep serving on the open slots
+      return false;
+    }
+    return true;
   }
 
   ~ServerImpl() {
@@ -461,6 +506,15 @@ struct ServerImpl {
           deliver((int)s);
           progressed = true;
         }
+      {
+        bool all_busy = true, waiting = false;
+        for (bool b : busy) all_busy &= b;
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          waiting = !pending.empty();
+        }
+        if (all_busy && waiting) admit_slot();
+      }
       for (size_t s = 0; s < slots.size(); ++s) {
         if (busy[s]) continue;
         bool filled = false;
@@ -696,6 +750,19 @@ int sbwt_server_stats(sbwt_server_t *s, double *p50_s, double *p99_s, uint64_t *
   return SBWT_OK;
 }
 
+int sbwt_server_slots(sbwt_server_t *s, int *open_slots, uint64_t *slot_bytes,
+                      uint64_t *denied) {
+  if (!s) {
+    set_last_error("null argument");
+    return SBWT_E_INVALID;
+  }
+  std::lock_guard<std::mutex> g(s->impl->mu);
+  if (open_slots) *open_slots = (int)s->impl->slots.size();
+  if (slot_bytes) *slot_bytes = s->impl->slot_bytes;
+  if (denied) *denied = s->impl->denied;
+  return SBWT_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -738,11 +805,27 @@ int sbwt_autotune(const sbwt_index_t *index, const char *d_chars, uint64_t n_cha
     LaunchConfig best_cfg = saved;
     bool have_ref = false;
     std::vector<u64> h_ref, h_out;
-    for (u32 p = ix.p_max; p >= std::min<u32>(8, ix.p_max); --p) {
+    // With the k-mer table (k <= 31, suffix groups, fewer than 192 * 2^24
+    // nodes) the read search never reads the presearch table: the first axis
+    // is then the kernel (table kernel, or walks kernel with 1, 2 or 4 walks
+    // per lane at its register budget), else the presearch depth.
+    const bool table_axis = ix.view.kmer_table && ix.view.suffix_group_starts && ix.k <= 31 &&
+                            ix.num_bits < (192ULL << 24);
+    std::vector<std::pair<u32, u32>> first;  // (presearch, kernel mode)
+    if (table_axis) {
+      for (u32 m : {1u, 2u, 3u, 4u, 5u}) first.emplace_back(ix.p_max, m);
+    } else {
+      for (u32 p = ix.p_max; p >= std::min<u32>(8, ix.p_max); --p) {
+        first.emplace_back(p, saved.table_kernel);
+        if (p == 0) break;
+      }
+    }
+    for (const auto &pm : first) {
       for (u64 tile : {0ULL, 64ULL, 256ULL, 1024ULL}) {
         for (u32 bps : {2u, 3u, 4u, 6u, 8u}) {
           LaunchConfig c = saved;
-          c.presearch_letters = p;
+          c.presearch_letters = pm.first;
+          c.table_kernel = pm.second;
           c.tile = tile;
           c.blocks_per_sm = bps;
           default_launch_config() = c;
@@ -772,7 +855,6 @@ int sbwt_autotune(const sbwt_index_t *index, const char *d_chars, uint64_t n_cha
           }
         }
       }
-      if (p == 0) break;
     }
     default_launch_config() = best_cfg;
     cudaEventDestroy(e0);

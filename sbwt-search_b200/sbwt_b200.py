@@ -102,6 +102,8 @@ def lib():
         L.sbwt_server_wait.argtypes = [vp, u64, C.c_double, C.POINTER(vp), C.POINTER(u64),
                                        C.POINTER(vp), C.POINTER(u64), C.POINTER(vp),
                                        C.POINTER(u64)]
+        L.sbwt_get_launch_config.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_int)]
+        L.sbwt_server_slots.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(u64), C.POINTER(u64)]
         L.sbwt_server_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                         C.POINTER(u64), C.POINTER(u64), C.POINTER(u64),
                                         C.POINTER(C.c_double), C.c_int]
@@ -483,22 +485,32 @@ class Server:
         return {"p50_s": p50.value, "p99_s": p99.value, "requests": nd.value,
                 "reads": rd.value, "batches": nb.value, "elapsed_s": el.value}
 
+    def slots(self) -> dict:
+        """Slots open now, device bytes per slot, and how often a waiting
+        batch found too little free device memory to open one."""
+        n, b, d = C.c_int(), C.c_uint64(), C.c_uint64()
+        check(lib().sbwt_server_slots(self._h, C.byref(n), C.byref(b), C.byref(d)))
+        return {"open": n.value, "slot_bytes": b.value, "denied": d.value}
+
 
 AUTOTUNE_CACHE = HERE / "_build" / "autotune.json"
 
 
 def autotune(index: SbwtIndex, d_chars, d_read_ends, sample_chars: int = 256 << 20,
              use_cache: bool = True) -> dict:
-    """Chooses presearch depth, tile size and blocks per SM for this GPU and
-    index with the library's autotuner (sbwt_autotune) and applies them; the
-    choice is cached per (GPU name, SBWT nodes, k) in _build/autotune.json."""
+    """Chooses the read search kernel (walks per lane) or presearch depth,
+    tile size and blocks per SM for this GPU and index with the library's
+    autotuner (sbwt_autotune) and applies them; the choice is cached per
+    (GPU name, SBWT nodes, k, k-mer table present) in _build/autotune.json."""
     import json
     try:
         import torch
         gpu = torch.cuda.get_device_name(index.device)
     except Exception:
         gpu = "cuda"
-    key = f"{gpu}|{index.num_bits}|{index.k}"
+    info = IndexInfo()
+    check(lib().sbwt_index_get_info(index._h, C.byref(info)))
+    key = f"{gpu}|{index.num_bits}|{index.k}|table={int(info.kmer_table_bytes > 0)}"
     cache = {}
     if use_cache and AUTOTUNE_CACHE.exists():
         try:
@@ -508,14 +520,17 @@ def autotune(index: SbwtIndex, d_chars, d_read_ends, sample_chars: int = 256 << 
     if use_cache and key in cache:
         c = cache[key]
         set_launch_config(c["presearch"], c["blocks_per_sm"], c["tile"], 0)
+        set_table_kernel(c.get("table_kernel", TABLE_KERNEL_DEFAULT))
         return dict(c, cached=True)
     p, b = C.c_uint32(), C.c_uint32()
     t, ms = C.c_uint64(), C.c_double()
     check(lib().sbwt_autotune(index._h, _ptr(d_chars), d_chars.numel(), _ptr(d_read_ends),
                               d_read_ends.numel(), sample_chars, C.byref(p), C.byref(b),
                               C.byref(t), C.byref(ms)))
+    mode = C.c_int()
+    check(lib().sbwt_get_launch_config(None, None, None, None, C.byref(mode)))
     c = {"presearch": p.value, "blocks_per_sm": b.value, "tile": t.value,
-         "sample_ms": ms.value}
+         "table_kernel": mode.value, "sample_ms": ms.value}
     if use_cache:
         cache[key] = c
         AUTOTUNE_CACHE.parent.mkdir(parents=True, exist_ok=True)

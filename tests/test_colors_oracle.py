@@ -58,3 +58,21 @@ def test_threshold_rule():
             m = int(math.ceil(size * tau))
             exp = [] if m == 0 else [c for c in range(tc.num_colors) if counts[r, c] >= m]
             assert rows[r] == exp
+
+
+def test_multithreaded_restatement_matches_single_thread():
+    """The OpenMP form of the restatement (the colors CPU baseline) gives
+    the single-thread restatement's ids per read (count and checksum)."""
+    g, sp, cp = colored()
+    tc = O.ColorsFile.read(cp)
+    oc = O.OracleColors(tc)
+    per = found_lists(oracle_index(sp, 8), g, 11, 300)
+    found = [p[p < O.INVALID] for p in per]
+    nf = [int((p == O.NOT_FOUND).sum()) for p in per]
+    inv = [int((p == O.INVALID).sum()) for p in per]
+    offs = np.zeros(len(found) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(f) for f in found])
+    rows = oc.pseudoalign(found, nf, inv, 0.7)
+    n_ids, ck = oc.pseudoalign_mt(np.concatenate(found), offs, nf, inv, 0.7, threads=4)
+    assert list(n_ids) == [len(r) for r in rows]
+    assert np.array_equal(ck, O.ids_checksum(rows))

@@ -109,3 +109,35 @@ def test_server_index_mode_splits_large_requests():
     empty = srv.wait(srv.submit(b"", np.zeros(0, np.uint64)))
     assert len(empty[0]) == 0
     srv.close()
+
+
+def test_server_admits_slots_by_free_device_memory():
+    """The server opens one slot at creation and more only while batches
+    wait and the device has a slot's bytes free above an eighth of its
+    memory.  With that room taken by another allocation no slot opens (the
+    refusals are counted) and requests still complete, on the one slot, with
+    the results of direct calls."""
+    import torch
+    g, sp, cp = colored()
+    idx, ci = S.SbwtIndex.open(sp), S.ColorIndex.open(cp)
+    srv = S.Server(idx, ci, batch_chars=200_000, batch_reads=1500, slots=4, tau=0.7)
+    info = srv.slots()
+    assert info["open"] == 1 and info["slot_bytes"] > 0
+    reqs = _requests(g, 24, 5)
+    p = S.Pipeline(idx, ci, 1 << 22, 1 << 16, tau=0.7)
+    exp = [p.run(*r) for r in reqs]
+    free, total = torch.cuda.mem_get_info()
+    keep = total // 8 + info["slot_bytes"] // 2  # less than a slot above the reserve
+    hog = torch.empty(max(free - keep, 0), dtype=torch.uint8, device="cuda")
+    try:
+        got = [srv.wait(rid) for rid in [srv.submit(*r) for r in reqs]]
+        assert got == exp
+        after = srv.slots()
+        assert after["open"] == 1 and after["denied"] > 0
+    finally:
+        del hog
+        torch.cuda.empty_cache()
+    got = [srv.wait(rid) for rid in [srv.submit(*r) for r in reqs]]
+    assert got == exp
+    assert 1 <= srv.slots()["open"] <= 4
+    srv.close()

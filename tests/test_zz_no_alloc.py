@@ -71,3 +71,56 @@ def test_noalloc_rejects_oversized_batches():
     assert b"at most" in S.lib().sbwt_last_error()
     rc = f(idx._h, p, 100, p, MAX_READS + 1, p, 64, C.byref(n), 0, None)
     assert rc == S.E_INVALID
+
+
+def _reads(n_reads, length, seed):
+    rng = np.random.default_rng(seed)
+    chars = rng.choice(np.frombuffer(b"ACGT", np.uint8), n_reads * length)
+    ends = np.arange(1, n_reads + 1, dtype=np.uint64) * length
+    return chars, ends
+
+
+@pytest.mark.parametrize("shape", [(MAX_READS, MAX_CHARS // MAX_READS),
+                                   (MAX_CHARS // 400, 400)])
+@pytest.mark.parametrize("kernel", [0, 1, S.TABLE_KERNEL_DEFAULT])
+def test_noalloc_at_its_limits_allocates_nothing(shape, kernel):
+    """A batch at the stated limits (every read slot used, or nearly every
+    char with the smallest tile, 16 k-mers, so that the tile table is full)
+    gives sbwt_search_reads's results on every read search kernel, and the
+    call leaves the device's free memory unchanged."""
+    import torch
+    n_reads, length = shape
+    g, path, sb = synthetic(7, 4, 6000, 31, 2, 0.02)
+    idx = S.SbwtIndex.open(path)
+    chars, ends = _reads(n_reads, length, 3 + length)
+    # half of the reads from the genomes, so that k-mers are found
+    gen = g.chars[: (n_reads // 2) * length]
+    chars[: len(gen)] = gen
+    assert len(chars) <= MAX_CHARS and len(ends) <= MAX_READS
+    d_chars = torch.from_numpy(chars.copy()).cuda()
+    d_ends = torch.from_numpy(ends.view(np.int64).copy()).cuda()
+    n_k = idx.count_kmers(ends)
+    S.set_table_kernel(kernel)
+    S.set_launch_config(tile=16)
+    try:
+        ref = torch.empty(n_k, dtype=torch.int64, device="cuda")
+        assert idx.search_reads(d_chars, d_ends, out=ref) == n_k
+        expected = ref.cpu().numpy().view(np.uint64)
+        assert (expected < (1 << 62)).any()
+        f = _noalloc()
+        out = torch.full((n_k,), -7, dtype=torch.int64, device="cuda")
+        n = C.c_uint64(0)
+        S.check(f(idx._h, d_chars.data_ptr(), len(chars), d_ends.data_ptr(), len(ends),
+                  out.data_ptr(), n_k, C.byref(n), 0, None))
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        out.fill_(-7)
+        S.check(f(idx._h, d_chars.data_ptr(), len(chars), d_ends.data_ptr(), len(ends),
+                  out.data_ptr(), n_k, C.byref(n), 0, None))
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free0
+        assert n.value == n_k
+        assert np.array_equal(out.cpu().numpy().view(np.uint64), expected)
+    finally:
+        S.set_table_kernel(S.TABLE_KERNEL_DEFAULT)
+        S.set_launch_config()

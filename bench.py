@@ -532,6 +532,9 @@ def parse():
     ap.add_argument("--kernel", type=int, default=-1,
                     help="read search kernel with a k-mer table (sbwt_set_table_kernel): "
                          "0 general, 1 table, 2..5 walks variants, -1 library default")
+    ap.add_argument("--gather-sweep", action="store_true",
+                    help="print the random-sector gather rate against working-set size "
+                         "and exit")
     ap.add_argument("--write-workload", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--seed-reads", type=int, default=1000, help=argparse.SUPPRESS)
     return ap.parse_args()
@@ -663,6 +666,31 @@ def write_workload(args):
     with open(os.path.join(args.write_workload, "meta.json"), "w") as f:
         json.dump({"nodes": int(nodes), "kmers": kmer_count(ends, CFG["k"]),
                    "chars": int(ends[-1])}, f)
+
+
+def gather_sweep(S, dev):
+    """Random 32-byte-sector gather rate against the working-set size: for
+    buffers of 32 MB .. 8 GB and 1, 4 and 8 independent dependent-load
+    chains per thread (2048 threads per SM), sbwt_measure_random_sectors;
+    the implied loaded latency is threads x chains / rate.  The read search
+    looks up random sectors in working sets of these sizes, so this curve is
+    its ceiling."""
+    import torch
+    L = S.lib()
+    L.sbwt_measure_random_sectors.argtypes = [C.c_int, C.c_uint64, C.c_int,
+                                              C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    threads = torch.cuda.get_device_properties(dev).multi_processor_count * 2048
+    rows = []
+    for mb in (32, 64, 128, 256, 512, 1024, 2048, 4096, 8192):
+        row = {"bytes": mb << 20}
+        for chains in (1, 4, 8):
+            gbs, sps = C.c_double(), C.c_double()
+            S.check(L.sbwt_measure_random_sectors(dev, mb << 20, chains, C.byref(gbs),
+                                                  C.byref(sps)))
+            row[f"gsectors_s_{chains}"] = sps.value / 1e9
+            row[f"latency_us_{chains}"] = threads * chains / sps.value * 1e6
+        rows.append(row)
+    return {"gather_sweep": rows, "threads": threads}
 
 
 def random_sector_peak(S, dev, ws_bytes):
@@ -1033,6 +1061,13 @@ def main():
     import sbwt_b200 as S
     torch.cuda.set_device(local)
     dev = local
+    if args.gather_sweep:
+        if rank == 0:
+            print(json.dumps(gather_sweep(S, dev)), flush=True)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
     S.set_table_kernel(args.kernel)
     L = S.lib()
     L.sbwt_profile_enable.argtypes = [C.c_int, C.c_int]
@@ -1113,7 +1148,11 @@ def main():
         assert np.array_equal(ho[:200_000], out_host), "e2e output differs from device path"
         e2e = {"value": n_kmers * world / e_dt, "unit": UNIT,
                "h2d_bytes_per_step": int(chars.nbytes + ends.nbytes),
-               "d2h_bytes_per_step": int(n_kmers * 8), "ms_per_step": e_dt * 1e3}
+               "d2h_bytes_per_step": int(n_kmers * idx.host_result_bytes()),
+               "ms_per_step": e_dt * 1e3,
+               "results": "u64 per k-mer in pinned host memory (the device sends "
+                          f"{idx.host_result_bytes()} bytes per k-mer; 32-bit codes are "
+                          "widened on host threads inside the call)"}
 
     # roofline of the dominant kernel (the read search kernel)
     peak, peak_kind = load_peaks()

@@ -68,6 +68,10 @@ typedef struct {
   int has_key_kmer_marks;
   uint64_t kmer_table_bytes;  /* k-mer -> node table (0 when absent) */
   uint64_t kmer_filter_bytes; /* k-mer filter in front of the table (0 when absent) */
+  uint32_t host_result_bytes; /* bytes per k-mer a host-pointer sbwt_search_reads moves
+                                 device -> host with default flags: 4 (32-bit codes
+                                 widened on host threads) or 8 */
+  uint32_t reserved;
 } sbwt_index_info_t;
 
 /* Loads a .sbwt / .tdbg file (and, when colors_path is not NULL, the key

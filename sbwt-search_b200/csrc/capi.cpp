@@ -104,6 +104,8 @@ int sbwt_index_get_info(const sbwt_index_t *index, sbwt_index_info_t *info) {
   info->has_key_kmer_marks = x.view.key_marks != nullptr;
   info->kmer_table_bytes = x.kmer_table.size();
   info->kmer_filter_bytes = x.kmer_filter.size();
+  info->host_result_bytes = x.host_result_bytes(default_launch_config());
+  info->reserved = 0;
   return SBWT_OK;
 }
 

@@ -9,6 +9,7 @@
 //   build_positions        PositionsBuilder/PositionsBuilder.cpp:15-47
 //   -1 / -2 mapping        IndexResultsPrinter/ContinuousIndexResultsPrinter.hpp:196-205
 #include <cuda_runtime.h>
+#include <emmintrin.h>
 
 #include <algorithm>
 #include <atomic>
@@ -330,6 +331,8 @@ struct ReadsView {
   const uint64_t *n_kmers_dev;  // if set, the k-mer total is read from here
   unsigned long long *queue;    // work-queue counter (tiles handed out), zeroed
   uint64_t n_kmers_bound;       // > every chunk position, slot and read number
+  uint32_t *out32;  // walks kernel only: 32-bit results here instead of `out`
+                    // (node, 0xFFFFFFFF not found, 0xFFFFFFFE invalid)
 };
 
 __device__ __forceinline__ bool invalid_at(const uint32_t *inv, uint64_t i) {
@@ -1181,6 +1184,13 @@ __device__ __forceinline__ uint64_t load_u64_nc(const uint64_t *p) {
   return v;
 }
 
+__device__ __forceinline__ void store_u32x4_cs(uint32_t *p, uint32_t a, uint32_t b,
+                                               uint32_t c, uint32_t d) {
+  asm volatile("st.global.cs.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(a), "r"(b), "r"(c),
+               "r"(d)
+               : "memory");
+}
+
 __device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_t b,
                                                 uint64_t c, uint64_t d) {
   asm volatile("st.global.cs.v4.u64 [%0], {%1,%2,%3,%4};" ::"l"(p), "l"(a), "l"(b), "l"(c),
@@ -1208,6 +1218,8 @@ __global__ void __launch_bounds__(256, MINB)
   const I base = (I)rv.base;
   const I out_cap = (I)min(rv.out_capacity, (uint64_t)NONE);
   const bool vec_out = ((uintptr_t)rv.out & 31) == 0;
+  uint32_t *const out32 = rv.out32;
+  const bool vec_out32 = ((uintptr_t)out32 & 15) == 0;
   uint64_t n_table = 0, n_block = 0, n_sg = 0, n_filter = 0, n_iter = 0, n_lane = 0,
            n_known = 0, n_searched = 0, n_stream = 0, n_step = 0, n_distinct = 0;
   I slot[W], slot_end[W], r[W], r_next[W], pos[W], last_inv1[W], v[W], x[W], hslot[W];
@@ -1230,7 +1242,17 @@ __global__ void __launch_bounds__(256, MINB)
   auto flush = [&](int w) {  // the staged slots of walk w's open group
     const I g = obase[w];
     const uint32_t t = threadIdx.x;
-    if (omask[w] == 15u && vec_out && g + 4 <= out_cap) {
+    if (out32) {  // 32-bit codes: the value's low word (markers stay markers)
+      if (omask[w] == 15u && vec_out32 && g + 4 <= out_cap) {
+        store_u32x4_cs(out32 + g, (uint32_t)sh_out[0][w][t], (uint32_t)sh_out[1][w][t],
+                       (uint32_t)sh_out[2][w][t], (uint32_t)sh_out[3][w][t]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (((omask[w] >> q) & 1u) && g + q < out_cap)
+            __stcs(out32 + g + q, (unsigned int)sh_out[q][w][t]);
+      }
+    } else if (omask[w] == 15u && vec_out && g + 4 <= out_cap) {
       store_sector_cs(rv.out + g, sh_out[0][w][t], sh_out[1][w][t], sh_out[2][w][t],
                       sh_out[3][w][t]);
     } else {
@@ -1359,8 +1381,13 @@ __global__ void __launch_bounds__(256, MINB)
         const int q = __ffs(runs) - 1;
         const I q_slot = __shfl_sync(0xFFFFFFFFu, run_slot[w], q);
         const uint32_t q_n = __shfl_sync(0xFFFFFFFFu, run_n[w], q);
-        for (uint32_t j = lane; j < q_n; j += 32)
-          if (q_slot + j < out_cap) __stcs(rv.out + q_slot + j, (unsigned long long)SBWT_INVALID);
+        for (uint32_t j = lane; j < q_n; j += 32) {
+          if (q_slot + j >= out_cap) continue;
+          if (out32)
+            __stcs(out32 + q_slot + j, 0xFFFFFFFEu);
+          else
+            __stcs(rv.out + q_slot + j, (unsigned long long)SBWT_INVALID);
+        }
       }
     }
     bool all_done = true;
@@ -1582,6 +1609,15 @@ static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStrea
 // walks kernel with (walks per lane, blocks per SM) = (1, 5), (2, 4), (2, 3),
 // (4, 2) (the table kernel when the index has no k-mer filter).  Results
 // never depend on it.
+// Whether launch_search_kernel runs the walks kernel (the only one that can
+// write 32-bit results, ReadsView::out32).
+static bool walks_kernel_applies(const SbwtView &sv, const ReadsView &rv, bool stream,
+                                 uint32_t mtk, uint32_t kernel_mode) {
+  const bool narrow = sv.num_bits < kNarrowLimit && rv.n_kmers_bound < (1ULL << 32);
+  return kernel_mode >= 2 && stream && narrow && sv.kmer_table && sv.kmer_filter &&
+         sv.k <= 31 && mtk == 0 && sv.suffix_group_starts;
+}
+
 // instrument = false keeps the launch free of the profiler's events and
 // counter buffer (the allocation-free entry point).
 static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsView &rv,
@@ -1612,7 +1648,9 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
   const bool narrow = sv.num_bits < kNarrowLimit && rv.n_kmers_bound < (1ULL << 32);
   const bool table = kernel_mode != 0 && stream && narrow && sv.kmer_table && sv.k <= 31 &&
                      mtk == 0 && sv.suffix_group_starts;
-  const bool walks = table && kernel_mode >= 2 && sv.kmer_filter;
+  const bool walks = walks_kernel_applies(sv, rv, stream, mtk, kernel_mode);
+  if (rv.out32 && !walks)
+    throw Error(SBWT_E_INVALID, "32-bit results need the walks kernel");
 #define SBWT_LAUNCH(S_, C_, K_)                                                          \
   do {                                                                                   \
     if (narrow)                                                                          \
@@ -1835,10 +1873,22 @@ struct Workspace {
   int device = -1;
   cudaStream_t streams[2] = {nullptr, nullptr};
   DeviceBuffer chars[2], ends[2], kmer_off[2], packed[2], invalid[2], results[2],
-      block_sums[2], total[2], tile_read[2], queue[2], positions, bits;
+      block_sums[2], total[2], tile_read[2], queue[2], positions, bits, results32[2];
   uint32_t *err_host = nullptr;  // pinned
   DeviceBuffer err_dev;
   cudaEvent_t done[2] = {nullptr, nullptr};
+  uint32_t *stage[2] = {nullptr, nullptr};  // pinned: 32-bit results of a chunk
+  u64 stage_cap[2] = {0, 0};
+  uint32_t *staging(int b, u64 n) {
+    if (stage_cap[b] < n) {
+      if (stage[b]) cudaFreeHost(stage[b]);
+      stage[b] = nullptr;
+      stage_cap[b] = 0;
+      SBWT_CUDA(cudaHostAlloc((void **)&stage[b], n * 4, cudaHostAllocDefault));
+      stage_cap[b] = n;
+    }
+    return stage[b];
+  }
   ~Workspace() {
     if (device < 0) return;
     int prev = 0;
@@ -1849,9 +1899,47 @@ struct Workspace {
     for (auto &e : done)
       if (e) cudaEventDestroy(e);
     if (err_host) cudaFreeHost(err_host);
+    for (auto *p : stage)
+      if (p) cudaFreeHost(p);
     cudaSetDevice(prev);
   }
 };
+
+// 32-bit result codes -> the API's u64 values (0xFFFFFFFF -> SBWT_NOT_FOUND,
+// 0xFFFFFFFE -> SBWT_INVALID), on host threads, with streaming stores (the
+// caller reads the results later, not now).
+static inline u64 widen_code(uint32_t x) {
+  return x >= 0xFFFFFFFEu ? (0xFFFFFFFF00000000ULL | x) : (u64)x;
+}
+static void widen_range(const uint32_t *src, u64 *dst, u64 n) {
+  u64 i = 0;
+  for (; i < n && ((uintptr_t)(dst + i) & 15); ++i) dst[i] = widen_code(src[i]);
+  const __m128i m1 = _mm_set1_epi32(-1), m2 = _mm_set1_epi32(-2);
+  for (; i + 4 <= n; i += 4) {
+    const __m128i v = _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i));
+    const __m128i hi = _mm_or_si128(_mm_cmpeq_epi32(v, m1), _mm_cmpeq_epi32(v, m2));
+    _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i), _mm_unpacklo_epi32(v, hi));
+    _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i + 2), _mm_unpackhi_epi32(v, hi));
+  }
+  for (; i < n; ++i) dst[i] = widen_code(src[i]);
+  _mm_sfence();
+}
+static void widen_results(const uint32_t *src, u64 *dst, u64 n) {
+  const u64 per = 4ULL << 20;  // k-mers per thread at least
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned T = (unsigned)std::min<u64>(std::min<u64>(hw, 32), std::max<u64>(n / per, 1));
+  if (T <= 1) {
+    widen_range(src, dst, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  th.reserve(T);
+  for (unsigned t = 0; t < T; ++t) {
+    const u64 a = n * t / T, b = n * (t + 1) / T;
+    th.emplace_back(widen_range, src + a, dst + a, b - a);
+  }
+  for (auto &x : th) x.join();
+}
 
 static Workspace &workspace(int device) {
   thread_local std::map<int, std::unique_ptr<Workspace>> ws;
@@ -1940,9 +2028,10 @@ static void launch_search(const IndexImpl &ix, u64 n_chars, const u64 *d_ends, u
                           u64 base,
                           u64 n_kmers, u64 *d_out, u64 out_capacity, u32 flags,
                           const LaunchConfig &cfg, const ReadsScratch &sc,
-                          cudaStream_t st) {
+                          cudaStream_t st, uint32_t *d_out32 = nullptr) {
   if (n_reads == 0 || n_kmers == 0) return;
   ReadsView rv{};
+  rv.out32 = d_out32;
   rv.n_kmers_bound = std::max<u64>(n_chars, n_reads) + 64;
   rv.packed = sc.packed;
   rv.invalid = sc.invalid;
@@ -2062,6 +2151,16 @@ u64 count_kmers_host(const u64 *ends, u64 n_reads, u32 k, u64 base) {
   return n;
 }
 
+u32 IndexImpl::host_result_bytes(const LaunchConfig &cfg) const {
+  ReadsView probe{};
+  probe.n_kmers_bound = (64ULL << 20) + 64;
+  const SbwtView sv = view_for(cfg.presearch_letters);
+  return walks_kernel_applies(sv, probe, view.suffix_group_starts != nullptr, 0,
+                              cfg.table_kernel)
+             ? 4u
+             : 8u;
+}
+
 void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_ends,
                              u64 n_reads, u64 *results, u64 capacity,
                              u64 *n_results, u32 flags, cudaStream_t user_stream,
@@ -2095,9 +2194,25 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
   // ends, its k-mers and the ends' order checked over its own reads) while the
   // previous one is on the GPU, and its results are only copied back once
   // they fit the capacity.
+  // With the walks kernel the results of a chunk cross PCIe as 32-bit codes
+  // into a pinned staging buffer and are widened to u64 on host threads
+  // while the next chunk runs (half the device-to-host bytes).
   const u64 chunk_chars = cfg.chunk_chars ? cfg.chunk_chars : (64ULL << 20);
-  const bool pinned = is_host_pinned(chars) && is_host_pinned(results) &&
-                      is_host_pinned(read_ends);
+  const bool pinned_in = is_host_pinned(chars) && is_host_pinned(read_ends);
+  const bool pinned = pinned_in && is_host_pinned(results);
+  const SbwtView sv_host = view_for(cfg.presearch_letters);
+  const bool stream_host = !(flags & SBWT_PER_KMER_WALK) && view.suffix_group_starts;
+  const u32 mtk_host = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
+  struct Pending {
+    int b = -1;
+    u64 at = 0, n = 0;
+  } pend;
+  auto drain = [&]() {  // widens the chunk whose 32-bit results are in flight
+    if (pend.b < 0) return;
+    SBWT_CUDA(cudaEventSynchronize(ws.done[pend.b]));
+    widen_results(ws.stage[pend.b], results + pend.at, pend.n);
+    pend.b = -1;
+  };
   u64 r = 0, kacc = 0, prev_end = 0;
   bool over = false, unordered = false;
   for (size_t i = 0; r < n_reads; ++i) {
@@ -2120,25 +2235,49 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
     const int b = (int)(i & 1);
     cudaStream_t st = ws.streams[b];
     const u64 nc = prev - c0, nr = r1 - r0;
+    ReadsView probe{};
+    probe.n_kmers_bound = std::max<u64>(nc, nr) + 64;
+    const bool narrow =
+        walks_kernel_applies(sv_host, probe, stream_host, mtk_host, cfg.table_kernel);
     ws.chars[b].ensure(nc + 16);
     ws.ends[b].ensure(nr * 8);
-    ws.results[b].ensure(std::max<u64>(nk, 1) * 8);
+    if (narrow)
+      ws.results32[b].ensure(std::max<u64>(nk, 1) * 4);
+    else
+      ws.results[b].ensure(std::max<u64>(nk, 1) * 8);
     const ReadsScratch sc = scratch_for(ws, b, nc, nr, nk, tile_size(device, nk, cfg));
     SBWT_CUDA(cudaMemcpyAsync(ws.chars[b].get(), chars + c0, nc, cudaMemcpyHostToDevice, st));
     SBWT_CUDA(cudaMemcpyAsync(ws.ends[b].get(), read_ends + r0, nr * 8,
                               cudaMemcpyHostToDevice, st));
     launch_prepare(device, k, ws.chars[b].get<char>(), nc, ws.ends[b].get<u64>(), nr, c0, sc,
                    st);
-    launch_search(*this, nc, ws.ends[b].get<u64>(), nr, c0, nk, ws.results[b].get<u64>(), nk,
-                  flags, cfg, sc, st);
-    if (nk)
-      SBWT_CUDA(cudaMemcpyAsync(results + kacc, ws.results[b].get(), nk * 8,
-                                cudaMemcpyDeviceToHost, st));
-    if (!pinned) SBWT_CUDA(cudaStreamSynchronize(st));
+    if (narrow) {
+      uint32_t *stage = ws.staging(b, std::max<u64>(nk, 1));
+      launch_search(*this, nc, ws.ends[b].get<u64>(), nr, c0, nk, nullptr, nk, flags, cfg, sc,
+                    st, ws.results32[b].get<uint32_t>());
+      if (nk)
+        SBWT_CUDA(cudaMemcpyAsync(stage, ws.results32[b].get(), nk * 4,
+                                  cudaMemcpyDeviceToHost, st));
+      SBWT_CUDA(cudaEventRecord(ws.done[b], st));
+      drain();  // the previous chunk, while this one runs
+      pend.b = b;
+      pend.at = kacc;
+      pend.n = nk;
+      if (!pinned_in) drain();
+    } else {
+      drain();
+      launch_search(*this, nc, ws.ends[b].get<u64>(), nr, c0, nk, ws.results[b].get<u64>(), nk,
+                    flags, cfg, sc, st);
+      if (nk)
+        SBWT_CUDA(cudaMemcpyAsync(results + kacc, ws.results[b].get(), nk * 8,
+                                  cudaMemcpyDeviceToHost, st));
+      if (!pinned) SBWT_CUDA(cudaStreamSynchronize(st));
+    }
     kacc += nk;
     r = r1;
     prev_end = prev;
   }
+  drain();
   for (auto &s : ws.streams) SBWT_CUDA(cudaStreamSynchronize(s));
   if (unordered) throw Error(SBWT_E_INVALID, "read ends must be non-decreasing");
   if (over) {

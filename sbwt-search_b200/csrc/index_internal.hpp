@@ -49,6 +49,10 @@ struct IndexImpl {
                     u64 n_reads, u64 *results, u64 capacity, u64 *n_results,
                     u32 flags, cudaStream_t st, const LaunchConfig &cfg) const;
 
+  // Bytes per k-mer result that a host-pointer sbwt_search_reads moves from
+  // the device with default flags: 4 on the walks kernel, else 8.
+  u32 host_result_bytes(const LaunchConfig &cfg) const;
+
   void search_reads_noalloc(const char *d_chars, u64 n_chars, const u64 *d_ends,
                             u64 n_reads, u64 *d_results, u64 capacity, u64 *n_results,
                             u32 flags, cudaStream_t st, const LaunchConfig &cfg) const;

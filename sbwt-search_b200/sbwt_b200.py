@@ -46,7 +46,8 @@ class IndexInfo(C.Structure):
                 ("presearch_letters", C.c_uint32), ("c_map", C.c_uint64 * 5),
                 ("device_bytes", C.c_uint64), ("device", C.c_int),
                 ("has_key_kmer_marks", C.c_int), ("kmer_table_bytes", C.c_uint64),
-                ("kmer_filter_bytes", C.c_uint64)]
+                ("kmer_filter_bytes", C.c_uint64), ("host_result_bytes", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 _L = None
@@ -256,6 +257,12 @@ class SbwtIndex:
         check(lib().sbwt_index_get_info(self._h, C.byref(info)))
         self.device_bytes = info.device_bytes
         return nb.value
+
+    def host_result_bytes(self) -> int:
+        """Bytes per k-mer a host-pointer search_reads moves device -> host."""
+        info = IndexInfo()
+        check(lib().sbwt_index_get_info(self._h, C.byref(info)))
+        return int(info.host_result_bytes)
 
     def filter_bytes(self) -> int:
         """Size of the k-mer filter in front of the k-mer table (0 when absent)."""

@@ -130,6 +130,34 @@ def test_chunked_host_pipeline_matches_single_chunk():
     assert np.array_equal(one, many)
 
 
+@pytest.mark.parametrize("kernel", [1, S.TABLE_KERNEL_DEFAULT])
+def test_pinned_host_chunks_match_device_path(kernel):
+    """Host-pointer calls from pinned memory, many chunks in flight: on the
+    walks kernel the results cross as 32-bit codes and are widened on host
+    threads (with an output start that is not 16-byte aligned), on the table
+    kernel as u64; both equal the oracle, and no slot outside the output is
+    written."""
+    import torch
+    g, path, sb = synthetic(7, 4, 6000, 31, 2, 0.02)
+    idx = S.SbwtIndex.open(path)
+    chars, ends = mixed_reads(g, 33, 30000, sub=0.01, n_rate=0.005)
+    exp = oracle_results(oracle_index(path, 8), chars, ends)
+    S.set_table_kernel(kernel)
+    S.set_launch_config(chunk_chars=300_001)
+    try:
+        assert idx.host_result_bytes() == (4 if kernel != 1 else 8)
+        h_chars = torch.from_numpy(chars.copy()).pin_memory()
+        h_ends = torch.from_numpy(ends.view(np.int64).copy()).pin_memory()
+        h_out = torch.full((len(exp) + 3,), -7, dtype=torch.int64).pin_memory()
+        out = h_out.numpy()[1:1 + len(exp)].view(np.uint64)
+        idx.search_reads(h_chars.numpy(), h_ends.numpy().view(np.uint64), out=out)
+        assert np.array_equal(out, exp)
+        assert h_out[0].item() == -7 and (h_out[1 + len(exp):] == -7).all()
+    finally:
+        S.set_table_kernel(DEFAULT_TABLE_KERNEL)
+        S.set_launch_config()
+
+
 def test_errors_are_status_codes():
     with pytest.raises(S.SbwtError) as e:
         S.SbwtIndex.open("/nonexistent/file.sbwt")

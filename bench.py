@@ -128,7 +128,7 @@ def bench_batched(args, idx, S, torch, dev, scratch):
 # substitutions (about 4.5e10 chars in all).
 CFG4_FULL = dict(n_files=256, reads_lo=1_000, reads_hi=2_000_000, long_frac=0.1,
                  short_len=100, long_lo=1000, long_hi=10_000, sub=0.05,
-                 short_pool=2_000_000, long_pool=100_000, wave_chars=6_000_000_000)
+                 short_pool=2_000_000, long_pool=100_000, wave_chars=3_000_000_000)
 
 
 def _wave_checksum(torch, out, n):
@@ -278,7 +278,8 @@ def bench_batched_full(args, idx, S, torch, dev):
                         "log-uniform [1e3, 2e6], 10% files of 1-10 kbp reads (log-normal, "
                         "median 3 kbp), the rest 100 bp, 5% substitutions; reads are cyclic "
                         "runs of two seeded pools (2 M short, 100 k long reads) on the "
-                        "device; processed in waves of <= 6e9 chars",
+                        "device; processed in waves of <= 3e9 chars (a larger wave, or a "
+                        "larger file, runs on the 64-bit kernel: > 2^32 k-mer slots)",
             "files": len(files), "waves": len(waves), "reads": int(n_reads),
             "chars": int(n_chars), "kmers": int(n_kmers),
             "plain_kmers_per_s": n_kmers / tot["plain"],
@@ -711,7 +712,7 @@ def random_sector_peak(S, dev, ws_bytes):
 
 KERNELS = {0: "search_reads_kernel", 1: "search_table_kernel", 2: "search_walks_kernel",
            3: "search_walks_kernel", 4: "search_walks_kernel", 5: "search_walks_kernel"}
-DEFAULT_KERNEL_MODE = 3
+DEFAULT_KERNEL_MODE = 2
 
 
 def search_kernel_name(idx, mode: int) -> str:

@@ -365,6 +365,24 @@ __device__ __forceinline__ uint64_t chunk_word(const Block &b, uint64_t i) {
   return j == 0 ? b.w0 : (j == 1 ? b.w1 : (j == 2 ? b.w2 : b.w3));
 }
 
+// *out = the first read r in [r0, n_reads) with ends[r] > limit (n_reads if
+// none); one thread, binary search (ends are non-decreasing; the scan kernels
+// check that).
+__global__ void ends_upper_bound_kernel(const uint64_t *ends, uint64_t r0, uint64_t n_reads,
+                                        uint64_t limit, uint64_t *out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint64_t lo = r0, hi = n_reads;
+  while (lo < hi) {
+    const uint64_t mid = lo + (hi - lo) / 2;
+    if (ends[mid] > limit)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  out[0] = lo;
+  out[1] = lo > r0 ? ends[lo - 1] : limit;
+}
+
 // First read of every work tile: tile_read[t] = the read holding k-mer slot
 // t * tile.  One thread per read; reads without k-mers own no tile.
 __global__ void tile_reads_kernel(const uint64_t *kmer_off, uint64_t n_reads, uint64_t tile,
@@ -2151,6 +2169,51 @@ u64 count_kmers_host(const u64 *ends, u64 n_reads, u32 k, u64 base) {
   return n;
 }
 
+void IndexImpl::search_reads_device_pieces(const char *chars, u64 n_chars,
+                                           const u64 *read_ends, u64 n_reads, u64 *results,
+                                           u64 capacity, u64 *n_results, u32 flags,
+                                           cudaStream_t st, const LaunchConfig &cfg) const {
+  Workspace &ws = workspace(device);
+  // an explicit chunk size (a tuning and testing hook) sets the piece size
+  const u64 kPieceChars = cfg.chunk_chars ? std::min<u64>(cfg.chunk_chars, 1ULL << 31)
+                                          : (1ULL << 31);
+  DeviceBuffer bound(16);
+  u64 r0 = 0, c0 = 0, k_acc = 0;
+  bool over = false;
+  while (r0 < n_reads) {
+    u64 hb[2] = {0, 0};
+    ends_upper_bound_kernel<<<1, 32, 0, st>>>(read_ends, r0, n_reads, c0 + kPieceChars,
+                                              bound.get<u64>());
+    SBWT_CUDA(cudaGetLastError());
+    SBWT_CUDA(cudaMemcpyAsync(hb, bound.get(), 16, cudaMemcpyDeviceToHost, st));
+    SBWT_CUDA(cudaStreamSynchronize(st));
+    u64 r1 = hb[0], c1 = hb[1];
+    if (r1 == r0) {  // one read longer than a piece: it is a piece of its own
+      r1 = r0 + 1;
+      SBWT_CUDA(cudaMemcpy(&c1, read_ends + r0, 8, cudaMemcpyDeviceToHost));
+    }
+    if (c1 < c0 || c1 > n_chars)
+      throw Error(SBWT_E_INVALID, "read_ends are not non-decreasing within n_chars");
+    const u64 nc = c1 - c0, nr = r1 - r0;
+    const ReadsScratch sc = scratch_for(ws, 0, nc, nr, nc, 16);
+    launch_prepare(device, k, chars + c0, nc, read_ends + r0, nr, c0, sc, st);
+    u64 n_k = 0;
+    SBWT_CUDA(cudaMemcpyAsync(&n_k, sc.total, 8, cudaMemcpyDeviceToHost, st));
+    SBWT_CUDA(cudaStreamSynchronize(st));
+    check_err_word(ws, st);
+    if (k_acc + n_k > capacity) over = true;
+    if (!over)
+      launch_search(*this, nc, read_ends + r0, nr, c0, n_k, results + k_acc,
+                    capacity - k_acc, flags, cfg, sc, st);
+    k_acc += n_k;
+    r0 = r1;
+    c0 = c1;
+  }
+  check_err_word(ws, st);
+  if (n_results) *n_results = k_acc;
+  if (over) throw Error(SBWT_E_CAPACITY, "results_capacity smaller than the k-mer count");
+}
+
 u32 IndexImpl::host_result_bytes(const LaunchConfig &cfg) const {
   ReadsView probe{};
   probe.n_kmers_bound = (64ULL << 20) + 64;
@@ -2168,6 +2231,15 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
   DeviceGuard g(device);
   Workspace &ws = workspace(device);
   if (flags & SBWT_DEVICE_POINTERS) {
+    // The 32-bit kernels index chars and k-mer slots of one launch in 32
+    // bits: a batch of 2^32 or more chars on an index they serve runs as
+    // consecutive launches of at most 2^31 chars each (whole reads).
+    if (num_bits < kNarrowLimit && n_reads &&
+        (n_chars + 64 >= (1ULL << 32) || (cfg.chunk_chars && n_chars > cfg.chunk_chars))) {
+      search_reads_device_pieces(chars, n_chars, read_ends, n_reads, results, capacity,
+                                 n_results, flags, user_stream, cfg);
+      return;
+    }
     // everything resident; the k-mer count (needed for the tiling and the
     // capacity check) comes from the device scan
     u64 n_k = 0;

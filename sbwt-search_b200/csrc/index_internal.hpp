@@ -18,14 +18,15 @@ constexpr u64 kKmerTableMaxBytes = 32ULL << 30;
 constexpr u64 kFilterBitsPerKmer = 10;
 
 // Read search kernel of an index with a k-mer table and filter by default
-// (LaunchConfig::table_kernel): the walks kernel with 2 walks per lane.
-constexpr uint32_t kDefaultTableKernel = 3;
+// (LaunchConfig::table_kernel): the walks kernel with 1 walk per lane.
+constexpr uint32_t kDefaultTableKernel = 2;
 
 struct LaunchConfig {
   uint32_t presearch_letters = 0;  // <= the handle's pyramid depth
   uint32_t blocks_per_sm = 8;      // 256-thread blocks per SM in the grid
   uint64_t tile = 0;               // k-mer slots per work tile
-  uint64_t chunk_chars = 0;        // host-pointer path: chars per chunk
+  uint64_t chunk_chars = 0;        // host-pointer path: chars per chunk (when set, also
+                                   // the piece size of device-pointer batches)
   uint32_t probe_len = 0;          // absent-prefix probe length (0 = auto, ~0u = off)
   uint32_t l2_window = 0;          // persisting L2 window over the index's hot data
   uint32_t table_kernel = kDefaultTableKernel;  // read search kernel with a k-mer table
@@ -48,6 +49,12 @@ struct IndexImpl {
   void search_reads(const char *chars, u64 n_chars, const u64 *read_ends,
                     u64 n_reads, u64 *results, u64 capacity, u64 *n_results,
                     u32 flags, cudaStream_t st, const LaunchConfig &cfg) const;
+
+  // Device-pointer read search of 2^32 or more chars: pieces of at most 2^31
+  // chars (whole reads), each on the 32-bit kernels.
+  void search_reads_device_pieces(const char *chars, u64 n_chars, const u64 *read_ends,
+                                  u64 n_reads, u64 *results, u64 capacity, u64 *n_results,
+                                  u32 flags, cudaStream_t st, const LaunchConfig &cfg) const;
 
   // Bytes per k-mer result that a host-pointer sbwt_search_reads moves from
   // the device with default flags: 4 on the walks kernel, else 8.

@@ -311,7 +311,13 @@ struct ServerImpl {
   u32 flags_ = 0;
   double tau_ = 0;
   int max_slots = 1;
-  u64 denied = 0;  // times a waiting batch found no free memory for a slot
+  u64 denied = 0;  // times a waiting batch found no free memory for a slot (under mu)
+  // A slot is built on a helper thread (device buffers, pinned buffers: a
+  // few milliseconds) while the open slots keep serving; the worker adopts
+  // it once built.
+  std::thread creator;
+  bool creating = false;                 // under mu
+  std::unique_ptr<PipelineImpl> fresh;  // built, not yet adopted (under mu)
 
   static double slot_size(const ColorsImpl *ci, u64 chars, u64 reads) {
     const double per_char = 1 + 8 + 0.375 + 1.0 / 16 + 1;  // chars, results, packing, tiles
@@ -343,36 +349,57 @@ struct ServerImpl {
     worker = std::thread([this] { run(); });
   }
 
-  // Opens one more slot when batches wait, every slot is busy and the
-  // device has room for it; called by the worker thread only.
-  bool admit_slot() {
-    if ((int)slots.size() >= max_slots) return false;
+  // Starts building one more slot when batches wait, every slot is busy and
+  // the device has room for it; called by the worker thread only.
+  void admit_slot() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (creating || fresh || (int)slots.size() >= max_slots) return;
+    }
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
       cudaGetLastError();
-      return false;
+      return;
     }
+    std::lock_guard<std::mutex> lk(mu);
     if ((double)free_b < (double)slot_bytes + (double)total_b / 8) {
       ++denied;
-      return false;
+      return;
     }
-    try {
-      auto p = std::make_unique<PipelineImpl>(ix, ci, slot_chars_, slot_reads_, flags_, tau_);
-      std::lock_guard<std::mutex> lk(mu);
-      slots.push_back(std::move(p));
-      slot_pieces.emplace_back();
-      busy.push_back(false);
-    } catch (const Error &) {
-      ++denied;  // the allocation failed after all: keep serving on the open slots
-      return false;
-    }
-    return true;
+    creating = true;
+    if (creator.joinable()) creator.join();  // the previous build has finished
+    creator = std::thread([this] {
+      std::unique_ptr<PipelineImpl> p;
+      try {
+        DeviceGuard g(ix->device);
+        p = std::make_unique<PipelineImpl>(ix, ci, slot_chars_, slot_reads_, flags_, tau_);
+      } catch (const Error &) {
+        p.reset();  // the allocation failed after all: keep serving on the open slots
+      }
+      std::lock_guard<std::mutex> lk2(mu);
+      if (p)
+        fresh = std::move(p);
+      else
+        ++denied;
+      creating = false;
+      cv_work.notify_all();
+    });
+  }
+
+  // Adopts a slot the helper thread has built; worker thread only.
+  void adopt_slot() {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!fresh) return;
+    slots.push_back(std::move(fresh));
+    slot_pieces.emplace_back();
+    busy.push_back(false);
   }
 
   ~ServerImpl() {
     stop = true;
     cv_work.notify_all();
     if (worker.joinable()) worker.join();
+    if (creator.joinable()) creator.join();
   }
 
   u64 submit(const char *chars, u64 n_chars, const u64 *ends, u64 n_reads) {
@@ -506,6 +533,7 @@ struct ServerImpl {
           deliver((int)s);
           progressed = true;
         }
+      adopt_slot();
       {
         bool all_busy = true, waiting = false;
         for (bool b : busy) all_busy &= b;

@@ -158,6 +158,36 @@ def test_pinned_host_chunks_match_device_path(kernel):
         S.set_launch_config()
 
 
+@pytest.mark.parametrize("kernel", [0, 1, S.TABLE_KERNEL_DEFAULT])
+def test_device_batch_in_pieces_matches_one_launch(kernel):
+    """A device-pointer batch split into pieces of whole reads (as batches of
+    2^32 or more chars are, for the 32-bit kernels; here forced small): the
+    same results as one launch, including the capacity error."""
+    import torch
+    g, path, sb = synthetic(7, 4, 6000, 31, 2, 0.02)
+    idx = S.SbwtIndex.open(path)
+    chars, ends = mixed_reads(g, 35, 6000, sub=0.01, n_rate=0.005, len_min=0, len_max=800)
+    exp = oracle_results(oracle_index(path, 8), chars, ends)
+    d_chars = torch.from_numpy(chars.copy()).cuda()
+    d_ends = torch.from_numpy(ends.view(np.int64).copy()).cuda()
+    S.set_table_kernel(kernel)
+    try:
+        for piece in (700, 50_001):  # 700: pieces of one read each, reads up to 800
+            S.set_launch_config(chunk_chars=piece)
+            out = torch.full((len(exp) + 8,), -7, dtype=torch.int64, device="cuda")
+            assert idx.search_reads(d_chars, d_ends, out=out) == len(exp)
+            got = out.cpu().numpy()
+            assert np.array_equal(got[:len(exp)].view(np.uint64), exp)
+            assert (got[len(exp):] == -7).all()
+        small = torch.empty(len(exp) - 1, dtype=torch.int64, device="cuda")
+        with pytest.raises(S.SbwtError) as e:
+            idx.search_reads(d_chars, d_ends, out=small)
+        assert e.value.code == S.E_CAPACITY
+    finally:
+        S.set_table_kernel(DEFAULT_TABLE_KERNEL)
+        S.set_launch_config()
+
+
 def test_errors_are_status_codes():
     with pytest.raises(S.SbwtError) as e:
         S.SbwtIndex.open("/nonexistent/file.sbwt")

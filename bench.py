@@ -711,15 +711,25 @@ def random_sector_peak(S, dev, ws_bytes):
 
 
 KERNELS = {0: "search_reads_kernel", 1: "search_table_kernel", 2: "search_walks_kernel",
-           3: "search_walks_kernel", 4: "search_walks_kernel", 5: "search_walks_kernel"}
+           3: "search_walks_kernel", 4: "search_walks_kernel", 5: "search_walks_kernel",
+           6: "search_kmers_kernel"}
 DEFAULT_KERNEL_MODE = 2
+KMERS_KERNEL_MAX_BYTES = 256 << 20  # mode 7 picks the k-mers kernel up to this
 
 
 def search_kernel_name(idx, mode: int) -> str:
     """The read search kernel that runs for `mode` (sbwt_set_table_kernel) on
     an index: without a k-mer table always the general kernel."""
     mode = DEFAULT_KERNEL_MODE if mode < 0 else mode
-    return KERNELS[mode] if idx.set_kmer_table(True) else KERNELS[0]
+    table = idx.set_kmer_table(True)
+    if not table:
+        return KERNELS[0]
+    if mode == 7:
+        mode = 6 if table + idx.filter_bytes() <= KMERS_KERNEL_MAX_BYTES else 2
+    return KERNELS[mode]
+
+
+FILTER_KERNELS = ("search_walks_kernel", "search_kmers_kernel")
 
 
 def index_working_sets(idx):
@@ -791,7 +801,7 @@ def bench_cfg1(args, S, torch, dev, tmpdir):
     L.sbwt_profile_read(None, None, None, ctr)
     L.sbwt_profile_enable(0, 0)
     kernel = search_kernel_name(idx, args.kernel)
-    n_filter = int(ctr[3]) if kernel == "search_walks_kernel" else 0
+    n_filter = int(ctr[3]) if kernel in FILTER_KERNELS else 0
     sectors = int(ctr[0]) + int(ctr[1]) + int(ctr[2]) + n_filter
     for _ in range(max(3, args.warmup)):
         step()
@@ -1149,11 +1159,9 @@ def main():
         assert np.array_equal(ho[:200_000], out_host), "e2e output differs from device path"
         e2e = {"value": n_kmers * world / e_dt, "unit": UNIT,
                "h2d_bytes_per_step": int(chars.nbytes + ends.nbytes),
-               "d2h_bytes_per_step": int(n_kmers * idx.host_result_bytes()),
+               "d2h_bytes_per_step": int(n_kmers * 8),
                "ms_per_step": e_dt * 1e3,
-               "results": "u64 per k-mer in pinned host memory (the device sends "
-                          f"{idx.host_result_bytes()} bytes per k-mer; 32-bit codes are "
-                          "widened on host threads inside the call)"}
+               "results": "u64 per k-mer, DMA into pinned host memory"}
 
     # roofline of the dominant kernel (the read search kernel)
     peak, peak_kind = load_peaks()
@@ -1161,7 +1169,7 @@ def main():
     # the kernel that ran: with the k-mer table (k <= 31) the walks kernel by
     # default, else the general kernel
     kernel = search_kernel_name(idx, args.kernel)
-    n_filter = n_probe if kernel == "search_walks_kernel" else 0
+    n_filter = n_probe if kernel in FILTER_KERNELS else 0
     if n_filter:
         n_probe = 0
     # algorithmic bytes per launch (what this kernel's algorithm must move):

@@ -69,8 +69,9 @@ typedef struct {
   uint64_t kmer_table_bytes;  /* k-mer -> node table (0 when absent) */
   uint64_t kmer_filter_bytes; /* k-mer filter in front of the table (0 when absent) */
   uint32_t host_result_bytes; /* bytes per k-mer a host-pointer sbwt_search_reads moves
-                                 device -> host with default flags: 4 (32-bit codes
-                                 widened on host threads) or 8 */
+                                 device -> host into a pageable results buffer with
+                                 default flags: 4 (32-bit codes widened on host
+                                 threads) or 8; a pinned buffer always takes 8 */
   uint32_t reserved;
 } sbwt_index_info_t;
 
@@ -279,12 +280,13 @@ int sbwt_pipeline_run(sbwt_pipeline_t *p, const char *chars, uint64_t n_chars,
  * background thread keeps every open slot busy with the pending requests in
  * arrival order (continuous batching: a request arriving while batches run
  * joins the next free slot and runs concurrently with them; a large request
- * is split over several batches).  Admission by free device memory: one slot
- * opens at creation; another opens only when batches wait, every open slot
- * is busy and the device has a slot's bytes free above a reserve of an eighth
- * of its memory (so other tenants of the GPU keep their headroom); otherwise
- * the batch waits for a running slot.  Results are identical to the single
- * calls. */
+ * is split over several batches).  Admission by free device memory: a slot
+ * opens only while the device keeps a slot's bytes free above a reserve of an
+ * eighth of its memory (so other tenants of the GPU keep their headroom):
+ * at creation the first slot and as many more as fit; later, when batches
+ * wait, every open slot is busy and memory has freed up, one more at a time
+ * (built on a helper thread); otherwise the batch waits for a running slot.
+ * Results are identical to the single calls. */
 int sbwt_server_create(const sbwt_index_t *index, const sbwt_colors_t *colors,
                        uint64_t batch_chars, uint64_t batch_reads, int slots,
                        uint32_t flags, double tau, sbwt_server_t **out);
@@ -397,8 +399,11 @@ int sbwt_set_probe_length(uint32_t probe_len);
  *       loads in flight together, and 32-byte result stores) with
  *       (walks per lane, 256-thread blocks per SM) = (1, 5), (2, 4),
  *       (2, 3), (4, 2); 2 is the default;
+ *   6 = the k-mers kernel (every k-mer on its own: filter, then table; no
+ *       stream steps, all loads of a lane independent);
+ *   7 = automatic: 6 when the table and filter take at most 256 MiB, else 2;
  *   negative = the default.
- * Results never depend on it.  Returns SBWT_E_INVALID above 5. */
+ * Results never depend on it.  Returns SBWT_E_INVALID above 7. */
 int sbwt_set_table_kernel(int mode);
 /* The process-wide launch configuration (set by sbwt_set_launch_config,
  * sbwt_set_table_kernel, sbwt_autotune); any pointer may be NULL. */
@@ -423,9 +428,10 @@ int sbwt_measure_random_sectors(int device, uint64_t bytes, int chains,
  * unit) {auto, 64, 256, 1024} and 256-thread blocks per SM in the grid
  * {2, 3, 4, 6, 8}, checks that every configuration gives the same results,
  * and makes the fastest the process-wide launch configuration.  The first
- * axis is the read search kernel (sbwt_set_table_kernel 1..5: the table
- * kernel, or the walks kernel with 1, 2 or 4 walks per lane) when the index
- * has its k-mer table, else the presearch depth (8 up to the index's).
+ * axis is the read search kernel (sbwt_set_table_kernel 1..6: the table
+ * kernel, the walks kernel with 1, 2 or 4 walks per lane, the k-mers
+ * kernel) when the index has its k-mer table, else the presearch depth (8 up
+ * to the index's).
  * sbwt_get_launch_config reads the choice back. */
 int sbwt_autotune(const sbwt_index_t *index, const char *d_chars,
                   uint64_t n_chars, const uint64_t *d_read_ends,

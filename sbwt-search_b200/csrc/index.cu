@@ -1562,6 +1562,138 @@ __global__ void __launch_bounds__(256, MINB)
   }
 }
 
+// Read search with every k-mer looked up on its own (k <= 31, k-mer table and
+// filter): no stream steps, so no lane waits on the previous k-mer of its
+// read.  A warp takes chunks of 32 * PER consecutive k-mer slots; lane j
+// handles slots j, j + 32, ... of the chunk, so every warp store writes 32
+// consecutive results.  Per slot: its read (from the tile table, a few steps
+// forward), the k chars from the packed words, -2 if one is invalid, else the
+// filter word (all PER issued together), and for the keys the filter passes
+// the k-mer table pair of slots (probed to the first empty slot).  Results
+// equal the other kernels' (the table holds exactly the SBWT's k-mers; a
+// filter rejection is exact).  It beats the stream kernels when the table and
+// filter stay in L2 and inside the address-translation reach (small indexes):
+// all loads of a lane are independent.
+template <int PER, bool COUNT>
+__global__ void __launch_bounds__(256)
+    search_kmers_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
+                        unsigned long long *counters) {
+  using I = uint32_t;
+  constexpr I CH = 32 * PER;
+  const uint32_t k = s.k;
+  const uint32_t lane = threadIdx.x & 31;
+  const I n_kmers = (I)(rv.n_kmers_dev ? *rv.n_kmers_dev : rv.n_kmers);
+  const I base = (I)rv.base;
+  const I out_cap = (I)min(rv.out_capacity, (uint64_t)~I(0));
+  const I n_chunks = (n_kmers + CH - 1) / CH;
+  const uint64_t warp0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t pol_first = l2_policy_evict_first();
+  uint64_t n_table = 0, n_filter = 0, n_known = 0;
+  for (uint64_t ch = warp0; ch < n_chunks; ch += warps) {
+    const I c0 = (I)ch * CH;
+    // the read of the chunk's first slot: from the tile table, then forward
+    I r = (I)__ldg(tile_read + c0 / (I)rv.tile);
+    while (r + 1 < (I)rv.n_reads && (I)__ldg(rv.kmer_off + r + 1) <= c0) ++r;
+    I slot[PER];
+    uint64_t key[PER], z[PER], fw[PER];
+    uint32_t state[PER];  // 0 none, 1 invalid, 2 filter
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      slot[t] = c0 + (I)t * 32 + lane;
+      state[t] = 0;
+      key[t] = 0;
+      if (slot[t] >= n_kmers) continue;
+      while ((I)__ldg(rv.kmer_off + r + 1) <= slot[t]) ++r;
+      const I pos = (r ? (I)__ldg(rv.ends + r - 1) : base) - base +
+                    (slot[t] - (I)__ldg(rv.kmer_off + r));
+      // invalid chars in [pos, pos + k): 32-bit words pos >> 5 and the next
+      const I wi = pos >> 5;
+      const uint32_t off = pos & 31;
+      const uint64_t inv = (uint64_t)__ldg(rv.invalid + wi) |
+                           ((uint64_t)__ldg(rv.invalid + wi + 1) << 32);
+      if ((inv >> off) & low_mask(k)) {
+        state[t] = 1;
+        continue;
+      }
+      const uint64_t w0 = __ldg(rv.packed + wi), w1 = __ldg(rv.packed + wi + 1);
+      const uint64_t v = off ? (w0 << (2 * off)) | (w1 >> (64 - 2 * off)) : w0;
+      key[t] = v >> (64 - 2 * k);
+      state[t] = 2;
+    }
+    // filter words, all issued before any is used
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      fw[t] = 0;
+      z[t] = 0;
+      if (state[t] == 2) {
+        z[t] = kmer_mix(key[t]);
+        fw[t] = load_u64_nc(s.kmer_filter + kmer_filter_word(z[t], s.filter_words));
+      }
+    }
+    uint64_t res[PER];
+    bool look[PER];
+    I hs[PER];
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      res[t] = state[t] == 1 ? (uint64_t)SBWT_INVALID : (uint64_t)SBWT_NOT_FOUND;
+      const uint64_t bits = kmer_filter_bits(z[t]);
+      look[t] = state[t] == 2 && (fw[t] & bits) == bits;
+      hs[t] = look[t] ? (I)kmer_table_slot(z[t], s.kmer_table_mask) : 0;
+      if (COUNT) {
+        n_filter += state[t] == 2;
+        n_known += state[t] == 1;
+      }
+    }
+    // table probes of the keys the filter passed, one round of loads at a time
+    while (true) {
+      bool any = false;
+      Block A[PER];
+#pragma unroll
+      for (int t = 0; t < PER; ++t) {
+        A[t] = Block{0, 0, 0, 0};
+        if (look[t]) {
+          A[t] = load_block_hint(
+              reinterpret_cast<const Block *>(s.kmer_table + 2 * (uint64_t)hs[t]), pol_first);
+          any = true;
+        }
+      }
+      if (!any) break;
+#pragma unroll
+      for (int t = 0; t < PER; ++t) {
+        if (!look[t]) continue;
+        if (COUNT) ++n_table;
+        if (A[t].w0 == key[t]) {
+          res[t] = A[t].w1;
+          look[t] = false;
+        } else if (A[t].w2 == key[t]) {
+          res[t] = A[t].w3;
+          look[t] = false;
+        } else if (A[t].w0 == ~0ULL || A[t].w2 == ~0ULL) {
+          look[t] = false;  // an empty slot: absent
+        } else {
+          hs[t] = (I)(((uint64_t)hs[t] + 2) & s.kmer_table_mask);
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      if (slot[t] >= n_kmers || slot[t] >= out_cap) continue;
+      if (rv.out32)
+        __stcs(rv.out32 + slot[t], (unsigned int)res[t]);
+      else
+        __stcs(rv.out + slot[t], (unsigned long long)res[t]);
+    }
+  }
+  if (COUNT) {
+    atomicAdd(counters + 0, (unsigned long long)n_table);
+    atomicAdd(counters + 3, (unsigned long long)n_filter);
+    atomicAdd(counters + 6, (unsigned long long)n_known);
+    atomicAdd(counters + 9, (unsigned long long)n_filter);   // filter words
+    atomicAdd(counters + 12, (unsigned long long)n_table);   // table lookups
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -1625,8 +1757,9 @@ static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStrea
 
 // kernel_mode: 0 = the general kernel; 1 = the table kernel; 2..5 = the
 // walks kernel with (walks per lane, blocks per SM) = (1, 5), (2, 4), (2, 3),
-// (4, 2) (the table kernel when the index has no k-mer filter).  Results
-// never depend on it.
+// (4, 2) (the table kernel when the index has no k-mer filter); 6 = the
+// k-mers kernel; 7 = 6 when the table and filter are small, else 2.
+// Results never depend on it.
 // Whether launch_search_kernel runs the walks kernel (the only one that can
 // write 32-bit results, ReadsView::out32).
 static bool walks_kernel_applies(const SbwtView &sv, const ReadsView &rv, bool stream,
@@ -1634,6 +1767,15 @@ static bool walks_kernel_applies(const SbwtView &sv, const ReadsView &rv, bool s
   const bool narrow = sv.num_bits < kNarrowLimit && rv.n_kmers_bound < (1ULL << 32);
   return kernel_mode >= 2 && stream && narrow && sv.kmer_table && sv.kmer_filter &&
          sv.k <= 31 && mtk == 0 && sv.suffix_group_starts;
+}
+
+// The k-mers kernel (mode 6) has the walks kernel's conditions; mode 7
+// (automatic) picks it when the table and filter fit kKmersKernelMaxBytes.
+constexpr u64 kKmersKernelMaxBytes = 256ULL << 20;
+static uint32_t resolve_kernel_mode(const SbwtView &sv, uint32_t kernel_mode) {
+  if (kernel_mode != 7) return kernel_mode;
+  const u64 bytes = (sv.kmer_table_mask + 1) * 16 + sv.filter_words * 8;
+  return sv.kmer_table && bytes <= kKmersKernelMaxBytes ? 6u : 2u;
 }
 
 // instrument = false keeps the launch free of the profiler's events and
@@ -1666,6 +1808,7 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
   const bool narrow = sv.num_bits < kNarrowLimit && rv.n_kmers_bound < (1ULL << 32);
   const bool table = kernel_mode != 0 && stream && narrow && sv.kmer_table && sv.k <= 31 &&
                      mtk == 0 && sv.suffix_group_starts;
+  kernel_mode = resolve_kernel_mode(sv, kernel_mode);
   const bool walks = walks_kernel_applies(sv, rv, stream, mtk, kernel_mode);
   if (rv.out32 && !walks)
     throw Error(SBWT_E_INVALID, "32-bit results need the walks kernel");
@@ -1691,7 +1834,11 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
     if (kernel_mode == 2) SBWT_WALKS(1, 5);
     else if (kernel_mode == 3) SBWT_WALKS(2, 4);
     else if (kernel_mode == 4) SBWT_WALKS(2, 3);
-    else SBWT_WALKS(4, 2);
+    else if (kernel_mode == 5) SBWT_WALKS(4, 2);
+    else if (ctr)
+      launch_ex(search_kmers_kernel<4, true>, grid, threads, st, la, sv, rv, tile_read, ctr);
+    else
+      launch_ex(search_kmers_kernel<4, false>, grid, threads, st, la, sv, rv, tile_read, ctr);
 #undef SBWT_WALKS
   } else if (table) {
     if (ctr)
@@ -2219,7 +2366,7 @@ u32 IndexImpl::host_result_bytes(const LaunchConfig &cfg) const {
   probe.n_kmers_bound = (64ULL << 20) + 64;
   const SbwtView sv = view_for(cfg.presearch_letters);
   return walks_kernel_applies(sv, probe, view.suffix_group_starts != nullptr, 0,
-                              cfg.table_kernel)
+                              resolve_kernel_mode(sv, cfg.table_kernel))
              ? 4u
              : 8u;
 }
@@ -2266,8 +2413,10 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
   // ends, its k-mers and the ends' order checked over its own reads) while the
   // previous one is on the GPU, and its results are only copied back once
   // they fit the capacity.
-  // With the walks kernel the results of a chunk cross PCIe as 32-bit codes
-  // into a pinned staging buffer and are widened to u64 on host threads
+  // A pinned results buffer receives u64 results by DMA.  A pageable one
+  // would take them through the driver's staging copies; with the walks or
+  // k-mers kernel the results of a chunk then cross PCIe as 32-bit codes into
+  // a pinned staging buffer instead and are widened to u64 on host threads
   // while the next chunk runs (half the device-to-host bytes).
   const u64 chunk_chars = cfg.chunk_chars ? cfg.chunk_chars : (64ULL << 20);
   const bool pinned_in = is_host_pinned(chars) && is_host_pinned(read_ends);
@@ -2309,8 +2458,9 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
     const u64 nc = prev - c0, nr = r1 - r0;
     ReadsView probe{};
     probe.n_kmers_bound = std::max<u64>(nc, nr) + 64;
-    const bool narrow =
-        walks_kernel_applies(sv_host, probe, stream_host, mtk_host, cfg.table_kernel);
+    const bool narrow = !pinned && walks_kernel_applies(sv_host, probe, stream_host, mtk_host,
+                                                        resolve_kernel_mode(sv_host,
+                                                                            cfg.table_kernel));
     ws.chars[b].ensure(nc + 16);
     ws.ends[b].ensure(nr * 8);
     if (narrow)

@@ -162,8 +162,8 @@ TABLE_KERNEL_DEFAULT = -1
 def set_table_kernel(mode: int = TABLE_KERNEL_DEFAULT) -> None:
     """Read search kernel of an index with a k-mer table: 0 general, 1 table
     (True), 2..5 walks kernel with (walks per lane, blocks per SM) = (1, 5),
-    (2, 4), (2, 3), (4, 2), -1 the library default.  Results never depend
-    on it."""
+    (2, 4), (2, 3), (4, 2), 6 k-mers kernel, 7 automatic (6 for small
+    tables, else 2), -1 the library default.  Results never depend on it."""
     check(lib().sbwt_set_table_kernel(int(mode)))
 
 
@@ -259,7 +259,8 @@ class SbwtIndex:
         return nb.value
 
     def host_result_bytes(self) -> int:
-        """Bytes per k-mer a host-pointer search_reads moves device -> host."""
+        """Bytes per k-mer a host-pointer search_reads moves device -> host
+        into a pageable results buffer (a pinned one always takes 8)."""
         info = IndexInfo()
         check(lib().sbwt_index_get_info(self._h, C.byref(info)))
         return int(info.host_result_bytes)

@@ -14,9 +14,10 @@ pytestmark = pytest.mark.gpu
 
 # the library's default choice of read search kernel for indexes with a k-mer table
 DEFAULT_TABLE_KERNEL = S.TABLE_KERNEL_DEFAULT
-# read search kernels of an index with a k-mer table: general, table, and the
-# walks kernel as (walks per lane, blocks per SM) = (1, 5), (2, 4), (2, 3), (4, 2)
-KERNEL_MODES = [0, 1, 2, 3, 4, 5]
+# read search kernels of an index with a k-mer table: general, table, the
+# walks kernel as (walks per lane, blocks per SM) = (1, 5), (2, 4), (2, 3),
+# (4, 2), the k-mers kernel, automatic
+KERNEL_MODES = [0, 1, 2, 3, 4, 5, 6, 7]
 
 
 @pytest.fixture(scope="module")
@@ -130,13 +131,14 @@ def test_chunked_host_pipeline_matches_single_chunk():
     assert np.array_equal(one, many)
 
 
-@pytest.mark.parametrize("kernel", [1, S.TABLE_KERNEL_DEFAULT])
-def test_pinned_host_chunks_match_device_path(kernel):
-    """Host-pointer calls from pinned memory, many chunks in flight: on the
-    walks kernel the results cross as 32-bit codes and are widened on host
-    threads (with an output start that is not 16-byte aligned), on the table
-    kernel as u64; both equal the oracle, and no slot outside the output is
-    written."""
+@pytest.mark.parametrize("pinned_out", [True, False])
+@pytest.mark.parametrize("kernel", [1, 2, 6])
+def test_pinned_host_chunks_match_device_path(kernel, pinned_out):
+    """Host-pointer calls from pinned inputs, many chunks in flight.  Into a
+    pageable output on the walks and k-mers kernels the results cross as
+    32-bit codes and are widened on host threads (output start not 16-byte
+    aligned); into a pinned output, and on the table kernel, as u64.  All
+    equal the oracle, and no slot outside the output is written."""
     import torch
     g, path, sb = synthetic(7, 4, 6000, 31, 2, 0.02)
     idx = S.SbwtIndex.open(path)
@@ -148,7 +150,9 @@ def test_pinned_host_chunks_match_device_path(kernel):
         assert idx.host_result_bytes() == (4 if kernel != 1 else 8)
         h_chars = torch.from_numpy(chars.copy()).pin_memory()
         h_ends = torch.from_numpy(ends.view(np.int64).copy()).pin_memory()
-        h_out = torch.full((len(exp) + 3,), -7, dtype=torch.int64).pin_memory()
+        h_out = torch.full((len(exp) + 3,), -7, dtype=torch.int64)
+        if pinned_out:
+            h_out = h_out.pin_memory()
         out = h_out.numpy()[1:1 + len(exp)].view(np.uint64)
         idx.search_reads(h_chars.numpy(), h_ends.numpy().view(np.uint64), out=out)
         assert np.array_equal(out, exp)
@@ -158,7 +162,7 @@ def test_pinned_host_chunks_match_device_path(kernel):
         S.set_launch_config()
 
 
-@pytest.mark.parametrize("kernel", [0, 1, S.TABLE_KERNEL_DEFAULT])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 6])
 def test_device_batch_in_pieces_matches_one_launch(kernel):
     """A device-pointer batch split into pieces of whole reads (as batches of
     2^32 or more chars are, for the 32-bit kernels; here forced small): the

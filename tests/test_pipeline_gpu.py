@@ -112,24 +112,28 @@ def test_server_index_mode_splits_large_requests():
 
 
 def test_server_admits_slots_by_free_device_memory():
-    """The server opens one slot at creation and more only while batches
-    wait and the device has a slot's bytes free above an eighth of its
-    memory.  With that room taken by another allocation no slot opens (the
-    refusals are counted) and requests still complete, on the one slot, with
-    the results of direct calls."""
+    """A slot opens only while the device keeps a slot's bytes free above an
+    eighth of its memory: with room, all slots open at creation; with that
+    room taken by another allocation only the first opens, waiting batches
+    find no room (the refusals are counted) and requests still complete on
+    it with the results of direct calls; once the memory is back, slots open
+    again as batches wait."""
     import torch
     g, sp, cp = colored()
     idx, ci = S.SbwtIndex.open(sp), S.ColorIndex.open(cp)
-    srv = S.Server(idx, ci, batch_chars=200_000, batch_reads=1500, slots=4, tau=0.7)
-    info = srv.slots()
-    assert info["open"] == 1 and info["slot_bytes"] > 0
     reqs = _requests(g, 24, 5)
     p = S.Pipeline(idx, ci, 1 << 22, 1 << 16, tau=0.7)
     exp = [p.run(*r) for r in reqs]
+    srv = S.Server(idx, ci, batch_chars=200_000, batch_reads=1500, slots=4, tau=0.7)
+    info = srv.slots()
+    assert info["open"] == 4 and info["slot_bytes"] > 0
+    srv.close()
     free, total = torch.cuda.mem_get_info()
     keep = total // 8 + info["slot_bytes"] // 2  # less than a slot above the reserve
     hog = torch.empty(max(free - keep, 0), dtype=torch.uint8, device="cuda")
     try:
+        srv = S.Server(idx, ci, batch_chars=200_000, batch_reads=1500, slots=4, tau=0.7)
+        assert srv.slots()["open"] == 1
         got = [srv.wait(rid) for rid in [srv.submit(*r) for r in reqs]]
         assert got == exp
         after = srv.slots()

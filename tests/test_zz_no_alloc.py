@@ -82,7 +82,7 @@ def _reads(n_reads, length, seed):
 
 @pytest.mark.parametrize("shape", [(MAX_READS, MAX_CHARS // MAX_READS),
                                    (MAX_CHARS // 400, 400)])
-@pytest.mark.parametrize("kernel", [0, 1, S.TABLE_KERNEL_DEFAULT])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 6])
 def test_noalloc_at_its_limits_allocates_nothing(shape, kernel):
     """A batch at the stated limits (every read slot used, or nearly every
     char with the smallest tile, 16 k-mers, so that the tile table is full)

@@ -713,7 +713,7 @@ def random_sector_peak(S, dev, ws_bytes):
 KERNELS = {0: "search_reads_kernel", 1: "search_table_kernel", 2: "search_walks_kernel",
            3: "search_walks_kernel", 4: "search_walks_kernel", 5: "search_walks_kernel",
            6: "search_kmers_kernel"}
-DEFAULT_KERNEL_MODE = 2
+DEFAULT_KERNEL_MODE = 7
 KMERS_KERNEL_MAX_BYTES = 256 << 20  # mode 7 picks the k-mers kernel up to this
 
 
@@ -725,7 +725,8 @@ def search_kernel_name(idx, mode: int) -> str:
     if not table:
         return KERNELS[0]
     if mode == 7:
-        mode = 6 if table + idx.filter_bytes() <= KMERS_KERNEL_MAX_BYTES else 2
+        mode = 6 if 0 < idx.filter_bytes() and table + idx.filter_bytes() <= \
+            KMERS_KERNEL_MAX_BYTES else 1
     return KERNELS[mode]
 
 

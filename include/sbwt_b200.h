@@ -398,10 +398,11 @@ int sbwt_set_probe_length(uint32_t probe_len);
  *       filter in front of the table, several tiles per lane with their
  *       loads in flight together, and 32-byte result stores) with
  *       (walks per lane, 256-thread blocks per SM) = (1, 5), (2, 4),
- *       (2, 3), (4, 2); 2 is the default;
+ *       (2, 3), (4, 2);
  *   6 = the k-mers kernel (every k-mer on its own: filter, then table; no
  *       stream steps, all loads of a lane independent);
- *   7 = automatic: 6 when the table and filter take at most 256 MiB, else 2;
+ *   7 = automatic, the default: 6 when the table and filter take at most
+ *       256 MiB, else 1;
  *   negative = the default.
  * Results never depend on it.  Returns SBWT_E_INVALID above 7. */
 int sbwt_set_table_kernel(int mode);

@@ -113,11 +113,14 @@ __device__ __forceinline__ void add_weighted(uint64_t *planes, uint32_t stride, 
   }
 }
 
+// 2 rows in flight at a 12-blocks-per-SM register budget: 21.9 ms against
+// 23.6 ms for 4 rows at 6 blocks (2 M reads of the 2000-genome workload);
+// more rows in flight cost occupancy and were slower (8 rows: 44-50 ms)
 #ifndef SBWT_COLORS_ROWS_IN_FLIGHT
-#define SBWT_COLORS_ROWS_IN_FLIGHT 4
+#define SBWT_COLORS_ROWS_IN_FLIGHT 2
 #endif
 #ifndef SBWT_COLORS_BLOCKS_PER_SM
-#define SBWT_COLORS_BLOCKS_PER_SM 6
+#define SBWT_COLORS_BLOCKS_PER_SM 12
 #endif
 constexpr int kRowsInFlight = SBWT_COLORS_ROWS_IN_FLIGHT;  // dense rows loaded before the adds
 constexpr int kWindows = 4;  // windows of 32 k-mers whose lookups overlap

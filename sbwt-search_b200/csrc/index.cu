@@ -1218,7 +1218,10 @@ __device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_
 
 // W walks per lane; MINB = 256-thread blocks per SM the register budget
 // targets (W = 1: 5, W = 2: 4 or 3, W = 4: 2).
-template <int W, int MINB, bool COUNT>
+// LEAN: no filter and no staging (a walk without a previous node goes to the
+// table at once; each result is one 8-byte store), i.e. search_table_kernel's
+// work with W walks per lane.
+template <int W, int MINB, bool COUNT, bool LEAN = false>
 __global__ void __launch_bounds__(256, MINB)
     search_walks_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
                         unsigned long long *counters) {
@@ -1281,6 +1284,16 @@ __global__ void __launch_bounds__(256, MINB)
     omask[w] = 0;
   };
   auto emit = [&](int w, I sl, I node) {
+    if (LEAN) {
+      if (sl < out_cap) {
+        if (out32)
+          __stcs(out32 + sl, (unsigned int)node);
+        else
+          __stcs(rv.out + sl,
+                 node == NONE ? (unsigned long long)SBWT_NOT_FOUND : (unsigned long long)node);
+      }
+      return;
+    }
     const I g = sl & ~I(3);
     if (omask[w] && g != obase[w]) flush(w);
     obase[w] = g;
@@ -1378,6 +1391,9 @@ __global__ void __launch_bounds__(256, MINB)
         if (v[w] != NONE) {
           x[w] = v[w];
           mode[w] = WK_STREAM;
+        } else if (LEAN) {
+          hslot[w] = (I)kmer_table_bucket(cw[w].prefix(pos[w], k), s.kmer_table_mask);
+          mode[w] = WK_HASH;
         } else {
           // k-mers pos .. pos + nb - 1 of this read and tile, in the char
           // window, whose chars after newc are valid
@@ -1758,7 +1774,8 @@ static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStrea
 // kernel_mode: 0 = the general kernel; 1 = the table kernel; 2..5 = the
 // walks kernel with (walks per lane, blocks per SM) = (1, 5), (2, 4), (2, 3),
 // (4, 2) (the table kernel when the index has no k-mer filter); 6 = the
-// k-mers kernel; 7 = 6 when the table and filter are small, else 2.
+// k-mers kernel; 7 = 6 when the table and filter are small, else 1; 8, 9 =
+// the walks kernel without filter and staging, 1 or 2 walks per lane.
 // Results never depend on it.
 // Whether launch_search_kernel runs the walks kernel (the only one that can
 // write 32-bit results, ReadsView::out32).
@@ -1769,13 +1786,17 @@ static bool walks_kernel_applies(const SbwtView &sv, const ReadsView &rv, bool s
          sv.k <= 31 && mtk == 0 && sv.suffix_group_starts;
 }
 
-// The k-mers kernel (mode 6) has the walks kernel's conditions; mode 7
-// (automatic) picks it when the table and filter fit kKmersKernelMaxBytes.
+// The k-mers kernel (mode 6) has the walks kernel's conditions.  Mode 7
+// (automatic, the default) picks it when the table and filter fit
+// kKmersKernelMaxBytes (they then stay in L2 and inside the translation
+// reach, and independent lookups beat the chained stream steps), else the
+// table kernel (a large table: the stream steps' rank blocks are the smaller
+// random working set).
 constexpr u64 kKmersKernelMaxBytes = 256ULL << 20;
 static uint32_t resolve_kernel_mode(const SbwtView &sv, uint32_t kernel_mode) {
   if (kernel_mode != 7) return kernel_mode;
   const u64 bytes = (sv.kmer_table_mask + 1) * 16 + sv.filter_words * 8;
-  return sv.kmer_table && bytes <= kKmersKernelMaxBytes ? 6u : 2u;
+  return sv.kmer_table && sv.kmer_filter && bytes <= kKmersKernelMaxBytes ? 6u : 1u;
 }
 
 // instrument = false keeps the launch free of the profiler's events and
@@ -1822,6 +1843,15 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
                 tile_read, mtk, d_err, ctr);                                             \
   } while (0)
   if (walks) {
+#define SBWT_LEAN(W_, B_)                                                                  \
+  do {                                                                                     \
+    if (ctr)                                                                               \
+      launch_ex(search_walks_kernel<W_, B_, true, true>, grid, threads, st, la, sv, rv,    \
+                tile_read, ctr);                                                           \
+    else                                                                                   \
+      launch_ex(search_walks_kernel<W_, B_, false, true>, grid, threads, st, la, sv, rv,   \
+                tile_read, ctr);                                                           \
+  } while (0)
 #define SBWT_WALKS(W_, B_)                                                                 \
   do {                                                                                     \
     if (ctr)                                                                               \
@@ -1835,11 +1865,14 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
     else if (kernel_mode == 3) SBWT_WALKS(2, 4);
     else if (kernel_mode == 4) SBWT_WALKS(2, 3);
     else if (kernel_mode == 5) SBWT_WALKS(4, 2);
+    else if (kernel_mode == 8) SBWT_LEAN(1, 5);
+    else if (kernel_mode == 9) SBWT_LEAN(2, 3);
     else if (ctr)
       launch_ex(search_kmers_kernel<4, true>, grid, threads, st, la, sv, rv, tile_read, ctr);
     else
       launch_ex(search_kmers_kernel<4, false>, grid, threads, st, la, sv, rv, tile_read, ctr);
 #undef SBWT_WALKS
+#undef SBWT_LEAN
   } else if (table) {
     if (ctr)
       launch_ex(search_table_kernel<true>, grid, threads, st, la, sv, rv, tile_read, ctr);
@@ -2163,8 +2196,11 @@ static u64 tile_size(int device, u64 n_kmers, const LaunchConfig &cfg) {
   if (cfg.tile) return cfg.tile;
   const u64 resident = (u64)sm_count(device) * cfg.blocks_per_sm * 256;
   u64 tile = n_kmers / (resident * 8);
-  // a multiple of 4 slots: the walks kernel stores 4 results per 32 bytes
-  return (std::min<u64>(std::max<u64>(tile, 16), 1024) + 3) & ~3ULL;
+  // at most 128 slots: the tiles in flight then span less of the chars and
+  // results (fewer pages and DRAM rows at a time; 10 % faster than 577 on the
+  // 100 Mbp workload); a multiple of 4 slots: the walks kernel stores 4
+  // results per 32 bytes
+  return (std::min<u64>(std::max<u64>(tile, 16), 128) + 3) & ~3ULL;
 }
 
 // Scan of per-read k-mer counts and the packing of the chars (device-resident

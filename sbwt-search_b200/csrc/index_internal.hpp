@@ -17,9 +17,10 @@ constexpr u64 kKmerTableMaxBytes = 32ULL << 30;
 // Bits per k-mer of the k-mer filter built with the table.
 constexpr u64 kFilterBitsPerKmer = 10;
 
-// Read search kernel of an index with a k-mer table and filter by default
-// (LaunchConfig::table_kernel): the walks kernel with 1 walk per lane.
-constexpr uint32_t kDefaultTableKernel = 2;
+// Read search kernel of an index with a k-mer table by default
+// (LaunchConfig::table_kernel): automatic (the k-mers kernel for small
+// tables, else the table kernel).
+constexpr uint32_t kDefaultTableKernel = 7;
 
 struct LaunchConfig {
   uint32_t presearch_letters = 0;  // <= the handle's pyramid depth

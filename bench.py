@@ -527,6 +527,8 @@ def parse():
     ap.add_argument("--colors-reads", type=int, default=CFG3["n_reads"])
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--colors-cpu-reads", type=int, default=200_000)
+    ap.add_argument("--cli-full", action=argparse.BooleanOptionalAction, default=True,
+                    help="time the CLI file -> file on all reads of the workload")
     ap.add_argument("--no-full-batched", action="store_true",
                     help="skip the full-size batched workload")
     ap.add_argument("--colors-plain-reads", type=int, default=500_000)
@@ -712,7 +714,8 @@ def random_sector_peak(S, dev, ws_bytes):
 
 KERNELS = {0: "search_reads_kernel", 1: "search_table_kernel", 2: "search_walks_kernel",
            3: "search_walks_kernel", 4: "search_walks_kernel", 5: "search_walks_kernel",
-           6: "search_kmers_kernel"}
+           6: "search_kmers_kernel", 8: "search_walks_kernel", 9: "search_walks_kernel",
+           10: "search_walks_kernel"}
 DEFAULT_KERNEL_MODE = 7
 KMERS_KERNEL_MAX_BYTES = 256 << 20  # mode 7 picks the k-mers kernel up to this
 
@@ -961,6 +964,45 @@ def bench_io(args, S, torch, dev, tmpdir, idx, path, chars, ends, d_out, d_ends,
                              "--no-headers", "wall_s": t_cli, "kmers": n_sk,
                   "kmers_per_s_incl_index_load": n_sk / t_cli,
                   "output_equal_host_writer": bool(cli_same), "rc": r.returncode}
+    if args.cli_full:
+        # file -> file on all reads of the workload: the FASTQ written in
+        # pieces, the CLI once on an empty query (process start, index load:
+        # rank blocks, presearch pyramid, k-mer table and filter) and once on
+        # the full query; the difference is the search itself, file to file
+        full = os.path.join(tmpdir, "full.fq")
+        with open(full, "wb") as f:
+            for lo in range(0, len(ends), 1_000_000):
+                hi = min(len(ends), lo + 1_000_000)
+                base = int(ends[lo - 1]) if lo else 0
+                f.write(fastq_text(chars[base:int(ends[hi - 1])], ends[lo:hi] - base).tobytes())
+        empty = os.path.join(tmpdir, "empty.fq")
+        open(empty, "wb").close()
+        fq_bytes = os.path.getsize(full)
+        t0 = time.perf_counter()
+        r0 = subprocess.run([str(cli), "index", "-i", path, "-q", empty, "-o",
+                             os.path.join(tmpdir, "cli_empty"), "--no-headers"],
+                            capture_output=True)
+        t_load = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        r1 = subprocess.run([str(cli), "index", "-i", path, "-q", full, "-o",
+                             os.path.join(tmpdir, "cli_full"), "--no-headers"],
+                            capture_output=True)
+        t_all = time.perf_counter() - t0
+        out_bytes = os.path.getsize(os.path.join(tmpdir, "cli_full.txt")) if r1.returncode == 0 \
+            else 0
+        for x in ("full.fq", "cli_full.txt"):
+            try:
+                os.remove(os.path.join(tmpdir, x))
+            except OSError:
+                pass
+        out["cli_full"] = {
+            "command": "sbwt_search index -i <cfg2.sbwt> -q <all reads as FASTQ> -o <prefix> "
+                       "--no-headers (ascii output)",
+            "reads": int(len(ends)), "kmers": int(n_kmers), "fastq_bytes": int(fq_bytes),
+            "output_bytes": int(out_bytes), "rc": [r0.returncode, r1.returncode],
+            "wall_s": t_all, "index_load_and_start_s": t_load,
+            "kmers_per_s_file_to_file": n_kmers / max(t_all - t_load, 1e-9),
+            "kmers_per_s_incl_index_load": n_kmers / t_all}
     return out
 
 

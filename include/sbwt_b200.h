@@ -403,8 +403,11 @@ int sbwt_set_probe_length(uint32_t probe_len);
  *       stream steps, all loads of a lane independent);
  *   7 = automatic, the default: 6 when the table and filter take at most
  *       256 MiB, else 1;
+ *   8, 9 = the walks kernel without the filter and the staged stores, 1 or 2
+ *       walks per lane; 10 = the same with 1 walk and the filter in front of
+ *       the table, one k-mer at a time;
  *   negative = the default.
- * Results never depend on it.  Returns SBWT_E_INVALID above 7. */
+ * Results never depend on it.  Returns SBWT_E_INVALID above 10. */
 int sbwt_set_table_kernel(int mode);
 /* The process-wide launch configuration (set by sbwt_set_launch_config,
  * sbwt_set_table_kernel, sbwt_autotune); any pointer may be NULL. */

@@ -1221,7 +1221,8 @@ __device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_
 // LEAN: no filter and no staging (a walk without a previous node goes to the
 // table at once; each result is one 8-byte store), i.e. search_table_kernel's
 // work with W walks per lane.
-template <int W, int MINB, bool COUNT, bool LEAN = false>
+// LFILTER (with LEAN): the filter in front of the table, one k-mer at a time.
+template <int W, int MINB, bool COUNT, bool LEAN = false, bool LFILTER = false>
 __global__ void __launch_bounds__(256, MINB)
     search_walks_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
                         unsigned long long *counters) {
@@ -1391,6 +1392,9 @@ __global__ void __launch_bounds__(256, MINB)
         if (v[w] != NONE) {
           x[w] = v[w];
           mode[w] = WK_STREAM;
+        } else if (LEAN && LFILTER) {
+          nb[w] = 1;
+          mode[w] = WK_FILTER;
         } else if (LEAN) {
           hslot[w] = (I)kmer_table_bucket(cw[w].prefix(pos[w], k), s.kmer_table_mask);
           mode[w] = WK_HASH;
@@ -1775,7 +1779,8 @@ static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStrea
 // walks kernel with (walks per lane, blocks per SM) = (1, 5), (2, 4), (2, 3),
 // (4, 2) (the table kernel when the index has no k-mer filter); 6 = the
 // k-mers kernel; 7 = 6 when the table and filter are small, else 1; 8, 9 =
-// the walks kernel without filter and staging, 1 or 2 walks per lane.
+// the walks kernel without filter and staging, 1 or 2 walks per lane; 10 =
+// the same with the filter in front of the table, one k-mer at a time.
 // Results never depend on it.
 // Whether launch_search_kernel runs the walks kernel (the only one that can
 // write 32-bit results, ReadsView::out32).
@@ -1843,14 +1848,14 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
                 tile_read, mtk, d_err, ctr);                                             \
   } while (0)
   if (walks) {
-#define SBWT_LEAN(W_, B_)                                                                  \
+#define SBWT_LEAN(W_, B_, F_)                                                              \
   do {                                                                                     \
     if (ctr)                                                                               \
-      launch_ex(search_walks_kernel<W_, B_, true, true>, grid, threads, st, la, sv, rv,    \
+      launch_ex(search_walks_kernel<W_, B_, true, true, F_>, grid, threads, st, la, sv, rv, \
                 tile_read, ctr);                                                           \
     else                                                                                   \
-      launch_ex(search_walks_kernel<W_, B_, false, true>, grid, threads, st, la, sv, rv,   \
-                tile_read, ctr);                                                           \
+      launch_ex(search_walks_kernel<W_, B_, false, true, F_>, grid, threads, st, la, sv,   \
+                rv, tile_read, ctr);                                                       \
   } while (0)
 #define SBWT_WALKS(W_, B_)                                                                 \
   do {                                                                                     \
@@ -1865,8 +1870,9 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
     else if (kernel_mode == 3) SBWT_WALKS(2, 4);
     else if (kernel_mode == 4) SBWT_WALKS(2, 3);
     else if (kernel_mode == 5) SBWT_WALKS(4, 2);
-    else if (kernel_mode == 8) SBWT_LEAN(1, 5);
-    else if (kernel_mode == 9) SBWT_LEAN(2, 3);
+    else if (kernel_mode == 8) SBWT_LEAN(1, 5, false);
+    else if (kernel_mode == 9) SBWT_LEAN(2, 3, false);
+    else if (kernel_mode == 10) SBWT_LEAN(1, 5, true);
     else if (ctr)
       launch_ex(search_kmers_kernel<4, true>, grid, threads, st, la, sv, rv, tile_read, ctr);
     else

@@ -1600,9 +1600,11 @@ __global__ void __launch_bounds__(256)
                         unsigned long long *counters) {
   using I = uint32_t;
   constexpr I CH = 32 * PER;
+  constexpr int MR = 5;  // reads of a chunk resolved from one round of loads
   const uint32_t k = s.k;
   const uint32_t lane = threadIdx.x & 31;
   const I n_kmers = (I)(rv.n_kmers_dev ? *rv.n_kmers_dev : rv.n_kmers);
+  const I n_reads = (I)rv.n_reads;
   const I base = (I)rv.base;
   const I out_cap = (I)min(rv.out_capacity, (uint64_t)~I(0));
   const I n_chunks = (n_kmers + CH - 1) / CH;
@@ -1610,36 +1612,76 @@ __global__ void __launch_bounds__(256)
   const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint64_t pol_first = l2_policy_evict_first();
   uint64_t n_table = 0, n_filter = 0, n_known = 0;
+  // Every phase below issues all its loads before it uses any (no load waits
+  // on a branch over another's value), so one chunk costs about four
+  // round trips: read offsets, chars, filter words, table.  The tile-table
+  // entry of the next chunk is loaded one chunk ahead.
+  I r_next = warp0 < n_chunks ? (I)__ldg(tile_read + (I)warp0 * CH / (I)rv.tile) : 0;
   for (uint64_t ch = warp0; ch < n_chunks; ch += warps) {
     const I c0 = (I)ch * CH;
-    // the read of the chunk's first slot: from the tile table, then forward
-    I r = (I)__ldg(tile_read + c0 / (I)rv.tile);
-    while (r + 1 < (I)rv.n_reads && (I)__ldg(rv.kmer_off + r + 1) <= c0) ++r;
-    I slot[PER];
+    I r = r_next;
+    if (ch + warps < n_chunks)
+      r_next = (I)__ldg(tile_read + (I)(ch + warps) * CH / (I)rv.tile);
+    // offsets and ends of reads r .. r + MR - 1 (one round of loads); the
+    // chunk's first read is r itself when the tile size divides the chunk
+    I ko[MR + 1], st[MR];
+    while (true) {
+#pragma unroll
+      for (int j = 0; j <= MR; ++j) ko[j] = (I)__ldg(rv.kmer_off + min(r + j, n_reads));
+#pragma unroll
+      for (int j = 0; j < MR; ++j) {
+        const I rr = min(r + j, n_reads);
+        st[j] = (rr ? (I)__ldg(rv.ends + rr - 1) : base) - base;
+      }
+      if (ko[1] > c0 || r + 1 >= n_reads) break;
+      // forward to the chunk's first read (tiles that do not divide chunks)
+      while (r + 1 < n_reads && (I)__ldg(rv.kmer_off + r + 1) <= c0) ++r;
+    }
+    I slot[PER], pos[PER];
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      slot[t] = c0 + (I)t * 32 + lane;
+      pos[t] = 0;
+      if (slot[t] >= n_kmers) continue;
+      int j = 0;
+#pragma unroll
+      for (int q = 1; q < MR; ++q) j += ko[q] <= slot[t] ? 1 : 0;
+      if (ko[MR] <= slot[t]) {  // beyond the loaded reads: walk on (short reads)
+        I rr = r + MR;
+        while ((I)__ldg(rv.kmer_off + rr + 1) <= slot[t]) ++rr;
+        pos[t] = (I)__ldg(rv.ends + rr - 1) - base + (slot[t] - (I)__ldg(rv.kmer_off + rr));
+      } else {
+        I ko_j = ko[0], st_j = st[0];
+#pragma unroll
+        for (int q = 1; q < MR; ++q)
+          if (q == j) {
+            ko_j = ko[q];
+            st_j = st[q];
+          }
+        pos[t] = st_j + (slot[t] - ko_j);
+      }
+    }
+    // chars and invalid bits of every k-mer of the lane
+    uint64_t w0[PER], w1[PER], inv[PER];
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      const I wi = pos[t] >> 5;
+      const bool in = slot[t] < n_kmers;
+      w0[t] = in ? __ldg(rv.packed + wi) : 0;
+      w1[t] = in ? __ldg(rv.packed + wi + 1) : 0;
+      inv[t] = in ? ((uint64_t)__ldg(rv.invalid + wi) |
+                     ((uint64_t)__ldg(rv.invalid + wi + 1) << 32))
+                  : 0;
+    }
     uint64_t key[PER], z[PER], fw[PER];
     uint32_t state[PER];  // 0 none, 1 invalid, 2 filter
 #pragma unroll
     for (int t = 0; t < PER; ++t) {
-      slot[t] = c0 + (I)t * 32 + lane;
-      state[t] = 0;
+      const uint32_t off = pos[t] & 31;
       key[t] = 0;
-      if (slot[t] >= n_kmers) continue;
-      while ((I)__ldg(rv.kmer_off + r + 1) <= slot[t]) ++r;
-      const I pos = (r ? (I)__ldg(rv.ends + r - 1) : base) - base +
-                    (slot[t] - (I)__ldg(rv.kmer_off + r));
-      // invalid chars in [pos, pos + k): 32-bit words pos >> 5 and the next
-      const I wi = pos >> 5;
-      const uint32_t off = pos & 31;
-      const uint64_t inv = (uint64_t)__ldg(rv.invalid + wi) |
-                           ((uint64_t)__ldg(rv.invalid + wi + 1) << 32);
-      if ((inv >> off) & low_mask(k)) {
-        state[t] = 1;
-        continue;
-      }
-      const uint64_t w0 = __ldg(rv.packed + wi), w1 = __ldg(rv.packed + wi + 1);
-      const uint64_t v = off ? (w0 << (2 * off)) | (w1 >> (64 - 2 * off)) : w0;
-      key[t] = v >> (64 - 2 * k);
-      state[t] = 2;
+      state[t] = slot[t] >= n_kmers ? 0u : (((inv[t] >> off) & low_mask(k)) ? 1u : 2u);
+      const uint64_t v = off ? (w0[t] << (2 * off)) | (w1[t] >> (64 - 2 * off)) : w0[t];
+      if (state[t] == 2) key[t] = v >> (64 - 2 * k);
     }
     // filter words, all issued before any is used
 #pragma unroll

@@ -535,6 +535,8 @@ def parse():
     ap.add_argument("--kernel", type=int, default=-1,
                     help="read search kernel with a k-mer table (sbwt_set_table_kernel): "
                          "0 general, 1 table, 2..5 walks variants, -1 library default")
+    ap.add_argument("--colors-only", action="store_true",
+                    help="run only the colors and serving sections (profiling runs)")
     ap.add_argument("--gather-sweep", action="store_true",
                     help="print the random-sector gather rate against working-set size "
                          "and exit")
@@ -990,7 +992,17 @@ def bench_io(args, S, torch, dev, tmpdir, idx, path, chars, ends, d_out, d_ends,
         t_all = time.perf_counter() - t0
         out_bytes = os.path.getsize(os.path.join(tmpdir, "cli_full.txt")) if r1.returncode == 0 \
             else 0
-        for x in ("full.fq", "cli_full.txt"):
+        try:
+            os.remove(os.path.join(tmpdir, "cli_full.txt"))
+        except OSError:
+            pass
+        # the same with the bool print mode (1 byte per k-mer: less to write)
+        t0 = time.perf_counter()
+        r2 = subprocess.run([str(cli), "index", "-i", path, "-q", full, "-o",
+                             os.path.join(tmpdir, "cli_bool"), "--no-headers", "-p", "bool"],
+                            capture_output=True)
+        t_bool = time.perf_counter() - t0
+        for x in ("full.fq", "cli_bool.bool"):
             try:
                 os.remove(os.path.join(tmpdir, x))
             except OSError:
@@ -1002,7 +1014,10 @@ def bench_io(args, S, torch, dev, tmpdir, idx, path, chars, ends, d_out, d_ends,
             "output_bytes": int(out_bytes), "rc": [r0.returncode, r1.returncode],
             "wall_s": t_all, "index_load_and_start_s": t_load,
             "kmers_per_s_file_to_file": n_kmers / max(t_all - t_load, 1e-9),
-            "kmers_per_s_incl_index_load": n_kmers / t_all}
+            "kmers_per_s_incl_index_load": n_kmers / t_all,
+            "bool_print_mode": {"rc": r2.returncode, "wall_s": t_bool,
+                                "kmers_per_s_file_to_file":
+                                    n_kmers / max(t_bool - t_load, 1e-9)}}
     return out
 
 
@@ -1115,9 +1130,14 @@ def main():
     import sbwt_b200 as S
     torch.cuda.set_device(local)
     dev = local
-    if args.gather_sweep:
+    if args.gather_sweep or args.colors_only:
         if rank == 0:
-            print(json.dumps(gather_sweep(S, dev)), flush=True)
+            if args.gather_sweep:
+                print(json.dumps(gather_sweep(S, dev)), flush=True)
+            else:
+                with tempfile.TemporaryDirectory() as d:
+                    print(json.dumps(bench_colors_and_serving(args, S, torch, dev, d, rank)),
+                          flush=True)
         if pg:
             pg.barrier()
             pg.destroy_process_group()

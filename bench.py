@@ -115,6 +115,7 @@ def bench_batched(args, idx, S, torch, dev, scratch):
     exact = bool(torch.equal(d_out, d_plain))
     S.set_launch_config()
     S.set_table_kernel(args.kernel)
+    S.set_block_threads(256)
     return {"workload": "256 files vs the 100 Mbp index, reads/file log-uniform [50, 1e5] "
                         "(full-size range [1e3, 2e6] scaled 1/20), 10% files of 1-10 kbp "
                         "reads, 5% substitutions", "files": len(files),
@@ -261,12 +262,14 @@ def bench_batched_full(args, idx, S, torch, dev):
             S.set_launch_config(presearch_letters=tune["presearch"],
                                 blocks_per_sm=tune["blocks_per_sm"], tile=tune["tile"])
             S.set_table_kernel(tune["table_kernel"])
+            S.set_block_threads(tune["block_threads"])
         tot["batched_tuned"] += timed(batched)
         exact &= _wave_checksum(torch, d_out, n_k) == ref_ck
         tot["plain_tuned"] += timed(plain)
         exact &= _wave_checksum(torch, d_out, n_k) == ref_ck
         S.set_launch_config()
         S.set_table_kernel(args.kernel)
+        S.set_block_threads(256)
         n_kmers += n_k
         n_chars += int(ends[-1])
         n_reads += len(ends)

@@ -413,7 +413,11 @@ int sbwt_set_table_kernel(int mode);
 /* The process-wide launch configuration (set by sbwt_set_launch_config,
  * sbwt_set_table_kernel, sbwt_autotune); any pointer may be NULL. */
 int sbwt_get_launch_config(uint32_t *presearch_letters, uint32_t *blocks_per_sm,
-                           uint64_t *tile, uint64_t *chunk_chars, int *table_kernel);
+                           uint64_t *tile, uint64_t *chunk_chars, int *table_kernel,
+                           uint32_t *block_threads);
+/* Threads per block of the read search kernels: 128 or 256 (the default;
+ * 0 = the default).  Results never depend on it. */
+int sbwt_set_block_threads(uint32_t threads);
 /* Persisting-L2 access-policy window over the index's rank blocks on the
  * search launches (0 = off, the default; 1 = on: sets this context's
  * persisting-L2 size). */
@@ -430,13 +434,13 @@ int sbwt_measure_random_sectors(int device, uint64_t bytes, int chains,
                                 double *gbs, double *sectors_per_s);
 /* Autotuner: times the read search on the first sample_chars chars of a
  * device-resident batch over a first axis, tile size (k-mers per walk work
- * unit) {auto, 64, 256, 1024} and 256-thread blocks per SM in the grid
- * {2, 3, 4, 6, 8}, checks that every configuration gives the same results,
+ * unit) {auto, 64, 256}, blocks per SM in the grid {2, 4, 6, 8} and threads
+ * per block {128, 256}, checks that every configuration gives the same results,
  * and makes the fastest the process-wide launch configuration.  The first
  * axis is the read search kernel (sbwt_set_table_kernel 1..6: the table
  * kernel, the walks kernel with 1, 2 or 4 walks per lane, the k-mers
  * kernel) when the index has its k-mer table, else the presearch depth (8 up
- * to the index's).
+ * to the index's); the block size (128 or 256 threads) is swept too.
  * sbwt_get_launch_config reads the choice back. */
 int sbwt_autotune(const sbwt_index_t *index, const char *d_chars,
                   uint64_t n_chars, const uint64_t *d_read_ends,

@@ -275,7 +275,8 @@ int sbwt_search_reads_noalloc(const sbwt_index_t *index, const char *d_chars,
 int sbwt_set_launch_config(uint32_t presearch_letters, uint32_t blocks_per_sm,
                            uint64_t tile, uint64_t chunk_chars) {
   LaunchConfig &c = default_launch_config();
-  const uint32_t probe = c.probe_len, l2w = c.l2_window, tk = c.table_kernel;
+  const uint32_t probe = c.probe_len, l2w = c.l2_window, tk = c.table_kernel,
+                 bt = c.block_threads;
   c.presearch_letters = presearch_letters;
   c.blocks_per_sm = blocks_per_sm ? blocks_per_sm : 8;
   c.tile = tile;
@@ -283,14 +284,28 @@ int sbwt_set_launch_config(uint32_t presearch_letters, uint32_t blocks_per_sm,
   c.probe_len = probe;
   c.l2_window = l2w;
   c.table_kernel = tk;
+  c.block_threads = bt;
+  return SBWT_OK;
+}
+
+// Tuning hook: threads per block of the read search kernels (128 or 256,
+// the default; 0 = the default).  Results do not depend on it.
+int sbwt_set_block_threads(uint32_t threads) {
+  if (threads != 0 && threads != 128 && threads != 256) {
+    set_last_error("block threads must be 128 or 256");
+    return SBWT_E_INVALID;
+  }
+  default_launch_config().block_threads = threads ? threads : 256;
   return SBWT_OK;
 }
 
 // The process-wide launch configuration (what sbwt_set_launch_config,
 // sbwt_set_table_kernel and sbwt_autotune set); any pointer may be NULL.
 int sbwt_get_launch_config(uint32_t *presearch_letters, uint32_t *blocks_per_sm,
-                           uint64_t *tile, uint64_t *chunk_chars, int *table_kernel) {
+                           uint64_t *tile, uint64_t *chunk_chars, int *table_kernel,
+                           uint32_t *block_threads) {
   const LaunchConfig &c = default_launch_config();
+  if (block_threads) *block_threads = c.block_threads;
   if (presearch_letters) *presearch_letters = c.presearch_letters;
   if (blocks_per_sm) *blocks_per_sm = c.blocks_per_sm;
   if (tile) *tile = c.tile;

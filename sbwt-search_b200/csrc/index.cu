@@ -2315,7 +2315,7 @@ static uint32_t probe_length(u64 num_bits, u32 k, const LaunchConfig &cfg) {
 
 static u64 tile_size(int device, u64 n_kmers, const LaunchConfig &cfg) {
   if (cfg.tile) return cfg.tile;
-  const u64 resident = (u64)sm_count(device) * cfg.blocks_per_sm * 256;
+  const u64 resident = (u64)sm_count(device) * cfg.blocks_per_sm * cfg.block_threads;
   u64 tile = n_kmers / (resident * 8);
   // at most 128 slots: the tiles in flight then span less of the chars and
   // results (fewer pages and DRAM rows at a time; 10 % faster than 577 on the
@@ -2377,7 +2377,7 @@ static void launch_search(const IndexImpl &ix, u64 n_chars, const u64 *d_ends, u
       sc.kmer_off, n_reads, rv.tile, sc.tile_read);
   SBWT_CUDA(cudaGetLastError());
   note_launches(1);
-  const int threads = 256;
+  const int threads = (int)cfg.block_threads;
   const int grid = grid_for(ix.device, rv.n_tiles, threads, cfg.blocks_per_sm);
   const SbwtView sv = ix.view_for(cfg.presearch_letters);
   const bool stream = !(flags & SBWT_PER_KMER_WALK) && ix.view.suffix_group_starts;
@@ -2438,8 +2438,8 @@ void enqueue_index_step(const IndexImpl &ix, const char *d_chars, u64 n_chars,
   const SbwtView sv = ix.view_for(cfg.presearch_letters);
   const bool stream = !(flags & SBWT_PER_KMER_WALK) && ix.view.suffix_group_starts;
   const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
-  launch_search_kernel(stream, sv, rv, sc.tile_read, mtk, sc.err, grid, 256, st,
-                       LaunchAttrs{}, cfg.table_kernel);
+  launch_search_kernel(stream, sv, rv, sc.tile_read, mtk, sc.err, grid,
+                       (int)cfg.block_threads, st, LaunchAttrs{}, cfg.table_kernel);
   note_launches(1);
 }
 
@@ -2830,13 +2830,14 @@ void IndexImpl::search_reads_noalloc(const char *d_chars, u64 n_chars, const u64
   rv.queue = sc.queue;
   tile_reads_kernel<<<grid_for(device, n_reads, 256, 16), 256, 0, st>>>(sc.kmer_off, n_reads,
                                                                         rv.tile, sc.tile_read);
-  const int grid = grid_for(device, rv.n_tiles, 256, cfg.blocks_per_sm);
+  const int grid = grid_for(device, rv.n_tiles, (int)cfg.block_threads, cfg.blocks_per_sm);
   const SbwtView sv = view_for(cfg.presearch_letters);
   const u32 mtk = (flags & SBWT_MOVE_TO_KEY_KMER) ? 1u : 0u;
   const bool stream = !(flags & SBWT_PER_KMER_WALK) && view.suffix_group_starts;
   // the same kernel choice as sbwt_search_reads, without the profiler
-  launch_search_kernel(stream, sv, rv, sc.tile_read, mtk, sc.err, grid, 256, st,
-                       LaunchAttrs{}, cfg.table_kernel, /*instrument=*/false);
+  launch_search_kernel(stream, sv, rv, sc.tile_read, mtk, sc.err, grid,
+                       (int)cfg.block_threads, st, LaunchAttrs{}, cfg.table_kernel,
+                       /*instrument=*/false);
   SBWT_CUDA(cudaMemcpyAsync(&err, sc.err, 4, cudaMemcpyDeviceToHost, st));
   SBWT_CUDA(cudaStreamSynchronize(st));
   if (err)

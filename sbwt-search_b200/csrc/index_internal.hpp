@@ -24,7 +24,8 @@ constexpr uint32_t kDefaultTableKernel = 7;
 
 struct LaunchConfig {
   uint32_t presearch_letters = 0;  // <= the handle's pyramid depth
-  uint32_t blocks_per_sm = 8;      // 256-thread blocks per SM in the grid
+  uint32_t blocks_per_sm = 8;      // blocks per SM in the grid
+  uint32_t block_threads = 256;    // threads per block of the read search (128 or 256)
   uint64_t tile = 0;               // k-mer slots per work tile
   uint64_t chunk_chars = 0;        // host-pointer path: chars per chunk (when set, also
                                    // the piece size of device-pointer batches)

@@ -858,13 +858,15 @@ int sbwt_autotune(const sbwt_index_t *index, const char *d_chars, uint64_t n_cha
       }
     }
     for (const auto &pm : first) {
-      for (u64 tile : {0ULL, 64ULL, 256ULL, 1024ULL}) {
-        for (u32 bps : {2u, 3u, 4u, 6u, 8u}) {
+      for (u64 tile : {0ULL, 64ULL, 256ULL}) {
+        for (u32 bps : {2u, 4u, 6u, 8u}) {
+         for (u32 bt : {128u, 256u}) {
           LaunchConfig c = saved;
           c.presearch_letters = pm.first;
           c.table_kernel = pm.second;
           c.tile = tile;
-          c.blocks_per_sm = bps;
+          c.blocks_per_sm = bt == 128 ? 2 * bps : bps;  // the same threads per SM
+          c.block_threads = bt;
           default_launch_config() = c;
           u64 n = 0;
           ix.search_reads(d_chars, nc, d_read_ends, nr, out.get<u64>(), nk, &n,
@@ -890,6 +892,7 @@ int sbwt_autotune(const sbwt_index_t *index, const char *d_chars, uint64_t n_cha
             best = ms / 3;
             best_cfg = c;
           }
+         }
         }
       }
     }

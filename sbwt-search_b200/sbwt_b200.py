@@ -103,7 +103,8 @@ def lib():
         L.sbwt_server_wait.argtypes = [vp, u64, C.c_double, C.POINTER(vp), C.POINTER(u64),
                                        C.POINTER(vp), C.POINTER(u64), C.POINTER(vp),
                                        C.POINTER(u64)]
-        L.sbwt_get_launch_config.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_int)]
+        L.sbwt_get_launch_config.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_int), vp]
+        L.sbwt_set_block_threads.argtypes = [u32]
         L.sbwt_server_slots.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(u64), C.POINTER(u64)]
         L.sbwt_server_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                         C.POINTER(u64), C.POINTER(u64), C.POINTER(u64),
@@ -157,6 +158,11 @@ def set_probe_length(probe_len: int = 0) -> None:
 
 
 TABLE_KERNEL_DEFAULT = -1
+
+
+def set_block_threads(threads: int = 256) -> None:
+    """Threads per block of the read search kernels (128 or 256)."""
+    check(lib().sbwt_set_block_threads(int(threads)))
 
 
 def set_table_kernel(mode: int = TABLE_KERNEL_DEFAULT) -> None:
@@ -531,16 +537,17 @@ def autotune(index: SbwtIndex, d_chars, d_read_ends, sample_chars: int = 256 << 
         c = cache[key]
         set_launch_config(c["presearch"], c["blocks_per_sm"], c["tile"], 0)
         set_table_kernel(c.get("table_kernel", TABLE_KERNEL_DEFAULT))
+        set_block_threads(c.get("block_threads", 256))
         return dict(c, cached=True)
     p, b = C.c_uint32(), C.c_uint32()
     t, ms = C.c_uint64(), C.c_double()
     check(lib().sbwt_autotune(index._h, _ptr(d_chars), d_chars.numel(), _ptr(d_read_ends),
                               d_read_ends.numel(), sample_chars, C.byref(p), C.byref(b),
                               C.byref(t), C.byref(ms)))
-    mode = C.c_int()
-    check(lib().sbwt_get_launch_config(None, None, None, None, C.byref(mode)))
+    mode, bt = C.c_int(), C.c_uint32()
+    check(lib().sbwt_get_launch_config(None, None, None, None, C.byref(mode), C.byref(bt)))
     c = {"presearch": p.value, "blocks_per_sm": b.value, "tile": t.value,
-         "table_kernel": mode.value, "sample_ms": ms.value}
+         "table_kernel": mode.value, "block_threads": bt.value, "sample_ms": ms.value}
     if use_cache:
         cache[key] = c
         AUTOTUNE_CACHE.parent.mkdir(parents=True, exist_ok=True)

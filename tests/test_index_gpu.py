@@ -193,6 +193,29 @@ def test_device_batch_in_pieces_matches_one_launch(kernel):
         S.set_launch_config()
 
 
+@pytest.mark.parametrize("kernel", [0, 1, 2, 6, 8])
+def test_128_thread_blocks_match_oracle(kernel):
+    """The read search kernels launched with 128-thread blocks (an autotuner
+    axis): the oracle's results."""
+    g, path, sb = synthetic(41, 3, 5000, 31, 2, 0.02)
+    idx = S.SbwtIndex.open(path)
+    chars, ends = mixed_reads(g, 43, 2000, median=90, sigma=0.8, len_min=0, len_max=500,
+                              sub=0.01, n_rate=0.01)
+    exp = oracle_results(oracle_index(path, 8), chars, ends)
+    S.set_table_kernel(kernel)
+    S.set_block_threads(128)
+    try:
+        for tile in (0, 64):
+            S.set_launch_config(tile=tile)
+            assert np.array_equal(idx.search_reads(chars, ends), exp)
+    finally:
+        S.set_block_threads(256)
+        S.set_table_kernel(DEFAULT_TABLE_KERNEL)
+        S.set_launch_config()
+    with pytest.raises(S.SbwtError):
+        S.set_block_threads(512)
+
+
 def test_errors_are_status_codes():
     with pytest.raises(S.SbwtError) as e:
         S.SbwtIndex.open("/nonexistent/file.sbwt")

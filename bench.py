@@ -540,6 +540,8 @@ def parse():
                          "0 general, 1 table, 2..5 walks variants, -1 library default")
     ap.add_argument("--colors-only", action="store_true",
                     help="run only the colors and serving sections (profiling runs)")
+    ap.add_argument("--cfg1-only", action="store_true",
+                    help="run only the 1 Mbp case (profiling runs)")
     ap.add_argument("--gather-sweep", action="store_true",
                     help="print the random-sector gather rate against working-set size "
                          "and exit")
@@ -1133,10 +1135,14 @@ def main():
     import sbwt_b200 as S
     torch.cuda.set_device(local)
     dev = local
-    if args.gather_sweep or args.colors_only:
+    if args.gather_sweep or args.colors_only or args.cfg1_only:
         if rank == 0:
             if args.gather_sweep:
                 print(json.dumps(gather_sweep(S, dev)), flush=True)
+            elif args.cfg1_only:
+                S.set_table_kernel(args.kernel)
+                with tempfile.TemporaryDirectory() as d:
+                    print(json.dumps(bench_cfg1(args, S, torch, dev, d)), flush=True)
             else:
                 with tempfile.TemporaryDirectory() as d:
                     print(json.dumps(bench_colors_and_serving(args, S, torch, dev, d, rank)),

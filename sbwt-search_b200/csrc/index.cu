@@ -98,11 +98,9 @@ __global__ void pack_kernel(const char *__restrict__ chars, uint64_t n,
   }
 }
 
-// The same packing, 16 chars per thread from one 16-byte load (chars 16-byte
-// aligned): byte-parallel codes and validity (SIMD byte compares), two
-// threads per 64-bit word.  pack_kernel's one 32-byte load per warp
-// iteration left it latency-bound (0.4 TB/s on 1.7 GB of chars); this one
-// streams.
+// The same packing from 16-byte loads (chars 16-byte aligned): byte-parallel
+// codes and validity (SIMD byte compares).  pack_kernel's one 32-byte load
+// per warp iteration left it latency-bound (0.4 TB/s on 1.7 GB of chars).
 __device__ __forceinline__ void pack_4chars(uint32_t x, uint32_t &codes8, uint32_t &inv4) {
   const uint32_t lower = x | 0x20202020u;
   const uint32_t ok = __vcmpeq4(lower, 0x61616161u) | __vcmpeq4(lower, 0x63636363u) |
@@ -114,50 +112,59 @@ __device__ __forceinline__ void pack_4chars(uint32_t x, uint32_t &codes8, uint32
   inv4 = ((bad >> 7) & 1u) | ((bad >> 14) & 2u) | ((bad >> 21) & 4u) | ((bad >> 28) & 8u);
 }
 
+// One 64-bit word (32 chars, two 16-byte loads) per thread and two words per
+// iteration, so four loads are in flight per thread.
+__device__ __forceinline__ void pack_word(const char *__restrict__ chars, uint64_t n,
+                                          uint64_t w, uint64_t &word, uint32_t &inv) {
+  const uint64_t i0 = w * 32;
+  uint32_t x[8];
+  if (i0 + 32 <= n) {
+    const uint4 a = __ldg(reinterpret_cast<const uint4 *>(chars + i0));
+    const uint4 b = __ldg(reinterpret_cast<const uint4 *>(chars + i0 + 16));
+    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+    x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+  } else {  // the last word: chars past n pack as 'A' (code 0, valid)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      x[q] = 0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const uint64_t i = i0 + 4 * q + c;
+        x[q] |= (uint32_t)(i < n ? (uint8_t)chars[i] : (uint8_t)'A') << (8 * c);
+      }
+    }
+  }
+  uint32_t hi = 0, lo = 0;
+  inv = 0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    uint32_t c8, i4;
+    pack_4chars(x[q], c8, i4);
+    if (q < 4)
+      hi |= c8 << (24 - 8 * q);
+    else
+      lo |= c8 << (24 - 8 * (q - 4));
+    inv |= i4 << (4 * q);
+  }
+  word = ((uint64_t)hi << 32) | lo;
+}
+
 __global__ void pack16_kernel(const char *__restrict__ chars, uint64_t n,
                               uint64_t *__restrict__ packed, uint32_t *__restrict__ invalid,
                               uint64_t n_words) {
-  const uint64_t n_chunks = n_words * 2;  // 16 chars each
   const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
-  // grid-stride over pairs of chunks so both threads of a word stay together
-  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < ((n_chunks + 63) & ~63ULL);
-       t += step) {
-    uint32_t codes = 0, inv = 0;
-    if (t < n_chunks) {
-      const uint64_t i0 = t * 16;
-      uint32_t x[4];
-      if (i0 + 16 <= n) {
-        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(chars + i0));
-        x[0] = v.x;
-        x[1] = v.y;
-        x[2] = v.z;
-        x[3] = v.w;
-      } else {  // the last chunk: chars past n pack as 'A' (code 0, valid)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          x[q] = 0;
-#pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            const uint64_t i = i0 + 4 * q + b;
-            x[q] |= (uint32_t)(i < n ? (uint8_t)chars[i] : (uint8_t)'A') << (8 * b);
-          }
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        uint32_t c8, i4;
-        pack_4chars(x[q], c8, i4);
-        codes |= c8 << (24 - 8 * q);
-        inv |= i4 << (4 * q);
-      }
-    }
-    // the odd thread of a word holds its chars 16..31
-    const uint32_t codes_hi = __shfl_down_sync(0xFFFFFFFFu, codes, 1);
-    const uint32_t inv_hi = __shfl_down_sync(0xFFFFFFFFu, inv, 1);
-    if ((t & 1) == 0 && t < n_chunks) {
-      const uint64_t w = t >> 1;
-      packed[w] = ((uint64_t)codes << 32) | codes_hi;
-      invalid[w] = inv | (inv_hi << 16);
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < n_words;
+       w += 2 * step) {
+    const uint64_t w2 = w + step;
+    uint64_t a = 0, b = 0;
+    uint32_t ia = 0, ib = 0;
+    pack_word(chars, n, w, a, ia);
+    if (w2 < n_words) pack_word(chars, n, w2, b, ib);
+    packed[w] = a;
+    invalid[w] = ia;
+    if (w2 < n_words) {
+      packed[w2] = b;
+      invalid[w2] = ib;
     }
   }
 }
@@ -2339,7 +2346,7 @@ static void launch_prepare(int device, u32 k, const char *d_chars, u64 n_chars,
   SBWT_CUDA(cudaMemsetAsync(sc.packed + n_words, 0, 16, st));
   SBWT_CUDA(cudaMemsetAsync(sc.invalid + n_words, 0, 8, st));
   if (n_words && ((uintptr_t)d_chars & 15) == 0)
-    pack16_kernel<<<grid_for(device, n_words * 2, 256, 16), 256, 0, st>>>(
+    pack16_kernel<<<grid_for(device, (n_words + 1) / 2, 256, 8), 256, 0, st>>>(
         d_chars, n_chars, sc.packed, sc.invalid, n_words);
   else if (n_words)
     pack_kernel<<<grid_for(device, n_words * 32, 256, 32), 256, 0, st>>>(

@@ -406,9 +406,10 @@ int sbwt_set_probe_length(uint32_t probe_len);
  *   8, 9 = the walks kernel without the filter and the staged stores, 1 or 2
  *       walks per lane; 10 = the same with 1 walk and the filter in front of
  *       the table, one k-mer at a time; 11, 12 = the k-mers kernel with 2 or
- *       8 k-mers per lane (6 has 4);
+ *       8 k-mers per lane (6 has 4); 13, 14 = 8 and 10 with the staged
+ *       32-byte result stores;
  *   negative = the default.
- * Results never depend on it.  Returns SBWT_E_INVALID above 12. */
+ * Results never depend on it.  Returns SBWT_E_INVALID above 14. */
 int sbwt_set_table_kernel(int mode);
 /* The process-wide launch configuration (set by sbwt_set_launch_config,
  * sbwt_set_table_kernel, sbwt_autotune); any pointer may be NULL. */

@@ -1293,7 +1293,10 @@ __device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_
 // table at once; each result is one 8-byte store), i.e. search_table_kernel's
 // work with W walks per lane.
 // LFILTER (with LEAN): the filter in front of the table, one k-mer at a time.
-template <int W, int MINB, bool COUNT, bool LEAN = false, bool LFILTER = false>
+// LSTAGE (with LEAN): results staged and stored 4 slots per store as in the
+// full walks kernel.
+template <int W, int MINB, bool COUNT, bool LEAN = false, bool LFILTER = false,
+          bool LSTAGE = false>
 __global__ void __launch_bounds__(256, MINB)
     search_walks_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
                         unsigned long long *counters) {
@@ -1356,7 +1359,7 @@ __global__ void __launch_bounds__(256, MINB)
     omask[w] = 0;
   };
   auto emit = [&](int w, I sl, I node) {
-    if (LEAN) {
+    if (LEAN && !LSTAGE) {
       if (sl < out_cap) {
         if (out32)
           __stcs(out32 + sl, (unsigned int)node);
@@ -1894,8 +1897,9 @@ static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStrea
 // k-mers kernel; 7 = 6 when the table and filter are small, else 1; 8, 9 =
 // the walks kernel without filter and staging, 1 or 2 walks per lane; 10 =
 // the same with the filter in front of the table, one k-mer at a time; 11,
-// 12 = the k-mers kernel with 2 or 8 k-mers per lane (6: 4).
-// Results never depend on it.
+// 12 = the k-mers kernel with 2 or 8 k-mers per lane (6: 4); 13, 14 = the
+// lean walks kernel (1 walk) with staged stores, without and with the
+// one-k-mer filter.  Results never depend on it.
 // Whether launch_search_kernel runs the walks kernel (the only one that can
 // write 32-bit results, ReadsView::out32).
 static bool walks_kernel_applies(const SbwtView &sv, const ReadsView &rv, bool stream,
@@ -1971,6 +1975,15 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
       launch_ex(search_walks_kernel<W_, B_, false, true, F_>, grid, threads, st, la, sv,   \
                 rv, tile_read, ctr);                                                       \
   } while (0)
+#define SBWT_LEANS(W_, B_, F_)                                                             \
+  do {                                                                                     \
+    if (ctr)                                                                               \
+      launch_ex(search_walks_kernel<W_, B_, true, true, F_, true>, grid, threads, st, la,  \
+                sv, rv, tile_read, ctr);                                                   \
+    else                                                                                   \
+      launch_ex(search_walks_kernel<W_, B_, false, true, F_, true>, grid, threads, st, la, \
+                sv, rv, tile_read, ctr);                                                   \
+  } while (0)
 #define SBWT_WALKS(W_, B_)                                                                 \
   do {                                                                                     \
     if (ctr)                                                                               \
@@ -1987,6 +2000,8 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
     else if (kernel_mode == 8) SBWT_LEAN(1, 5, false);
     else if (kernel_mode == 9) SBWT_LEAN(2, 3, false);
     else if (kernel_mode == 10) SBWT_LEAN(1, 5, true);
+    else if (kernel_mode == 13) SBWT_LEANS(1, 5, false);
+    else if (kernel_mode == 14) SBWT_LEANS(1, 5, true);
     else if (kernel_mode == 11 && ctr)
       launch_ex(search_kmers_kernel<2, true>, grid, threads, st, la, sv, rv, tile_read, ctr);
     else if (kernel_mode == 11)
@@ -2001,6 +2016,7 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
       launch_ex(search_kmers_kernel<4, false>, grid, threads, st, la, sv, rv, tile_read, ctr);
 #undef SBWT_WALKS
 #undef SBWT_LEAN
+#undef SBWT_LEANS
   } else if (table) {
     if (ctr)
       launch_ex(search_table_kernel<true>, grid, threads, st, la, sv, rv, tile_read, ctr);

@@ -723,7 +723,7 @@ KERNELS = {0: "search_reads_kernel", 1: "search_table_kernel", 2: "search_walks_
            3: "search_walks_kernel", 4: "search_walks_kernel", 5: "search_walks_kernel",
            6: "search_kmers_kernel", 8: "search_walks_kernel", 9: "search_walks_kernel",
            10: "search_walks_kernel", 11: "search_kmers_kernel", 12: "search_kmers_kernel",
-           13: "search_walks_kernel", 14: "search_walks_kernel"}
+           13: "search_walks_kernel", 14: "search_walks_kernel", 15: "search_kmers_seq_kernel"}
 DEFAULT_KERNEL_MODE = 7
 KMERS_KERNEL_MAX_BYTES = 256 << 20  # mode 7 picks the k-mers kernel up to this
 
@@ -741,7 +741,7 @@ def search_kernel_name(idx, mode: int) -> str:
     return KERNELS[mode]
 
 
-FILTER_KERNELS = ("search_walks_kernel", "search_kmers_kernel")
+FILTER_KERNELS = ("search_walks_kernel", "search_kmers_kernel", "search_kmers_seq_kernel")
 
 
 def index_working_sets(idx):

@@ -1830,6 +1830,212 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+template <int PER, bool COUNT>
+__global__ void __launch_bounds__(256)
+    search_kmers_seq_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
+                        unsigned long long *counters) {
+  using I = uint32_t;
+  constexpr I CH = 32 * PER;
+  constexpr int MR = 5;  // reads of a chunk resolved from one round of loads
+  const uint32_t k = s.k;
+  const uint32_t lane = threadIdx.x & 31;
+  const I n_kmers = (I)(rv.n_kmers_dev ? *rv.n_kmers_dev : rv.n_kmers);
+  const I n_reads = (I)rv.n_reads;
+  const I base = (I)rv.base;
+  const I out_cap = (I)min(rv.out_capacity, (uint64_t)~I(0));
+  const I n_chunks = (n_kmers + CH - 1) / CH;
+  const uint64_t warp0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t pol_first = l2_policy_evict_first();
+  uint64_t n_table = 0, n_filter = 0, n_known = 0;
+  // Every phase below issues all its loads before it uses any (no load waits
+  // on a branch over another's value), so one chunk costs about four
+  // round trips: read offsets, chars, filter words, table.  The tile-table
+  // entry of the next chunk is loaded one chunk ahead.
+  I r_next = warp0 < n_chunks ? (I)__ldg(tile_read + (I)warp0 * CH / (I)rv.tile) : 0;
+  for (uint64_t ch = warp0; ch < n_chunks; ch += warps) {
+    const I c0 = (I)ch * CH;
+    I r = r_next;
+    if (ch + warps < n_chunks)
+      r_next = (I)__ldg(tile_read + (I)(ch + warps) * CH / (I)rv.tile);
+    // offsets and ends of reads r .. r + MR - 1 (one round of loads); the
+    // chunk's first read is r itself when the tile size divides the chunk
+    I ko[MR + 1], st[MR];
+    while (true) {
+#pragma unroll
+      for (int j = 0; j <= MR; ++j) ko[j] = (I)__ldg(rv.kmer_off + min(r + j, n_reads));
+#pragma unroll
+      for (int j = 0; j < MR; ++j) {
+        const I rr = min(r + j, n_reads);
+        st[j] = (rr ? (I)__ldg(rv.ends + rr - 1) : base) - base;
+      }
+      if (ko[1] > c0 || r + 1 >= n_reads) break;
+      // forward to the chunk's first read (tiles that do not divide chunks)
+      while (r + 1 < n_reads && (I)__ldg(rv.kmer_off + r + 1) <= c0) ++r;
+    }
+    I slot[PER], pos[PER];
+    // this lane's PER consecutive slots; when they lie in one read their
+    // chars come from one window of three packed words
+    const I s0 = c0 + lane * (I)PER;
+    bool one_read = false;
+    {
+      int j = 0;
+#pragma unroll
+      for (int q = 1; q < MR; ++q) j += ko[q] <= s0 ? 1 : 0;
+      I kend = ko[MR];
+#pragma unroll
+      for (int q = 1; q < MR; ++q)
+        if (q == j + 1) kend = ko[q];
+      one_read = ko[MR] > s0 && s0 + (I)PER <= kend && s0 + (I)PER <= n_kmers;
+    }
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      slot[t] = s0 + (I)t;
+      pos[t] = 0;
+      if (slot[t] >= n_kmers) continue;
+      if (one_read && t > 0) {
+        pos[t] = pos[0] + (I)t;
+        continue;
+      }
+      int j = 0;
+#pragma unroll
+      for (int q = 1; q < MR; ++q) j += ko[q] <= slot[t] ? 1 : 0;
+      if (ko[MR] <= slot[t]) {  // beyond the loaded reads: walk on (short reads)
+        I rr = r + MR;
+        while ((I)__ldg(rv.kmer_off + rr + 1) <= slot[t]) ++rr;
+        pos[t] = (I)__ldg(rv.ends + rr - 1) - base + (slot[t] - (I)__ldg(rv.kmer_off + rr));
+      } else {
+        I ko_j = ko[0], st_j = st[0];
+#pragma unroll
+        for (int q = 1; q < MR; ++q)
+          if (q == j) {
+            ko_j = ko[q];
+            st_j = st[q];
+          }
+        pos[t] = st_j + (slot[t] - ko_j);
+      }
+    }
+    uint64_t key[PER], z[PER], fw[PER];
+    uint32_t state[PER];  // 0 none, 1 invalid, 2 filter
+    if (one_read) {  // one window: words pos0 >> 5 .. + 2
+      const I wi = pos[0] >> 5;
+      const uint64_t p0 = __ldg(rv.packed + wi), p1 = __ldg(rv.packed + wi + 1),
+                     p2 = __ldg(rv.packed + wi + 2);
+      const uint32_t i0 = __ldg(rv.invalid + wi), i1 = __ldg(rv.invalid + wi + 1),
+                     i2 = __ldg(rv.invalid + wi + 2);
+      const uint32_t off0 = pos[0] & 31;
+#pragma unroll
+      for (int t = 0; t < PER; ++t) {
+        const uint32_t o = off0 + t;  // < 32 + PER
+        const bool hi = o >= 32;
+        const uint32_t oo = o & 31;
+        const uint64_t a = hi ? p1 : p0, b = hi ? p2 : p1;
+        const uint64_t iw = hi ? ((uint64_t)i1 | ((uint64_t)i2 << 32))
+                               : ((uint64_t)i0 | ((uint64_t)i1 << 32));
+        const uint64_t v = oo ? (a << (2 * oo)) | (b >> (64 - 2 * oo)) : a;
+        state[t] = ((iw >> oo) & low_mask(k)) ? 1u : 2u;
+        key[t] = state[t] == 2 ? v >> (64 - 2 * k) : 0;
+      }
+    } else {
+      // chars and invalid bits of every k-mer of the lane
+      uint64_t w0[PER], w1[PER], inv[PER];
+#pragma unroll
+      for (int t = 0; t < PER; ++t) {
+        const I wi = pos[t] >> 5;
+        const bool in = slot[t] < n_kmers;
+        w0[t] = in ? __ldg(rv.packed + wi) : 0;
+        w1[t] = in ? __ldg(rv.packed + wi + 1) : 0;
+        inv[t] = in ? ((uint64_t)__ldg(rv.invalid + wi) |
+                       ((uint64_t)__ldg(rv.invalid + wi + 1) << 32))
+                    : 0;
+      }
+#pragma unroll
+      for (int t = 0; t < PER; ++t) {
+        const uint32_t off = pos[t] & 31;
+        key[t] = 0;
+        state[t] = slot[t] >= n_kmers ? 0u : (((inv[t] >> off) & low_mask(k)) ? 1u : 2u);
+        const uint64_t v = off ? (w0[t] << (2 * off)) | (w1[t] >> (64 - 2 * off)) : w0[t];
+        if (state[t] == 2) key[t] = v >> (64 - 2 * k);
+      }
+    }
+    // filter words, all issued before any is used
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      fw[t] = 0;
+      z[t] = 0;
+      if (state[t] == 2) {
+        z[t] = kmer_mix(key[t]);
+        fw[t] = load_u64_nc(s.kmer_filter + kmer_filter_word(z[t], s.filter_words));
+      }
+    }
+    uint64_t res[PER];
+    bool look[PER];
+    I hs[PER];
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      res[t] = state[t] == 1 ? (uint64_t)SBWT_INVALID : (uint64_t)SBWT_NOT_FOUND;
+      const uint64_t bits = kmer_filter_bits(z[t]);
+      look[t] = state[t] == 2 && (fw[t] & bits) == bits;
+      hs[t] = look[t] ? (I)kmer_table_slot(z[t], s.kmer_table_mask) : 0;
+      if (COUNT) {
+        n_filter += state[t] == 2;
+        n_known += state[t] == 1;
+      }
+    }
+    // table probes of the keys the filter passed, one round of loads at a time
+    while (true) {
+      bool any = false;
+      Block A[PER];
+#pragma unroll
+      for (int t = 0; t < PER; ++t) {
+        A[t] = Block{0, 0, 0, 0};
+        if (look[t]) {
+          A[t] = load_block_hint(
+              reinterpret_cast<const Block *>(s.kmer_table + 2 * (uint64_t)hs[t]), pol_first);
+          any = true;
+        }
+      }
+      if (!any) break;
+#pragma unroll
+      for (int t = 0; t < PER; ++t) {
+        if (!look[t]) continue;
+        if (COUNT) ++n_table;
+        if (A[t].w0 == key[t]) {
+          res[t] = A[t].w1;
+          look[t] = false;
+        } else if (A[t].w2 == key[t]) {
+          res[t] = A[t].w3;
+          look[t] = false;
+        } else if (A[t].w0 == ~0ULL || A[t].w2 == ~0ULL) {
+          look[t] = false;  // an empty slot: absent
+        } else {
+          hs[t] = (I)(((uint64_t)hs[t] + 2) & s.kmer_table_mask);
+        }
+      }
+    }
+    if (PER == 4 && !rv.out32 && s0 + 4 <= n_kmers && s0 + 4 <= out_cap &&
+        ((uintptr_t)(rv.out + s0) & 31) == 0) {
+      store_sector_cs(rv.out + s0, res[0], res[1], res[PER > 2 ? 2 : 0], res[PER > 3 ? 3 : 0]);
+    } else {
+#pragma unroll
+      for (int t = 0; t < PER; ++t) {
+        if (slot[t] >= n_kmers || slot[t] >= out_cap) continue;
+        if (rv.out32)
+          __stcs(rv.out32 + slot[t], (unsigned int)res[t]);
+        else
+          __stcs(rv.out + slot[t], (unsigned long long)res[t]);
+      }
+    }
+  }
+  if (COUNT) {
+    atomicAdd(counters + 0, (unsigned long long)n_table);
+    atomicAdd(counters + 3, (unsigned long long)n_filter);
+    atomicAdd(counters + 6, (unsigned long long)n_known);
+    atomicAdd(counters + 9, (unsigned long long)n_filter);   // filter words
+    atomicAdd(counters + 12, (unsigned long long)n_table);   // table lookups
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -1899,7 +2105,8 @@ static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStrea
 // the same with the filter in front of the table, one k-mer at a time; 11,
 // 12 = the k-mers kernel with 2 or 8 k-mers per lane (6: 4); 13, 14 = the
 // lean walks kernel (1 walk) with staged stores, without and with the
-// one-k-mer filter.  Results never depend on it.
+// one-k-mer filter; 15 = the k-mers kernel with consecutive slots per lane.
+// Results never depend on it.
 // Whether launch_search_kernel runs the walks kernel (the only one that can
 // write 32-bit results, ReadsView::out32).
 static bool walks_kernel_applies(const SbwtView &sv, const ReadsView &rv, bool stream,
@@ -2000,6 +2207,12 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
     else if (kernel_mode == 8) SBWT_LEAN(1, 5, false);
     else if (kernel_mode == 9) SBWT_LEAN(2, 3, false);
     else if (kernel_mode == 10) SBWT_LEAN(1, 5, true);
+    else if (kernel_mode == 15 && ctr)
+      launch_ex(search_kmers_seq_kernel<4, true>, grid, threads, st, la, sv, rv, tile_read,
+                ctr);
+    else if (kernel_mode == 15)
+      launch_ex(search_kmers_seq_kernel<4, false>, grid, threads, st, la, sv, rv, tile_read,
+                ctr);
     else if (kernel_mode == 13) SBWT_LEANS(1, 5, false);
     else if (kernel_mode == 14) SBWT_LEANS(1, 5, true);
     else if (kernel_mode == 11 && ctr)

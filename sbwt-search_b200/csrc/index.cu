@@ -1295,15 +1295,18 @@ __device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_
 // LFILTER (with LEAN): the filter in front of the table, one k-mer at a time.
 // LSTAGE (with LEAN): results staged and stored 4 slots per store as in the
 // full walks kernel.
+// G: slots staged per walk before they are stored (4, 8 or 16; 32 bytes per
+// 4 slots per store).
 template <int W, int MINB, bool COUNT, bool LEAN = false, bool LFILTER = false,
-          bool LSTAGE = false>
+          bool LSTAGE = false, int G = 4>
 __global__ void __launch_bounds__(256, MINB)
     search_walks_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
                         unsigned long long *counters) {
   using I = uint32_t;
   constexpr I NONE = ~I(0);
   __shared__ uint32_t sh_cmap[4];
-  __shared__ unsigned long long sh_out[4][W][256];  // staged results, slot & 3 first
+  __shared__ unsigned long long sh_out[G][W][256];  // staged results, slot % G first
+  constexpr uint32_t GFULL = (1u << G) - 1u;
   if (threadIdx.x < 4) sh_cmap[threadIdx.x] = (uint32_t)s.c_map[threadIdx.x];
   __syncthreads();
   const uint32_t k = s.k;
@@ -1338,22 +1341,28 @@ __global__ void __launch_bounds__(256, MINB)
   auto flush = [&](int w) {  // the staged slots of walk w's open group
     const I g = obase[w];
     const uint32_t t = threadIdx.x;
+    const bool full = omask[w] == GFULL && g + G <= out_cap;
     if (out32) {  // 32-bit codes: the value's low word (markers stay markers)
-      if (omask[w] == 15u && vec_out32 && g + 4 <= out_cap) {
-        store_u32x4_cs(out32 + g, (uint32_t)sh_out[0][w][t], (uint32_t)sh_out[1][w][t],
-                       (uint32_t)sh_out[2][w][t], (uint32_t)sh_out[3][w][t]);
+      if (full && vec_out32) {
+#pragma unroll
+        for (int q = 0; q < G; q += 4)
+          store_u32x4_cs(out32 + g + q, (uint32_t)sh_out[q][w][t],
+                         (uint32_t)sh_out[q + 1][w][t], (uint32_t)sh_out[q + 2][w][t],
+                         (uint32_t)sh_out[q + 3][w][t]);
       } else {
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
+        for (int q = 0; q < G; ++q)
           if (((omask[w] >> q) & 1u) && g + q < out_cap)
             __stcs(out32 + g + q, (unsigned int)sh_out[q][w][t]);
       }
-    } else if (omask[w] == 15u && vec_out && g + 4 <= out_cap) {
-      store_sector_cs(rv.out + g, sh_out[0][w][t], sh_out[1][w][t], sh_out[2][w][t],
-                      sh_out[3][w][t]);
+    } else if (full && vec_out) {
+#pragma unroll
+      for (int q = 0; q < G; q += 4)
+        store_sector_cs(rv.out + g + q, sh_out[q][w][t], sh_out[q + 1][w][t],
+                        sh_out[q + 2][w][t], sh_out[q + 3][w][t]);
     } else {
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
+      for (int q = 0; q < G; ++q)
         if (((omask[w] >> q) & 1u) && g + q < out_cap) __stcs(rv.out + g + q, sh_out[q][w][t]);
     }
     omask[w] = 0;
@@ -1369,13 +1378,13 @@ __global__ void __launch_bounds__(256, MINB)
       }
       return;
     }
-    const I g = sl & ~I(3);
+    const I g = sl & ~I(G - 1);
     if (omask[w] && g != obase[w]) flush(w);
     obase[w] = g;
-    sh_out[sl & 3][w][threadIdx.x] =
+    sh_out[sl & (G - 1)][w][threadIdx.x] =
         node == NONE ? (unsigned long long)SBWT_NOT_FOUND : (unsigned long long)node;
-    omask[w] |= 1u << (sl & 3);
-    if (omask[w] == 15u) flush(w);
+    omask[w] |= 1u << (sl & (G - 1));
+    if (omask[w] == GFULL) flush(w);
   };
 
   while (true) {
@@ -2105,7 +2114,8 @@ static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStrea
 // the same with the filter in front of the table, one k-mer at a time; 11,
 // 12 = the k-mers kernel with 2 or 8 k-mers per lane (6: 4); 13, 14 = the
 // lean walks kernel (1 walk) with staged stores, without and with the
-// one-k-mer filter; 15 = the k-mers kernel with consecutive slots per lane.
+// one-k-mer filter; 15 = the k-mers kernel with consecutive slots per lane;
+// 16, 17 = 13 staging 8 or 16 slots per store group.
 // Results never depend on it.
 // Whether launch_search_kernel runs the walks kernel (the only one that can
 // write 32-bit results, ReadsView::out32).
@@ -2191,6 +2201,15 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
       launch_ex(search_walks_kernel<W_, B_, false, true, F_, true>, grid, threads, st, la, \
                 sv, rv, tile_read, ctr);                                                   \
   } while (0)
+#define SBWT_LEANSG(W_, B_, G_)                                                            \
+  do {                                                                                     \
+    if (ctr)                                                                               \
+      launch_ex(search_walks_kernel<W_, B_, true, true, false, true, G_>, grid, threads, st, \
+                la, sv, rv, tile_read, ctr);                                               \
+    else                                                                                   \
+      launch_ex(search_walks_kernel<W_, B_, false, true, false, true, G_>, grid, threads,  \
+                st, la, sv, rv, tile_read, ctr);                                           \
+  } while (0)
 #define SBWT_WALKS(W_, B_)                                                                 \
   do {                                                                                     \
     if (ctr)                                                                               \
@@ -2214,6 +2233,8 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
       launch_ex(search_kmers_seq_kernel<4, false>, grid, threads, st, la, sv, rv, tile_read,
                 ctr);
     else if (kernel_mode == 13) SBWT_LEANS(1, 5, false);
+    else if (kernel_mode == 16) SBWT_LEANSG(1, 5, 8);
+    else if (kernel_mode == 17) SBWT_LEANSG(1, 5, 16);
     else if (kernel_mode == 14) SBWT_LEANS(1, 5, true);
     else if (kernel_mode == 11 && ctr)
       launch_ex(search_kmers_kernel<2, true>, grid, threads, st, la, sv, rv, tile_read, ctr);
@@ -2230,6 +2251,7 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
 #undef SBWT_WALKS
 #undef SBWT_LEAN
 #undef SBWT_LEANS
+#undef SBWT_LEANSG
   } else if (table) {
     if (ctr)
       launch_ex(search_table_kernel<true>, grid, threads, st, la, sv, rv, tile_read, ctr);
@@ -2555,9 +2577,9 @@ static u64 tile_size(int device, u64 n_kmers, const LaunchConfig &cfg) {
   u64 tile = n_kmers / (resident * 8);
   // at most 128 slots: the tiles in flight then span less of the chars and
   // results (fewer pages and DRAM rows at a time; 10 % faster than 577 on the
-  // 100 Mbp workload); a multiple of 4 slots: the walks kernel stores 4
-  // results per 32 bytes
-  return (std::min<u64>(std::max<u64>(tile, 16), 128) + 3) & ~3ULL;
+  // 100 Mbp workload); a multiple of 16 slots: the walks kernels store
+  // groups of up to 16 staged results
+  return (std::min<u64>(std::max<u64>(tile, 16), 128) + 15) & ~15ULL;
 }
 
 // Scan of per-read k-mer counts and the packing of the chars (device-resident

@@ -333,10 +333,11 @@ int sbwt_set_probe_length(uint32_t probe_len) {
 // variants, 6 k-mers kernel, 7 automatic, 8/9/10 lean walks kernel, 11/12
 // k-mers kernel with 2/8 k-mers per lane, 13/14 lean walks kernel with staged
 // stores, 15 k-mers kernel with consecutive slots per lane, 16/17 lean walks
-// kernel staging 8/16 slots, negative = the library default.  Results do not depend on it.
+// kernel staging 8/16 slots, 18 the same with the filter and 16 slots,
+// negative = the library default.  Results do not depend on it.
 int sbwt_set_table_kernel(int mode) {
-  if (mode > 17) {
-    set_last_error("table kernel mode must be 0..17 (or negative for the default)");
+  if (mode > 18) {
+    set_last_error("table kernel mode must be 0..18 (or negative for the default)");
     return SBWT_E_INVALID;
   }
   default_launch_config().table_kernel = mode < 0 ? kDefaultTableKernel : (uint32_t)mode;

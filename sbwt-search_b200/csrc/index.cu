@@ -1273,6 +1273,15 @@ __device__ __forceinline__ uint64_t load_u64_nc(const uint64_t *p) {
   return v;
 }
 
+// load_u64_nc with an L2 eviction policy.
+__device__ __forceinline__ uint64_t load_u64_hint(const uint64_t *p, uint64_t policy) {
+  uint64_t v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u64 %0, [%1], %2;"
+      : "=l"(v)
+      : "l"(p), "l"(policy));
+  return v;
+}
+
 __device__ __forceinline__ void store_u32x4_cs(uint32_t *p, uint32_t a, uint32_t b,
                                                uint32_t c, uint32_t d) {
   asm volatile("st.global.cs.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(a), "r"(b), "r"(c),
@@ -1531,18 +1540,18 @@ __global__ void __launch_bounds__(256, MINB)
                                pol_first);
       } else if (mode[w] == WK_FILTER) {
         uint64_t z = kmer_mix(cw[w].prefix(pos[w], k));
-        A[w].w0 = load_u64_nc(s.kmer_filter + kmer_filter_word(z, s.filter_words));
+        A[w].w0 = load_u64_hint(s.kmer_filter + kmer_filter_word(z, s.filter_words), pol_first);
         if (nb[w] > 1) {
           z = kmer_mix(cw[w].prefix(pos[w] + 1, k));
-          A[w].w1 = load_u64_nc(s.kmer_filter + kmer_filter_word(z, s.filter_words));
+          A[w].w1 = load_u64_hint(s.kmer_filter + kmer_filter_word(z, s.filter_words), pol_first);
         }
         if (nb[w] > 2) {
           z = kmer_mix(cw[w].prefix(pos[w] + 2, k));
-          A[w].w2 = load_u64_nc(s.kmer_filter + kmer_filter_word(z, s.filter_words));
+          A[w].w2 = load_u64_hint(s.kmer_filter + kmer_filter_word(z, s.filter_words), pol_first);
         }
         if (nb[w] > 3) {
           z = kmer_mix(cw[w].prefix(pos[w] + 3, k));
-          A[w].w3 = load_u64_nc(s.kmer_filter + kmer_filter_word(z, s.filter_words));
+          A[w].w3 = load_u64_hint(s.kmer_filter + kmer_filter_word(z, s.filter_words), pol_first);
         }
       }
     }
@@ -2115,7 +2124,7 @@ static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStrea
 // 12 = the k-mers kernel with 2 or 8 k-mers per lane (6: 4); 13, 14 = the
 // lean walks kernel (1 walk) with staged stores, without and with the
 // one-k-mer filter; 15 = the k-mers kernel with consecutive slots per lane;
-// 16, 17 = 13 staging 8 or 16 slots per store group.
+// 16, 17 = 13 staging 8 or 16 slots per store group; 18 = 14 staging 16.
 // Results never depend on it.
 // Whether launch_search_kernel runs the walks kernel (the only one that can
 // write 32-bit results, ReadsView::out32).
@@ -2201,14 +2210,14 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
       launch_ex(search_walks_kernel<W_, B_, false, true, F_, true>, grid, threads, st, la, \
                 sv, rv, tile_read, ctr);                                                   \
   } while (0)
-#define SBWT_LEANSG(W_, B_, G_)                                                            \
+#define SBWT_LEANSG(W_, B_, F_, G_)                                                        \
   do {                                                                                     \
     if (ctr)                                                                               \
-      launch_ex(search_walks_kernel<W_, B_, true, true, false, true, G_>, grid, threads, st, \
+      launch_ex(search_walks_kernel<W_, B_, true, true, F_, true, G_>, grid, threads, st,  \
                 la, sv, rv, tile_read, ctr);                                               \
     else                                                                                   \
-      launch_ex(search_walks_kernel<W_, B_, false, true, false, true, G_>, grid, threads,  \
-                st, la, sv, rv, tile_read, ctr);                                           \
+      launch_ex(search_walks_kernel<W_, B_, false, true, F_, true, G_>, grid, threads, st, \
+                la, sv, rv, tile_read, ctr);                                               \
   } while (0)
 #define SBWT_WALKS(W_, B_)                                                                 \
   do {                                                                                     \
@@ -2233,8 +2242,9 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
       launch_ex(search_kmers_seq_kernel<4, false>, grid, threads, st, la, sv, rv, tile_read,
                 ctr);
     else if (kernel_mode == 13) SBWT_LEANS(1, 5, false);
-    else if (kernel_mode == 16) SBWT_LEANSG(1, 5, 8);
-    else if (kernel_mode == 17) SBWT_LEANSG(1, 5, 16);
+    else if (kernel_mode == 16) SBWT_LEANSG(1, 5, false, 8);
+    else if (kernel_mode == 17) SBWT_LEANSG(1, 5, false, 16);
+    else if (kernel_mode == 18) SBWT_LEANSG(1, 5, true, 16);
     else if (kernel_mode == 14) SBWT_LEANS(1, 5, true);
     else if (kernel_mode == 11 && ctr)
       launch_ex(search_kmers_kernel<2, true>, grid, threads, st, la, sv, rv, tile_read, ctr);

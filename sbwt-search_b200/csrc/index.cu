@@ -1289,6 +1289,11 @@ __device__ __forceinline__ void store_u32x4_cs(uint32_t *p, uint32_t a, uint32_t
                : "memory");
 }
 
+// A 32-bit node of the narrow kernels as a 64-bit result (~0u: not found).
+__device__ __forceinline__ uint64_t widen_node(uint32_t node) {
+  return node == ~0u ? (uint64_t)SBWT_NOT_FOUND : (uint64_t)node;
+}
+
 __device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_t b,
                                                 uint64_t c, uint64_t d) {
   asm volatile("st.global.cs.v4.u64 [%0], {%1,%2,%3,%4};" ::"l"(p), "l"(a), "l"(b), "l"(c),
@@ -1297,7 +1302,8 @@ __device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_
 }
 
 // W walks per lane; MINB = 256-thread blocks per SM the register budget
-// targets (W = 1: 5, W = 2: 4 or 3, W = 4: 2).
+// targets (W = 1: 5, or 6 for the lean staged kernels, which fit 40
+// registers without spills; W = 2: 4 or 3, W = 4: 2).
 // LEAN: no filter and no staging (a walk without a previous node goes to the
 // table at once; each result is one 8-byte store), i.e. search_table_kernel's
 // work with W walks per lane.
@@ -1314,7 +1320,8 @@ __global__ void __launch_bounds__(256, MINB)
   using I = uint32_t;
   constexpr I NONE = ~I(0);
   __shared__ uint32_t sh_cmap[4];
-  __shared__ unsigned long long sh_out[G][W][256];  // staged results, slot % G first
+  // staged results (32-bit nodes, NONE for not found), slot % G first
+  __shared__ uint32_t sh_out[G][W][256];
   constexpr uint32_t GFULL = (1u << G) - 1u;
   if (threadIdx.x < 4) sh_cmap[threadIdx.x] = (uint32_t)s.c_map[threadIdx.x];
   __syncthreads();
@@ -1355,24 +1362,25 @@ __global__ void __launch_bounds__(256, MINB)
       if (full && vec_out32) {
 #pragma unroll
         for (int q = 0; q < G; q += 4)
-          store_u32x4_cs(out32 + g + q, (uint32_t)sh_out[q][w][t],
-                         (uint32_t)sh_out[q + 1][w][t], (uint32_t)sh_out[q + 2][w][t],
-                         (uint32_t)sh_out[q + 3][w][t]);
+          store_u32x4_cs(out32 + g + q, sh_out[q][w][t], sh_out[q + 1][w][t],
+                         sh_out[q + 2][w][t], sh_out[q + 3][w][t]);
       } else {
 #pragma unroll
         for (int q = 0; q < G; ++q)
           if (((omask[w] >> q) & 1u) && g + q < out_cap)
-            __stcs(out32 + g + q, (unsigned int)sh_out[q][w][t]);
+            __stcs(out32 + g + q, sh_out[q][w][t]);
       }
     } else if (full && vec_out) {
 #pragma unroll
       for (int q = 0; q < G; q += 4)
-        store_sector_cs(rv.out + g + q, sh_out[q][w][t], sh_out[q + 1][w][t],
-                        sh_out[q + 2][w][t], sh_out[q + 3][w][t]);
+        store_sector_cs(rv.out + g + q, widen_node(sh_out[q][w][t]),
+                        widen_node(sh_out[q + 1][w][t]), widen_node(sh_out[q + 2][w][t]),
+                        widen_node(sh_out[q + 3][w][t]));
     } else {
 #pragma unroll
       for (int q = 0; q < G; ++q)
-        if (((omask[w] >> q) & 1u) && g + q < out_cap) __stcs(rv.out + g + q, sh_out[q][w][t]);
+        if (((omask[w] >> q) & 1u) && g + q < out_cap)
+          __stcs(rv.out + g + q, (unsigned long long)widen_node(sh_out[q][w][t]));
     }
     omask[w] = 0;
   };
@@ -1390,8 +1398,7 @@ __global__ void __launch_bounds__(256, MINB)
     const I g = sl & ~I(G - 1);
     if (omask[w] && g != obase[w]) flush(w);
     obase[w] = g;
-    sh_out[sl & (G - 1)][w][threadIdx.x] =
-        node == NONE ? (unsigned long long)SBWT_NOT_FOUND : (unsigned long long)node;
+    sh_out[sl & (G - 1)][w][threadIdx.x] = node;
     omask[w] |= 1u << (sl & (G - 1));
     if (omask[w] == GFULL) flush(w);
   };
@@ -2243,8 +2250,8 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
                 ctr);
     else if (kernel_mode == 13) SBWT_LEANS(1, 5, false);
     else if (kernel_mode == 16) SBWT_LEANSG(1, 5, false, 8);
-    else if (kernel_mode == 17) SBWT_LEANSG(1, 5, false, 16);
-    else if (kernel_mode == 18) SBWT_LEANSG(1, 5, true, 16);
+    else if (kernel_mode == 17) SBWT_LEANSG(1, 6, false, 16);
+    else if (kernel_mode == 18) SBWT_LEANSG(1, 6, true, 16);
     else if (kernel_mode == 14) SBWT_LEANS(1, 5, true);
     else if (kernel_mode == 11 && ctr)
       launch_ex(search_kmers_kernel<2, true>, grid, threads, st, la, sv, rv, tile_read, ctr);

@@ -738,7 +738,7 @@ def search_kernel_name(idx, mode: int) -> str:
         return KERNELS[0]
     if mode == 7:
         mode = 6 if 0 < idx.filter_bytes() and table + idx.filter_bytes() <= \
-            KMERS_KERNEL_MAX_BYTES else 1
+            KMERS_KERNEL_MAX_BYTES else 17
     return KERNELS[mode]
 
 

@@ -1302,8 +1302,8 @@ __device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_
 }
 
 // W walks per lane; MINB = 256-thread blocks per SM the register budget
-// targets (W = 1: 5, or 6 for the lean staged kernels, which fit 40
-// registers without spills; W = 2: 4 or 3, W = 4: 2).
+// targets (W = 1: 5, or 6 for the lean 16-slot kernel without the filter,
+// which fits 40 registers without spills; W = 2: 4 or 3, W = 4: 2).
 // LEAN: no filter and no staging (a walk without a previous node goes to the
 // table at once; each result is one 8-byte store), i.e. search_table_kernel's
 // work with W walks per lane.
@@ -2146,13 +2146,17 @@ static bool walks_kernel_applies(const SbwtView &sv, const ReadsView &rv, bool s
 // (automatic, the default) picks it when the table and filter fit
 // kKmersKernelMaxBytes (they then stay in L2 and inside the translation
 // reach, and independent lookups beat the chained stream steps), else the
-// table kernel (a large table: the stream steps' rank blocks are the smaller
-// random working set).
+// lean walks kernel with 16 staged slots per store group (mode 17: a large
+// table, where the stream steps' rank blocks are the smaller random working
+// set, a table lookup costs about what a filter probe does, and the staged
+// 64-byte result stores spare the DRAM the partial writes of the table
+// kernel's 8-byte stores).  Where the walks kernel does not apply, mode 17
+// runs the table kernel.
 constexpr u64 kKmersKernelMaxBytes = 256ULL << 20;
 static uint32_t resolve_kernel_mode(const SbwtView &sv, uint32_t kernel_mode) {
   if (kernel_mode != 7) return kernel_mode;
   const u64 bytes = (sv.kmer_table_mask + 1) * 16 + sv.filter_words * 8;
-  return sv.kmer_table && sv.kmer_filter && bytes <= kKmersKernelMaxBytes ? 6u : 1u;
+  return sv.kmer_table && sv.kmer_filter && bytes <= kKmersKernelMaxBytes ? 6u : 17u;
 }
 
 // instrument = false keeps the launch free of the profiler's events and
@@ -2251,7 +2255,7 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
     else if (kernel_mode == 13) SBWT_LEANS(1, 5, false);
     else if (kernel_mode == 16) SBWT_LEANSG(1, 5, false, 8);
     else if (kernel_mode == 17) SBWT_LEANSG(1, 6, false, 16);
-    else if (kernel_mode == 18) SBWT_LEANSG(1, 6, true, 16);
+    else if (kernel_mode == 18) SBWT_LEANSG(1, 5, true, 16);
     else if (kernel_mode == 14) SBWT_LEANS(1, 5, true);
     else if (kernel_mode == 11 && ctr)
       launch_ex(search_kmers_kernel<2, true>, grid, threads, st, la, sv, rv, tile_read, ctr);

@@ -844,13 +844,14 @@ int sbwt_autotune(const sbwt_index_t *index, const char *d_chars, uint64_t n_cha
     std::vector<u64> h_ref, h_out;
     // With the k-mer table (k <= 31, suffix groups, fewer than 192 * 2^24
     // nodes) the read search never reads the presearch table: the first axis
-    // is then the kernel (table kernel, walks kernel with 1, 2 or 4 walks per
-    // lane at its register budget, k-mers kernel), else the presearch depth.
+    // is then the kernel (table kernel, walks kernel with the filter, k-mers
+    // kernel, lean 16-slot walks kernel without and with the filter), else
+    // the presearch depth.
     const bool table_axis = ix.view.kmer_table && ix.view.suffix_group_starts && ix.k <= 31 &&
                             ix.num_bits < (192ULL << 24);
     std::vector<std::pair<u32, u32>> first;  // (presearch, kernel mode)
     if (table_axis) {
-      for (u32 m : {1u, 2u, 3u, 4u, 5u, 6u}) first.emplace_back(ix.p_max, m);
+      for (u32 m : {1u, 2u, 6u, 17u, 18u}) first.emplace_back(ix.p_max, m);
     } else {
       for (u32 p = ix.p_max; p >= std::min<u32>(8, ix.p_max); --p) {
         first.emplace_back(p, saved.table_kernel);

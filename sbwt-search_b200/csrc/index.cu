@@ -1308,10 +1308,14 @@ __device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_
 // table at once; each result is one 8-byte store), i.e. search_table_kernel's
 // work with W walks per lane.
 // LFILTER (with LEAN): the filter in front of the table, one k-mer at a time.
-// LSTAGE (with LEAN): results staged and stored 4 slots per store as in the
-// full walks kernel.
-// G: slots staged per walk before they are stored (4, 8 or 16; 32 bytes per
-// 4 slots per store).
+// LSTAGE (with LEAN, W = 1): results staged per lane in a shared-memory row
+// of G slots (one group of G consecutive k-mer slots) and stored by the warp
+// together: once per iteration, at a converged point, the lanes whose group
+// is complete or left behind (the walk moved past it or ended) hand their
+// rows to the warp, 32 / G rows per store instruction, each row one run of
+// G consecutive results (G * 8 bytes, a full 128-byte line for G = 16).
+// G: slots staged per walk before they are stored (4, 8 or 16); without
+// LEAN, results leave as 32-byte stores of 4 slots per lane.
 template <int W, int MINB, bool COUNT, bool LEAN = false, bool LFILTER = false,
           bool LSTAGE = false, int G = 4>
 __global__ void __launch_bounds__(256, MINB)
@@ -1320,8 +1324,14 @@ __global__ void __launch_bounds__(256, MINB)
   using I = uint32_t;
   constexpr I NONE = ~I(0);
   __shared__ uint32_t sh_cmap[4];
-  // staged results (32-bit nodes, NONE for not found), slot % G first
-  __shared__ uint32_t sh_out[G][W][256];
+  // staged results (32-bit nodes, NONE for not found): slot % G first for
+  // the per-lane stores; one padded row per lane for the warp's stores (the
+  // odd row stride keeps both the lanes' writes and a row read
+  // conflict-free)
+  constexpr bool COOP = LEAN && LSTAGE;
+  static_assert(!COOP || W == 1, "warp-stored staging takes one walk per lane");
+  __shared__ uint32_t sh_out[COOP ? 1 : G][W][256];
+  __shared__ uint32_t sh_row[COOP ? 256 : 1][G + 1];
   constexpr uint32_t GFULL = (1u << G) - 1u;
   if (threadIdx.x < 4) sh_cmap[threadIdx.x] = (uint32_t)s.c_map[threadIdx.x];
   __syncthreads();
@@ -1355,6 +1365,7 @@ __global__ void __launch_bounds__(256, MINB)
   const uint64_t pol_last = l2_policy_evict_last(), pol_first = l2_policy_evict_first();
 
   auto flush = [&](int w) {  // the staged slots of walk w's open group
+   if constexpr (!COOP) {
     const I g = obase[w];
     const uint32_t t = threadIdx.x;
     const bool full = omask[w] == GFULL && g + G <= out_cap;
@@ -1383,8 +1394,15 @@ __global__ void __launch_bounds__(256, MINB)
           __stcs(rv.out + g + q, (unsigned long long)widen_node(sh_out[q][w][t]));
     }
     omask[w] = 0;
+   }
   };
   auto emit = [&](int w, I sl, I node) {
+    if constexpr (COOP) {  // the group of sl is obase[w] or none is open
+      if (!omask[w]) obase[w] = sl & ~I(G - 1);
+      sh_row[threadIdx.x][sl & (G - 1)] = node;
+      omask[w] |= 1u << (sl & (G - 1));
+      return;
+    } else {
     if (LEAN && !LSTAGE) {
       if (sl < out_cap) {
         if (out32)
@@ -1401,23 +1419,43 @@ __global__ void __launch_bounds__(256, MINB)
     sh_out[sl & (G - 1)][w][threadIdx.x] = node;
     omask[w] |= 1u << (sl & (G - 1));
     if (omask[w] == GFULL) flush(w);
+    }
   };
 
   while (true) {
     // ---- work queue (warp-collective): one tile per walk that needs one
-    uint32_t need = 0;
-#pragma unroll
-    for (int w = 0; w < W; ++w) need += (mode[w] == WK_NEW && slot[w] >= slot_end[w]);
-    uint32_t incl = need;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if ((int)lane >= o) incl += t;
-    }
-    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
     I new_tile[W];
 #pragma unroll
     for (int w = 0; w < W; ++w) new_tile[w] = NONE;
+    if (W == 1) {  // one ballot: lanes in order take consecutive tiles
+      const bool nd = mode[0] == WK_NEW && slot[0] >= slot_end[0];
+      const unsigned nm = __ballot_sync(0xFFFFFFFFu, nd);
+      if (nm) {
+        const int leader = __ffs(nm) - 1;
+        unsigned long long qb = 0;
+        if ((int)lane == leader) qb = atomicAdd(rv.queue, (unsigned long long)__popc(nm));
+        qb = __shfl_sync(0xFFFFFFFFu, qb, leader);
+        if (nd) {
+          const unsigned long long t = qb + __popc(nm & ((1u << lane) - 1u));
+          if (t < (unsigned long long)n_tiles)
+            new_tile[0] = (I)t;
+          else
+            mode[0] = WK_DONE;
+        }
+      }
+    }
+    uint32_t need = 0, incl = 0, total = 0;
+    if (W > 1) {
+#pragma unroll
+      for (int w = 0; w < W; ++w) need += (mode[w] == WK_NEW && slot[w] >= slot_end[w]);
+      incl = need;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if ((int)lane >= o) incl += t;
+      }
+      total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    }
     if (total) {
       unsigned long long qb = 0;
       if (lane == 31) qb = atomicAdd(rv.queue, (unsigned long long)total);
@@ -1526,6 +1564,31 @@ __global__ void __launch_bounds__(256, MINB)
             __stcs(rv.out + q_slot + j, (unsigned long long)SBWT_INVALID);
         }
       }
+    }
+    if (COOP) {  // ---- the warp stores the rows of complete or left groups
+      const bool nf = omask[0] && (mode[0] == WK_DONE || omask[0] == GFULL ||
+                                   (slot[0] & ~I(G - 1)) != obase[0]);
+      constexpr int P = 32 / G;  // rows per store instruction
+      const int sub = (int)lane / G, q = (int)lane % G;
+      for (unsigned fm = __ballot_sync(0xFFFFFFFFu, nf); fm;) {
+        int src = -1;
+#pragma unroll
+        for (int i = 0; i < P; ++i) {  // the sub-th lane left in fm
+          if (i == sub && fm) src = __ffs(fm) - 1;
+          fm &= fm - 1;
+        }
+        const int from = src < 0 ? (int)lane : src;
+        const I gb = __shfl_sync(0xFFFFFFFFu, obase[0], from);
+        const uint32_t gm = __shfl_sync(0xFFFFFFFFu, omask[0], from);
+        if (src >= 0 && ((gm >> q) & 1u) && gb + (I)q < out_cap) {
+          const uint32_t val = sh_row[(threadIdx.x & ~31u) + (unsigned)src][q];
+          if (out32)
+            __stcs(out32 + gb + q, val);
+          else
+            __stcs(rv.out + gb + q, (unsigned long long)widen_node(val));
+        }
+      }
+      if (nf) omask[0] = 0;
     }
     bool all_done = true;
 #pragma unroll
@@ -1660,9 +1723,11 @@ __global__ void __launch_bounds__(256, MINB)
       }
     }
   }
+  if (!COOP) {
 #pragma unroll
-  for (int w = 0; w < W; ++w)
-    if (omask[w]) flush(w);
+    for (int w = 0; w < W; ++w)
+      if (omask[w]) flush(w);
+  }
   if (COUNT) {
     atomicAdd(counters + 0, (unsigned long long)n_table);
     atomicAdd(counters + 1, (unsigned long long)n_block);

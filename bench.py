@@ -1312,9 +1312,13 @@ def main():
         "dtype": "u64", "data": "synthetic (seeded; generated at start-up)",
         "config": index_config(args, world, nodes, n_kmers, n_chars),
         "launch": {"presearch_letters": idx.presearch_letters,
-                   "kernels": "library defaults: the k-mer table kernel (k <= 31), grid of "
-                              "8 x 256-thread blocks per SM (5 resident), tiles of "
-                              "k-mers / (resident threads x 8)"},
+                   "kernel_mode": args.kernel if args.kernel >= 0 else DEFAULT_KERNEL_MODE,
+                   "kernels": f"{kernel}"
+                              + (" (the default, automatic mode 7 picks it for this index)"
+                                 if args.kernel < 0 else f" (mode {args.kernel})")
+                              + ", grid of 8 x 256-thread blocks per SM, tiles of "
+                                "k-mers / (resident threads x 8) rounded up to 16 slots, "
+                                "16 to 128"},
         "gpu_launches": int(launches.value),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,

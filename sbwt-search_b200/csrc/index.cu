@@ -1596,13 +1596,21 @@ __global__ void __launch_bounds__(256, MINB)
     if (__all_sync(0xFFFFFFFFu, all_done)) break;
     // ---- phase 2: the loads of every walk, issued before any is used
     Block A[W];
+    I step_base[W];      // a step's C[c] (its char's first node)
+    uint32_t step_q[W];  // a step's offset of x in its rank block
+    uint64_t fz[W];      // the filter's first k-mer hash
 #pragma unroll
     for (int w = 0; w < W; ++w) {
       A[w] = Block{0, 0, 0, 0};
+      step_base[w] = 0;
+      step_q[w] = 0;
+      fz[w] = 0;
       if (mode[w] == WK_STREAM || mode[w] == WK_STEP) {
         const uint32_t c = cw[w].char_at(pos[w] + k - 1);
-        A[w] = load_block_hint(s.blocks0 + (uint64_t)c * s.block_stride + block_idx(x[w]),
-                               pol_last);
+        const I b = block_idx(x[w]);
+        A[w] = load_block_hint(s.blocks0 + (uint64_t)c * s.block_stride + b, pol_last);
+        step_base[w] = sh_cmap[c];
+        step_q[w] = x[w] - b * kBlockBits;
       } else if (mode[w] == WK_SG) {
         A[w] = load_block_hint(chunk_of(s.suffix_group_starts, (uint64_t)x[w]), pol_last);
       } else if (mode[w] == WK_HASH) {
@@ -1610,6 +1618,7 @@ __global__ void __launch_bounds__(256, MINB)
                                pol_first);
       } else if (mode[w] == WK_FILTER) {
         uint64_t z = kmer_mix(cw[w].prefix(pos[w], k));
+        fz[w] = z;
         A[w].w0 = load_u64_hint(s.kmer_filter + kmer_filter_word(z, s.filter_words), pol_first);
         if (nb[w] > 1) {
           z = kmer_mix(cw[w].prefix(pos[w] + 1, k));
@@ -1651,7 +1660,7 @@ __global__ void __launch_bounds__(256, MINB)
         // k-mers the filter rejects are absent; the first it passes is looked up
         uint32_t j = 0;
         for (; j < nb[w]; ++j) {
-          const uint64_t z = kmer_mix(cw[w].prefix(pos[w], k));
+          const uint64_t z = j == 0 ? fz[w] : kmer_mix(cw[w].prefix(pos[w], k));
           const uint64_t word = j == 0 ? A[w].w0 : (j == 1 ? A[w].w1 : (j == 2 ? A[w].w2 : A[w].w3));
           const uint64_t bits = kmer_filter_bits(z);
           if ((word & bits) == bits) {
@@ -1700,10 +1709,9 @@ __global__ void __launch_bounds__(256, MINB)
           ubit[w] = 63;
         }
       } else {  // a step on [x, x] with the k-mer's last char
-        const uint32_t c = cw[w].char_at(pos[w] + k - 1);
-        const uint32_t q = x[w] - block_idx(x[w]) * kBlockBits;
+        const uint32_t q = step_q[w];
         if (block_bit(A[w], q)) {
-          res = sh_cmap[c] + (I)block_rank(A[w], q);
+          res = step_base[w] + (I)block_rank(A[w], q);
           emitted = true;
         } else if (md == WK_STREAM) {  // no edge at v itself: v's group start
           ubit[w] = x[w] & 63;

@@ -410,9 +410,10 @@ int sbwt_set_probe_length(uint32_t probe_len);
  *       32-byte result stores; 15 = the k-mers kernel with 4 consecutive
  *       k-mer slots per lane (one char window, one 32-byte result store);
  *       16, 17 = 13 with 8 or 16 slots staged per store group; 18 = 14 with
- *       16 slots;
+ *       16 slots; 19 = 6 without the filter (every valid k-mer to the
+ *       table);
  *   negative = the default.
- * Results never depend on it.  Returns SBWT_E_INVALID above 18. */
+ * Results never depend on it.  Returns SBWT_E_INVALID above 19. */
 int sbwt_set_table_kernel(int mode);
 /* The process-wide launch configuration (set by sbwt_set_launch_config,
  * sbwt_set_table_kernel, sbwt_autotune); any pointer may be NULL. */

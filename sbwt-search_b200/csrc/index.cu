@@ -1765,8 +1765,10 @@ __global__ void __launch_bounds__(256, MINB)
 // equal the other kernels' (the table holds exactly the SBWT's k-mers; a
 // filter rejection is exact).  It beats the stream kernels when the table and
 // filter stay in L2 and inside the address-translation reach (small indexes):
-// all loads of a lane are independent.
-template <int PER, bool COUNT>
+// all loads of a lane are independent.  FILT = false skips the filter: every
+// valid k-mer goes to the table (one round trip fewer; for a table that stays
+// in L2 an absent k-mer's probe costs about what its filter word does).
+template <int PER, bool COUNT, bool FILT = true>
 __global__ void __launch_bounds__(256)
     search_kmers_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
                         unsigned long long *counters) {
@@ -1862,7 +1864,7 @@ __global__ void __launch_bounds__(256)
       z[t] = 0;
       if (state[t] == 2) {
         z[t] = kmer_mix(key[t]);
-        fw[t] = load_u64_nc(s.kmer_filter + kmer_filter_word(z[t], s.filter_words));
+        if (FILT) fw[t] = load_u64_nc(s.kmer_filter + kmer_filter_word(z[t], s.filter_words));
       }
     }
     uint64_t res[PER];
@@ -1872,10 +1874,10 @@ __global__ void __launch_bounds__(256)
     for (int t = 0; t < PER; ++t) {
       res[t] = state[t] == 1 ? (uint64_t)SBWT_INVALID : (uint64_t)SBWT_NOT_FOUND;
       const uint64_t bits = kmer_filter_bits(z[t]);
-      look[t] = state[t] == 2 && (fw[t] & bits) == bits;
+      look[t] = state[t] == 2 && (!FILT || (fw[t] & bits) == bits);
       hs[t] = look[t] ? (I)kmer_table_slot(z[t], s.kmer_table_mask) : 0;
       if (COUNT) {
-        n_filter += state[t] == 2;
+        n_filter += FILT && state[t] == 2;
         n_known += state[t] == 1;
       }
     }
@@ -2204,7 +2206,8 @@ static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStrea
 // 12 = the k-mers kernel with 2 or 8 k-mers per lane (6: 4); 13, 14 = the
 // lean walks kernel (1 walk) with staged stores, without and with the
 // one-k-mer filter; 15 = the k-mers kernel with consecutive slots per lane;
-// 16, 17 = 13 staging 8 or 16 slots per store group; 18 = 14 staging 16.
+// 16, 17 = 13 staging 8 or 16 slots per store group; 18 = 14 staging 16;
+// 19 = 6 without the filter.
 // Results never depend on it.
 // Whether launch_search_kernel runs the walks kernel (the only one that can
 // write 32-bit results, ReadsView::out32).
@@ -2334,6 +2337,12 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
       launch_ex(search_kmers_kernel<2, true>, grid, threads, st, la, sv, rv, tile_read, ctr);
     else if (kernel_mode == 11)
       launch_ex(search_kmers_kernel<2, false>, grid, threads, st, la, sv, rv, tile_read, ctr);
+    else if (kernel_mode == 19 && ctr)
+      launch_ex(search_kmers_kernel<4, true, false>, grid, threads, st, la, sv, rv, tile_read,
+                ctr);
+    else if (kernel_mode == 19)
+      launch_ex(search_kmers_kernel<4, false, false>, grid, threads, st, la, sv, rv, tile_read,
+                ctr);
     else if (kernel_mode == 12 && ctr)
       launch_ex(search_kmers_kernel<8, true>, grid, threads, st, la, sv, rv, tile_read, ctr);
     else if (kernel_mode == 12)

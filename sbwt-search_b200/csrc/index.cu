@@ -1317,7 +1317,7 @@ __device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_
 // G: slots staged per walk before they are stored (4, 8 or 16); without
 // LEAN, results leave as 32-byte stores of 4 slots per lane.
 template <int W, int MINB, bool COUNT, bool LEAN = false, bool LFILTER = false,
-          bool LSTAGE = false, int G = 4, bool ONELOAD = false>
+          bool LSTAGE = false, int G = 4>
 __global__ void __launch_bounds__(256, MINB)
     search_walks_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
                         unsigned long long *counters) {
@@ -1605,23 +1605,6 @@ __global__ void __launch_bounds__(256, MINB)
     uint64_t fz[W];      // the filter's first k-mer hash
 #pragma unroll
     for (int w = 0; w < W; ++w) {
-      if (ONELOAD && LEAN && !LFILTER) {
-        // one load per walk: every mode's address computed, one selected
-        // (no branch; lanes without a load leave A unused)
-        const uint32_t md = mode[w];
-        const uint32_t c = cw[w].char_at(pos[w] + k - 1);
-        const I b = block_idx(x[w]);
-        const Block *pr = s.blocks0 + (uint64_t)c * s.block_stride + b;
-        const Block *ps = chunk_of(s.suffix_group_starts, (uint64_t)x[w]);
-        const Block *ph = reinterpret_cast<const Block *>(s.kmer_table + 2 * (uint64_t)hslot[w]);
-        const Block *pa = md == WK_HASH ? ph : (md == WK_SG ? ps : pr);
-        step_base[w] = sh_cmap[c];
-        step_q[w] = x[w] - b * kBlockBits;
-        fz[w] = 0;
-        if (md == WK_STREAM || md == WK_STEP || md == WK_SG || md == WK_HASH)
-          A[w] = load_block_hint(pa, md == WK_HASH ? pol_first : pol_last);
-        continue;
-      }
       A[w] = Block{0, 0, 0, 0};
       step_base[w] = 0;
       step_q[w] = 0;
@@ -2228,8 +2211,7 @@ static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStrea
 // lean walks kernel (1 walk) with staged stores, without and with the
 // one-k-mer filter; 15 = the k-mers kernel with consecutive slots per lane;
 // 16, 17 = 13 staging 8 or 16 slots per store group; 18 = 14 staging 16;
-// 19 = 6 without the filter; 20, 21 = 17 with 2 walks per lane; 22 = 17 with
-// one selected load per walk.
+// 19 = 6 without the filter.
 // Results never depend on it.
 // Whether launch_search_kernel runs the walks kernel (the only one that can
 // write 32-bit results, ReadsView::out32).
@@ -2328,15 +2310,6 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
       launch_ex(search_walks_kernel<W_, B_, false, true, F_, true, G_>, grid, threads, st, \
                 la, sv, rv, tile_read, ctr);                                               \
   } while (0)
-#define SBWT_LEANSG1(W_, B_, G_)                                                           \
-  do {                                                                                     \
-    if (ctr)                                                                               \
-      launch_ex(search_walks_kernel<W_, B_, true, true, false, true, G_, true>, grid,      \
-                threads, st, la, sv, rv, tile_read, ctr);                                  \
-    else                                                                                   \
-      launch_ex(search_walks_kernel<W_, B_, false, true, false, true, G_, true>, grid,     \
-                threads, st, la, sv, rv, tile_read, ctr);                                  \
-  } while (0)
 #define SBWT_WALKS(W_, B_)                                                                 \
   do {                                                                                     \
     if (ctr)                                                                               \
@@ -2363,9 +2336,6 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
     else if (kernel_mode == 16) SBWT_LEANSG(1, 5, false, 8);
     else if (kernel_mode == 17) SBWT_LEANSG(1, 6, false, 16);
     else if (kernel_mode == 18) SBWT_LEANSG(1, 5, true, 16);
-    else if (kernel_mode == 20) SBWT_LEANSG(2, 4, false, 16);
-    else if (kernel_mode == 21) SBWT_LEANSG(2, 3, false, 16);
-    else if (kernel_mode == 22) SBWT_LEANSG1(1, 5, 16);
     else if (kernel_mode == 14) SBWT_LEANS(1, 5, true);
     else if (kernel_mode == 11 && ctr)
       launch_ex(search_kmers_kernel<2, true>, grid, threads, st, la, sv, rv, tile_read, ctr);
@@ -2389,7 +2359,6 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
 #undef SBWT_LEAN
 #undef SBWT_LEANS
 #undef SBWT_LEANSG
-#undef SBWT_LEANSG1
   } else if (table) {
     if (ctr)
       launch_ex(search_table_kernel<true>, grid, threads, st, la, sv, rv, tile_read, ctr);

@@ -2558,7 +2558,7 @@ struct Workspace {
   cudaStream_t streams[2] = {nullptr, nullptr};
   DeviceBuffer chars[2], ends[2], kmer_off[2], packed[2], invalid[2], results[2],
       block_sums[2], total[2], tile_read[2], queue[2], positions, bits, results32[2];
-  uint32_t *err_host = nullptr;  // pinned
+  uint32_t *err_host = nullptr;  // pinned: the error word, then (at +8 bytes) a k-mer count
   DeviceBuffer err_dev;
   cudaEvent_t done[2] = {nullptr, nullptr};
   uint32_t *stage[2] = {nullptr, nullptr};  // pinned: 32-bit results of a chunk
@@ -2634,7 +2634,7 @@ static Workspace &workspace(int device) {
     for (auto &s : p->streams)
       SBWT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     for (auto &e : p->done) SBWT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    SBWT_CUDA(cudaMallocHost(&p->err_host, sizeof(uint32_t)));
+    SBWT_CUDA(cudaMallocHost(&p->err_host, 16));
     p->err_dev.resize(sizeof(uint32_t));
     SBWT_CUDA(cudaMemset(p->err_dev.get(), 0, sizeof(uint32_t)));
   }
@@ -2919,9 +2919,12 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
       // k-mers <= chars, so a tile table sized for n_chars is always enough
       const ReadsScratch sc = scratch_for(ws, 0, n_chars, n_reads, n_chars, 16);
       launch_prepare(device, k, chars, n_chars, read_ends, n_reads, 0, sc, user_stream);
-      SBWT_CUDA(cudaMemcpyAsync(&n_k, sc.total, 8, cudaMemcpyDeviceToHost, user_stream));
-      SBWT_CUDA(cudaStreamSynchronize(user_stream));
+      // the count and the error word come back under one synchronisation
+      // (check_err_word's); the search runs only on a clean scan
+      u64 *const total_host = reinterpret_cast<u64 *>(ws.err_host + 2);
+      SBWT_CUDA(cudaMemcpyAsync(total_host, sc.total, 8, cudaMemcpyDeviceToHost, user_stream));
       check_err_word(ws, user_stream);
+      n_k = *total_host;
       if (n_results) *n_results = n_k;
       if (n_k > capacity)
         throw Error(SBWT_E_CAPACITY, "results_capacity smaller than the k-mer count");

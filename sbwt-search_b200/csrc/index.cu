@@ -2201,10 +2201,37 @@ static void launch_ex(void (*kernel)(KArgs...), int grid, int threads, cudaStrea
   SBWT_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
 }
 
+static int sm_count(int dev);
+
+// launch_ex with the grid capped at one wave of resident blocks: for kernels
+// that split their work statically over the grid (the k-mers kernels), a
+// partial last wave would leave most SMs idle at the end.
+template <typename... KArgs, typename... Args>
+static void launch_one_wave(void (*kernel)(KArgs...), int grid, int threads, cudaStream_t st,
+                            const LaunchAttrs &la, Args... args) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, int> per_sm;  // resident blocks per SM
+  int nb = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = per_sm.find({(const void *)kernel, threads});
+    if (it != per_sm.end()) {
+      nb = it->second;
+    } else {
+      SBWT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, 0));
+      per_sm[{(const void *)kernel, threads}] = nb;
+    }
+  }
+  int dev = 0;
+  SBWT_CUDA(cudaGetDevice(&dev));
+  const int wave = std::max(1, nb) * sm_count(dev);
+  launch_ex(kernel, std::min(grid, wave), threads, st, la, args...);
+}
+
 // kernel_mode: 0 = the general kernel; 1 = the table kernel; 2..5 = the
 // walks kernel with (walks per lane, blocks per SM) = (1, 5), (2, 4), (2, 3),
 // (4, 2) (the table kernel when the index has no k-mer filter); 6 = the
-// k-mers kernel; 7 = 6 when the table and filter are small, else 1; 8, 9 =
+// k-mers kernel; 7 = 6 when the table and filter are small, else 17; 8, 9 =
 // the walks kernel without filter and staging, 1 or 2 walks per lane; 10 =
 // the same with the filter in front of the table, one k-mer at a time; 11,
 // 12 = the k-mers kernel with 2 or 8 k-mers per lane (6: 4); 13, 14 = the
@@ -2327,34 +2354,40 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
     else if (kernel_mode == 9) SBWT_LEAN(2, 3, false);
     else if (kernel_mode == 10) SBWT_LEAN(1, 5, true);
     else if (kernel_mode == 15 && ctr)
-      launch_ex(search_kmers_seq_kernel<4, true>, grid, threads, st, la, sv, rv, tile_read,
-                ctr);
+      launch_one_wave(search_kmers_seq_kernel<4, true>,
+                      grid, threads, st, la, sv, rv, tile_read, ctr);
     else if (kernel_mode == 15)
-      launch_ex(search_kmers_seq_kernel<4, false>, grid, threads, st, la, sv, rv, tile_read,
-                ctr);
+      launch_one_wave(search_kmers_seq_kernel<4, false>,
+                      grid, threads, st, la, sv, rv, tile_read, ctr);
     else if (kernel_mode == 13) SBWT_LEANS(1, 5, false);
     else if (kernel_mode == 16) SBWT_LEANSG(1, 5, false, 8);
     else if (kernel_mode == 17) SBWT_LEANSG(1, 6, false, 16);
     else if (kernel_mode == 18) SBWT_LEANSG(1, 5, true, 16);
     else if (kernel_mode == 14) SBWT_LEANS(1, 5, true);
     else if (kernel_mode == 11 && ctr)
-      launch_ex(search_kmers_kernel<2, true>, grid, threads, st, la, sv, rv, tile_read, ctr);
+      launch_one_wave(search_kmers_kernel<2, true>,
+                      grid, threads, st, la, sv, rv, tile_read, ctr);
     else if (kernel_mode == 11)
-      launch_ex(search_kmers_kernel<2, false>, grid, threads, st, la, sv, rv, tile_read, ctr);
+      launch_one_wave(search_kmers_kernel<2, false>,
+                      grid, threads, st, la, sv, rv, tile_read, ctr);
     else if (kernel_mode == 19 && ctr)
-      launch_ex(search_kmers_kernel<4, true, false>, grid, threads, st, la, sv, rv, tile_read,
-                ctr);
+      launch_one_wave(search_kmers_kernel<4, true, false>,
+                      grid, threads, st, la, sv, rv, tile_read, ctr);
     else if (kernel_mode == 19)
-      launch_ex(search_kmers_kernel<4, false, false>, grid, threads, st, la, sv, rv, tile_read,
-                ctr);
+      launch_one_wave(search_kmers_kernel<4, false, false>,
+                      grid, threads, st, la, sv, rv, tile_read, ctr);
     else if (kernel_mode == 12 && ctr)
-      launch_ex(search_kmers_kernel<8, true>, grid, threads, st, la, sv, rv, tile_read, ctr);
+      launch_one_wave(search_kmers_kernel<8, true>,
+                      grid, threads, st, la, sv, rv, tile_read, ctr);
     else if (kernel_mode == 12)
-      launch_ex(search_kmers_kernel<8, false>, grid, threads, st, la, sv, rv, tile_read, ctr);
+      launch_one_wave(search_kmers_kernel<8, false>,
+                      grid, threads, st, la, sv, rv, tile_read, ctr);
     else if (ctr)
-      launch_ex(search_kmers_kernel<4, true>, grid, threads, st, la, sv, rv, tile_read, ctr);
+      launch_one_wave(search_kmers_kernel<4, true>,
+                      grid, threads, st, la, sv, rv, tile_read, ctr);
     else
-      launch_ex(search_kmers_kernel<4, false>, grid, threads, st, la, sv, rv, tile_read, ctr);
+      launch_one_wave(search_kmers_kernel<4, false>,
+                      grid, threads, st, la, sv, rv, tile_read, ctr);
 #undef SBWT_WALKS
 #undef SBWT_LEAN
 #undef SBWT_LEANS

@@ -22,6 +22,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -738,7 +739,7 @@ def search_kernel_name(idx, mode: int) -> str:
     if not table:
         return KERNELS[0]
     if mode == 7:
-        mode = 6 if 0 < idx.filter_bytes() and table + idx.filter_bytes() <= \
+        mode = 11 if 0 < idx.filter_bytes() and table + idx.filter_bytes() <= \
             KMERS_KERNEL_MAX_BYTES else 17
     return KERNELS[mode]
 
@@ -761,16 +762,38 @@ def index_working_sets(idx):
     return hot, (4 ** idx.presearch_letters) * entry, 0
 
 
-def sector_roofline(S, dev, idx, n_hot, n_pre, kernel_s, n_filter=0):
+def sector_roofline(S, dev, idx, n_hot, n_pre, kernel_s, n_filter=0, cold=False):
     """Random-sector roofline of the read search: the time the kernel's
     sectors take at the measured random-gather rate of their own working set
     (rank blocks + group words; the k-mer table or presearch level; the
-    k-mer filter), over the kernel time."""
+    k-mer filter), over the kernel time.  The rates are those of a warm L2
+    (the microbenchmark repeats its gathers over one buffer).  cold=True
+    (L2 flushed before the timed launch) adds `cold_l2`: each class's
+    expected distinct sectors, S * (1 - exp(-n / S)) for n uniform random
+    loads over S sectors, are first touches served by DRAM at the measured
+    rate of a 2 GiB buffer; the rest at the class's warm rate."""
     hot_b, pre_b, filt_b = index_working_sets(idx)
     r_hot = random_sector_peak(S, dev, hot_b)
     r_pre = random_sector_peak(S, dev, pre_b)
     r_filt = random_sector_peak(S, dev, filt_b) if (filt_b and n_filter) else 0.0
     t_min = n_hot / r_hot + n_pre / r_pre + (n_filter / r_filt if r_filt else 0.0)
+    cold_l2 = None
+    if cold:
+        r_dram = random_sector_peak(S, dev, 2 << 30)
+        t_cold, first = 0.0, {}
+        for name, n, ws, r in (("hot", n_hot, hot_b, r_hot), ("lookup", n_pre, pre_b, r_pre),
+                               ("filter", n_filter, filt_b, r_filt)):
+            if not n or not r:
+                continue
+            secs = max(1.0, ws / 32)
+            d = secs * -math.expm1(-n / secs)
+            first[name] = int(d)
+            t_cold += d / r_dram + (n - d) / r
+        cold_l2 = {"frac": t_cold / kernel_s, "t_min_ms": t_cold * 1e3,
+                   "dram_peak_gsectors_s": r_dram / 1e9, "first_touch_sectors": first,
+                   "model": "L2 flushed before the launch: a sector's first touch comes "
+                            "from DRAM (random-sector rate of a 2 GiB buffer), later "
+                            "touches at the working set's warm rate"}
     out = {"frac": t_min / kernel_s, "t_min_ms": t_min * 1e3, "kernel_ms": kernel_s * 1e3,
            "achieved_gsectors_s": (n_hot + n_pre + n_filter) / kernel_s / 1e9,
            "hot": {"sectors": int(n_hot), "working_set_bytes": int(hot_b),
@@ -782,6 +805,8 @@ def sector_roofline(S, dev, idx, n_hot, n_pre, kernel_s, n_filter=0):
     if n_filter:
         out["filter"] = {"sectors": int(n_filter), "working_set_bytes": int(filt_b),
                          "peak_gsectors_s": r_filt / 1e9}
+    if cold_l2 is not None:
+        out["cold_l2"] = cold_l2
     return out
 
 
@@ -843,7 +868,7 @@ def bench_cfg1(args, S, torch, dev, tmpdir):
            "l2": "flushed (256 MB write) before every timed step",
            "kernel": kernel,
            "random_sector": dict(sector_roofline(S, dev, idx, int(ctr[1]) + int(ctr[2]),
-                                                 int(ctr[0]), kern_s, n_filter),
+                                                 int(ctr[0]), kern_s, n_filter, cold=True),
                                  sectors_per_kmer=sectors / nk)}
     r = cpu_reference_rate(path, chars, ends, 31, len(ends))
     if r is not None:

@@ -401,7 +401,7 @@ int sbwt_set_probe_length(uint32_t probe_len);
  *       (2, 3), (4, 2);
  *   6 = the k-mers kernel (every k-mer on its own: filter, then table; no
  *       stream steps, all loads of a lane independent);
- *   7 = automatic, the default: 6 when the table and filter take at most
+ *   7 = automatic, the default: 11 when the table and filter take at most
  *       256 MiB, else 17;
  *   8, 9 = the walks kernel without the filter and the staged stores, 1 or 2
  *       walks per lane; 10 = the same with 1 walk and the filter in front of

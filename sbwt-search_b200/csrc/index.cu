@@ -2231,7 +2231,7 @@ static void launch_one_wave(void (*kernel)(KArgs...), int grid, int threads, cud
 // kernel_mode: 0 = the general kernel; 1 = the table kernel; 2..5 = the
 // walks kernel with (walks per lane, blocks per SM) = (1, 5), (2, 4), (2, 3),
 // (4, 2) (the table kernel when the index has no k-mer filter); 6 = the
-// k-mers kernel; 7 = 6 when the table and filter are small, else 17; 8, 9 =
+// k-mers kernel; 7 = 11 when the table and filter are small, else 17; 8, 9 =
 // the walks kernel without filter and staging, 1 or 2 walks per lane; 10 =
 // the same with the filter in front of the table, one k-mer at a time; 11,
 // 12 = the k-mers kernel with 2 or 8 k-mers per lane (6: 4); 13, 14 = the
@@ -2249,10 +2249,12 @@ static bool walks_kernel_applies(const SbwtView &sv, const ReadsView &rv, bool s
          sv.k <= 31 && mtk == 0 && sv.suffix_group_starts;
 }
 
-// The k-mers kernel (mode 6) has the walks kernel's conditions.  Mode 7
-// (automatic, the default) picks it when the table and filter fit
-// kKmersKernelMaxBytes (they then stay in L2 and inside the translation
-// reach, and independent lookups beat the chained stream steps), else the
+// The k-mers kernel (modes 6, 11) has the walks kernel's conditions.  Mode 7
+// (automatic, the default) picks it, with 2 k-mers per lane (mode 11: 51
+// registers, 5 blocks per SM; faster than 4 per lane at 3 blocks), when the
+// table and filter fit kKmersKernelMaxBytes (they then stay in L2 and inside
+// the translation reach, and independent lookups beat the chained stream
+// steps), else the
 // lean walks kernel with 16 staged slots per store group (mode 17: a large
 // table, where the stream steps' rank blocks are the smaller random working
 // set, a table lookup costs about what a filter probe does, and the staged
@@ -2263,7 +2265,7 @@ constexpr u64 kKmersKernelMaxBytes = 256ULL << 20;
 static uint32_t resolve_kernel_mode(const SbwtView &sv, uint32_t kernel_mode) {
   if (kernel_mode != 7) return kernel_mode;
   const u64 bytes = (sv.kmer_table_mask + 1) * 16 + sv.filter_words * 8;
-  return sv.kmer_table && sv.kmer_filter && bytes <= kKmersKernelMaxBytes ? 6u : 17u;
+  return sv.kmer_table && sv.kmer_filter && bytes <= kKmersKernelMaxBytes ? 11u : 17u;
 }
 
 // instrument = false keeps the launch free of the profiler's events and

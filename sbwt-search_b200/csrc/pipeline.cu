@@ -845,13 +845,14 @@ int sbwt_autotune(const sbwt_index_t *index, const char *d_chars, uint64_t n_cha
     // With the k-mer table (k <= 31, suffix groups, fewer than 192 * 2^24
     // nodes) the read search never reads the presearch table: the first axis
     // is then the kernel (table kernel, walks kernel with the filter, k-mers
-    // kernel, lean 16-slot walks kernel without and with the filter), else
+    // kernel with 4 and 2 k-mers per lane, lean 16-slot walks kernel without
+    // and with the filter), else
     // the presearch depth.
     const bool table_axis = ix.view.kmer_table && ix.view.suffix_group_starts && ix.k <= 31 &&
                             ix.num_bits < (192ULL << 24);
     std::vector<std::pair<u32, u32>> first;  // (presearch, kernel mode)
     if (table_axis) {
-      for (u32 m : {1u, 2u, 6u, 17u, 18u}) first.emplace_back(ix.p_max, m);
+      for (u32 m : {1u, 2u, 6u, 11u, 17u, 18u}) first.emplace_back(ix.p_max, m);
     } else {
       for (u32 p = ix.p_max; p >= std::min<u32>(8, ix.p_max); --p) {
         first.emplace_back(p, saved.table_kernel);

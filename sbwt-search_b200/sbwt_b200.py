@@ -168,7 +168,7 @@ def set_block_threads(threads: int = 256) -> None:
 def set_table_kernel(mode: int = TABLE_KERNEL_DEFAULT) -> None:
     """Read search kernel of an index with a k-mer table: 0 general, 1 table
     (True), 2..5 walks kernel with (walks per lane, blocks per SM) = (1, 5),
-    (2, 4), (2, 3), (4, 2), 6 k-mers kernel, 7 automatic (6 for small
+    (2, 4), (2, 3), (4, 2), 6 k-mers kernel, 7 automatic (11 for small
     tables, else 17), 8/9 walks kernel without filter and staging (1/2
     walks), 10 the same with 1 walk and a one-k-mer filter, 11/12 k-mers
     kernel with 2/8 k-mers per lane, 13/14 = 8/10 with staged stores,

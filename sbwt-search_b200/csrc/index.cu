@@ -226,8 +226,11 @@ __global__ void scan_reduce_kernel(const uint64_t *ends, uint64_t n_reads,
   if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
 }
 
+// A batch whose read ends failed the check (err bit 4) gets a total of 0 and
+// all-zero k-mer offsets: the launches queued after the scan then do nothing
+// (no host round trip is needed before them).
 __global__ void scan_sums_kernel(uint64_t *block_sums, uint64_t n_blocks,
-                                 uint64_t *grand_total) {
+                                 uint64_t *grand_total, const uint32_t *err) {
   __shared__ uint64_t carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
@@ -241,13 +244,21 @@ __global__ void scan_sums_kernel(uint64_t *block_sums, uint64_t n_blocks,
     if (threadIdx.x == 0) carry += total;
     __syncthreads();
   }
-  if (threadIdx.x == 0) *grand_total = carry;
+  if (threadIdx.x == 0) *grand_total = (*err & 4u) ? 0 : carry;
 }
 
 __global__ void scan_write_kernel(const uint64_t *ends, uint64_t n_reads,
                                   uint64_t base, uint32_t k,
-                                  const uint64_t *block_sums, uint64_t *kmer_off) {
+                                  const uint64_t *block_sums, uint64_t *kmer_off,
+                                  const uint32_t *err) {
   const uint64_t t0 = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  if (*err & 4u) {  // the same word for every thread: a uniform return
+    for (int i = 0; i < kScanItems; ++i) {
+      if (t0 + i < n_reads) kmer_off[t0 + i] = 0;
+      if (t0 + i == n_reads - 1) kmer_off[n_reads] = 0;
+    }
+    return;
+  }
   uint64_t v[kScanItems];
   uint64_t s = 0;
   for (int i = 0; i < kScanItems; ++i) {
@@ -2733,9 +2744,10 @@ static void launch_prepare(int device, u32 k, const char *d_chars, u64 n_chars,
   const u64 n_scan_blocks = (n_reads + kScanTile - 1) / kScanTile;
   scan_reduce_kernel<<<(unsigned)n_scan_blocks, kScanThreads, 0, st>>>(
       d_ends, n_reads, base, k, n_chars, sc.block_sums, sc.err);
-  scan_sums_kernel<<<1, kScanThreads, 0, st>>>(sc.block_sums, n_scan_blocks, sc.total);
+  scan_sums_kernel<<<1, kScanThreads, 0, st>>>(sc.block_sums, n_scan_blocks, sc.total,
+                                               sc.err);
   scan_write_kernel<<<(unsigned)n_scan_blocks, kScanThreads, 0, st>>>(
-      d_ends, n_reads, base, k, sc.block_sums, sc.kmer_off);
+      d_ends, n_reads, base, k, sc.block_sums, sc.kmer_off, sc.err);
   SBWT_CUDA(cudaMemsetAsync(sc.packed + n_words, 0, 16, st));
   SBWT_CUDA(cudaMemsetAsync(sc.invalid + n_words, 0, 8, st));
   if (n_words && ((uintptr_t)d_chars & 15) == 0)
@@ -2749,11 +2761,14 @@ static void launch_prepare(int device, u32 k, const char *d_chars, u64 n_chars,
 }
 
 // Tile table + the read search kernel over a prepared batch of n_kmers.
+// With d_total the kernels read the k-mer count from device memory (the
+// scan's total) and n_kmers is only an upper bound, for the tiling.
 static void launch_search(const IndexImpl &ix, u64 n_chars, const u64 *d_ends, u64 n_reads,
                           u64 base,
                           u64 n_kmers, u64 *d_out, u64 out_capacity, u32 flags,
                           const LaunchConfig &cfg, const ReadsScratch &sc,
-                          cudaStream_t st, uint32_t *d_out32 = nullptr) {
+                          cudaStream_t st, uint32_t *d_out32 = nullptr,
+                          const u64 *d_total = nullptr) {
   if (n_reads == 0 || n_kmers == 0) return;
   ReadsView rv{};
   rv.out32 = d_out32;
@@ -2770,7 +2785,7 @@ static void launch_search(const IndexImpl &ix, u64 n_chars, const u64 *d_ends, u
   rv.out = d_out;
   rv.out_capacity = out_capacity;
   rv.probe_len = probe_length(ix.num_bits, ix.k, cfg);
-  rv.n_kmers_dev = nullptr;
+  rv.n_kmers_dev = d_total;
   rv.queue = sc.queue;
   SBWT_CUDA(cudaMemsetAsync(sc.queue, 0, 8, st));
   tile_reads_kernel<<<grid_for(ix.device, n_reads, 256, 16), 256, 0, st>>>(
@@ -2953,9 +2968,14 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
     if (n_reads) {
       // k-mers <= chars, so a tile table sized for n_chars is always enough
       const ReadsScratch sc = scratch_for(ws, 0, n_chars, n_reads, n_chars, 16);
+      // scan, packing, tile table and search queued back to back: the search
+      // reads the k-mer count from the scan's total (a batch with bad read
+      // ends has a total of 0), tiles are sized for n_chars (>= the count),
+      // and no kernel writes at or past `capacity`.  The count and the error
+      // word come back under one synchronisation (check_err_word's).
       launch_prepare(device, k, chars, n_chars, read_ends, n_reads, 0, sc, user_stream);
-      // the count and the error word come back under one synchronisation
-      // (check_err_word's); the search runs only on a clean scan
+      launch_search(*this, n_chars, read_ends, n_reads, 0, n_chars, results, capacity, flags,
+                    cfg, sc, user_stream, nullptr, sc.total);
       u64 *const total_host = reinterpret_cast<u64 *>(ws.err_host + 2);
       SBWT_CUDA(cudaMemcpyAsync(total_host, sc.total, 8, cudaMemcpyDeviceToHost, user_stream));
       check_err_word(ws, user_stream);
@@ -2963,9 +2983,6 @@ void IndexImpl::search_reads(const char *chars, u64 n_chars, const u64 *read_end
       if (n_results) *n_results = n_k;
       if (n_k > capacity)
         throw Error(SBWT_E_CAPACITY, "results_capacity smaller than the k-mer count");
-      launch_search(*this, n_chars, read_ends, n_reads, 0, n_k, results, capacity, flags, cfg, sc,
-                    user_stream);
-      check_err_word(ws, user_stream);
     } else if (n_results) {
       *n_results = 0;
     }

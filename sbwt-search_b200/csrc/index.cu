@@ -1769,6 +1769,10 @@ __global__ void __launch_bounds__(256, MINB)
   }
 }
 
+// Tables up to this size stay in L2 (126 MB on B200) beside the filter and
+// the streams of one launch: the k-mers kernels load their lines evict-last.
+constexpr uint64_t kTableL2ResidentBytes = 96ULL << 20;
+
 // Read search with every k-mer looked up on its own (k <= 31, k-mer table and
 // filter): no stream steps, so no lane waits on the previous k-mer of its
 // read.  A warp takes chunks of 32 * PER consecutive k-mer slots; lane j
@@ -1799,7 +1803,11 @@ __global__ void __launch_bounds__(256)
   const I n_chunks = (n_kmers + CH - 1) / CH;
   const uint64_t warp0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  const uint64_t pol_first = l2_policy_evict_first();
+  // table lines: evict-last when the table fits well inside L2 (its lines
+  // are touched again by later k-mers), evict-first when it does not
+  const uint64_t pol_table = (s.kmer_table_mask + 1) * 16 <= kTableL2ResidentBytes
+                                 ? l2_policy_evict_last()
+                                 : l2_policy_evict_first();
   uint64_t n_table = 0, n_filter = 0, n_known = 0;
   // Every phase below issues all its loads before it uses any (no load waits
   // on a branch over another's value), so one chunk costs about four
@@ -1905,7 +1913,7 @@ __global__ void __launch_bounds__(256)
         A[t] = Block{0, 0, 0, 0};
         if (look[t]) {
           A[t] = load_block_hint(
-              reinterpret_cast<const Block *>(s.kmer_table + 2 * (uint64_t)hs[t]), pol_first);
+              reinterpret_cast<const Block *>(s.kmer_table + 2 * (uint64_t)hs[t]), pol_table);
           any = true;
         }
       }
@@ -1961,7 +1969,11 @@ __global__ void __launch_bounds__(256)
   const I n_chunks = (n_kmers + CH - 1) / CH;
   const uint64_t warp0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  const uint64_t pol_first = l2_policy_evict_first();
+  // table lines: evict-last when the table fits well inside L2 (its lines
+  // are touched again by later k-mers), evict-first when it does not
+  const uint64_t pol_table = (s.kmer_table_mask + 1) * 16 <= kTableL2ResidentBytes
+                                 ? l2_policy_evict_last()
+                                 : l2_policy_evict_first();
   uint64_t n_table = 0, n_filter = 0, n_known = 0;
   // Every phase below issues all its loads before it uses any (no load waits
   // on a branch over another's value), so one chunk costs about four
@@ -2106,7 +2118,7 @@ __global__ void __launch_bounds__(256)
         A[t] = Block{0, 0, 0, 0};
         if (look[t]) {
           A[t] = load_block_hint(
-              reinterpret_cast<const Block *>(s.kmer_table + 2 * (uint64_t)hs[t]), pol_first);
+              reinterpret_cast<const Block *>(s.kmer_table + 2 * (uint64_t)hs[t]), pol_table);
           any = true;
         }
       }

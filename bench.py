@@ -570,6 +570,34 @@ def profiled_traffic_per_kmer(kernel: str):
     return None
 
 
+def link_roofline(torch, dev, h2d_bytes, d2h_bytes, step_s):
+    """The host link's bound on an e2e step: pinned H2D and D2H copy rates of
+    this GPU measured on 1 GiB (CUDA events, best of 3), and the step's
+    minimum time if the two directions overlap fully (the larger of the two
+    transfer times), over the measured step time."""
+    n = 1 << 30
+    d = torch.empty(n, dtype=torch.uint8, device=f"cuda:{dev}")
+    h = torch.empty(n, dtype=torch.uint8).pin_memory()
+    rates = {}
+    for name, dst, src in (("h2d", d, h), ("d2h", h, d)):
+        best = 0.0
+        for _ in range(3):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            dst.copy_(src, non_blocking=True)
+            e1.record()
+            torch.cuda.synchronize()
+            best = max(best, n / (e0.elapsed_time(e1) / 1e3))
+        rates[name] = best
+    del d, h
+    t_min = max(h2d_bytes / rates["h2d"], d2h_bytes / rates["d2h"])
+    return {"h2d_gbs": rates["h2d"] / 1e9, "d2h_gbs": rates["d2h"] / 1e9,
+            "t_min_ms": t_min * 1e3, "frac": t_min / step_s,
+            "how": "cudaMemcpyAsync of 1 GiB between pinned host memory and the device, "
+                   "best of 3; t_min = max(H2D bytes / H2D rate, D2H bytes / D2H rate)"}
+
+
 def load_peaks():
     p = REPO / "MEASURED_PEAKS.json"
     if p.exists():
@@ -1261,7 +1289,10 @@ def main():
                "h2d_bytes_per_step": int(chars.nbytes + ends.nbytes),
                "d2h_bytes_per_step": int(n_kmers * 8),
                "ms_per_step": e_dt * 1e3,
-               "results": "u64 per k-mer, DMA into pinned host memory"}
+               "results": "u64 per k-mer, DMA into pinned host memory",
+               "link": link_roofline(torch, dev, chars.nbytes + ends.nbytes, n_kmers * 8,
+                                     e_dt)}
+        del h_chars, h_ends, h_out
 
     # roofline of the dominant kernel (the read search kernel)
     peak, peak_kind = load_peaks()

@@ -128,29 +128,34 @@ constexpr int kColorBlocksPerSm = SBWT_COLORS_BLOCKS_PER_SM;
 
 // Adds m copies of the sparse color list sparse[start, start + len) to this
 // warp's counters for the row words [wbase, wbase + 32 * WL).  Warp-uniform.
+// 32 ids at a time: each lane ORs its id's bit into the row word it falls in
+// (stage: the warp's 32 * WL zeroed words in shared memory), then every lane
+// adds its own staged words and zeroes them again.
 __device__ __forceinline__ void add_sparse(const ColorsView &cv, uint64_t *planes,
-                                           uint32_t stride, uint32_t P, uint32_t WL,
-                                           uint32_t wbase, uint32_t lane, uint64_t start,
-                                           uint32_t len, uint32_t m) {
+                                           uint64_t *stage, uint32_t stride, uint32_t P,
+                                           uint32_t WL, uint32_t wbase, uint32_t lane,
+                                           uint64_t start, uint32_t len, uint32_t m) {
   const uint32_t span = 32 * WL;
   for (uint32_t c0 = 0; c0 < len; c0 += 32) {
-    const uint32_t id = (c0 + lane < len) ? __ldg(cv.sparse + start + c0 + lane) : 0xFFFFFFFFu;
+    const bool in = c0 + lane < len;
+    const uint32_t id = in ? __ldg(cv.sparse + start + c0 + lane) : 0xFFFFFFFFu;
     const uint32_t n = min(32u, len - c0);
     if (cv.tiles > 1 && cv.sparse_sorted) {  // ascending ids: skip chunks outside the tile
       if ((__shfl_sync(0xFFFFFFFFu, id, n - 1) >> 6) < wbase) continue;
       if ((__shfl_sync(0xFFFFFFFFu, id, 0) >> 6) >= wbase + span) break;
     }
-    uint64_t x[4] = {0, 0, 0, 0};
-    for (uint32_t q = 0; q < n; ++q) {
-      const uint32_t c = __shfl_sync(0xFFFFFFFFu, id, q);
-      const uint32_t local = (c >> 6) - wbase;  // wraps above span when below the tile
-      const uint64_t bit = (local < span && (local & 31) == lane) ? 1ULL << (c & 63) : 0;
-#pragma unroll
-      for (uint32_t w = 0; w < 4; ++w) x[w] |= (local >> 5) == w ? bit : 0;
+    const uint32_t local = (id >> 6) - wbase;  // wraps above span when below the tile
+    if (in && local < span) atomicOr((unsigned long long *)(stage + local), 1ULL << (id & 63));
+    __syncwarp();
+    for (uint32_t w = 0; w < WL; ++w) {
+      const uint32_t li = lane + 32 * w;
+      const uint64_t x = stage[li];
+      if (x) {
+        stage[li] = 0;
+        add_weighted(planes + li, stride, P, x, m);
+      }
     }
-#pragma unroll
-    for (uint32_t w = 0; w < 4; ++w)
-      if (w < WL && x[w]) add_weighted(planes + lane + 32 * w, stride, P, x[w], m);
+    __syncwarp();
   }
 }
 
@@ -169,15 +174,17 @@ __global__ void __launch_bounds__(32 * kColorWarps, kColorBlocksPerSm)
   extern __shared__ uint64_t smem[];
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const uint32_t WL = cv.words_per_lane, P = job.planes, T = cv.tiles;
-  // per warp: P planes x (32 * WL) words, plane-major so lanes are contiguous
+  // per warp: P planes x (32 * WL) words, plane-major so lanes are contiguous,
+  // then 32 * WL staging words for the sparse lists
   const uint32_t stride = 32 * WL;
-  uint64_t *planes = smem + (uint64_t)wid * P * stride;
+  uint64_t *planes = smem + (uint64_t)wid * (P + 1) * stride;
+  uint64_t *stage = planes + (uint64_t)P * stride;
   const uint64_t warps = (uint64_t)gridDim.x * kColorWarps;
   const uint64_t n_items = job.n_reads * T;
   for (uint64_t item = blockIdx.x * (uint64_t)kColorWarps + wid; item < n_items; item += warps) {
     const uint64_t r = T == 1 ? item : item / T;
     const uint32_t wbase = (uint32_t)(item - r * T) * stride;
-    for (uint32_t q = lane; q < P * stride; q += 32) planes[q] = 0;
+    for (uint32_t q = lane; q < (P + 1) * stride; q += 32) planes[q] = 0;
     __syncwarp();
     const uint64_t o0 = job.offs[r], o1 = job.offs[r + 1];
     uint32_t found = 0, not_found = 0, invalid = 0;
@@ -238,7 +245,7 @@ __global__ void __launch_bounds__(32 * kColorWarps, kColorBlocksPerSm)
 #pragma unroll
           for (int u = 0; u < kRowsInFlight; ++u)
             if (wt[u] && !(rr[u] & 1ULL))
-              add_sparse(cv, planes, stride, P, WL, wbase, lane, rec_start(rr[u]),
+              add_sparse(cv, planes, stage, stride, P, WL, wbase, lane, rec_start(rr[u]),
                          rec_len(rr[u]), wt[u]);
         }
       }
@@ -635,7 +642,7 @@ void ColorsImpl::launch(const u64 *d_vals, const u64 *d_offs, const u64 *d_nf,
   job.pass_bits = d_pass_bits;
   job.pass_count = d_pass_count;
   job.counts = d_counts;
-  const size_t smem = (size_t)kColorWarps * job.planes * 32 * view.words_per_lane * 8;
+  const size_t smem = (size_t)kColorWarps * (job.planes + 1) * 32 * view.words_per_lane * 8;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   const u64 items = n_reads * view.tiles;
@@ -680,7 +687,7 @@ void ColorsImpl::enqueue_pseudoalign(const u64 *d_vals, const u64 *d_offs, u64 n
 
 void ColorsImpl::prepare_launch(u64 max_kmers) const {
   const uint32_t P = planes_for(max_kmers);
-  const size_t smem = (size_t)kColorWarps * P * 32 * view.words_per_lane * 8;
+  const size_t smem = (size_t)kColorWarps * (P + 1) * 32 * view.words_per_lane * 8;
   for (auto kernel : {colors_kernel<0, true>, colors_kernel<0, false>, colors_kernel<1, true>,
                       colors_kernel<1, false>})
     SBWT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

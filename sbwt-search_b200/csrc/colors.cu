@@ -113,28 +113,6 @@ __device__ __forceinline__ void add_weighted(uint64_t *planes, uint32_t stride, 
   }
 }
 
-// Adds m copies of row word x.  PF > 0 (the counters have PF planes and
-// m < 2^PF): one branch-free pass of a bit-sliced adder of the constant m
-// over all PF planes (sum = p ^ m_j ^ carry, carry = majority), whatever the
-// bits of m; the counters stay below 2^PF, so no carry leaves the top plane.
-// PF = 0: one ripple per set bit of m over the runtime P planes.
-template <int PF>
-__device__ __forceinline__ void add_rows(uint64_t *planes, uint32_t stride, uint32_t P,
-                                         uint64_t x, uint32_t m) {
-  if constexpr (PF > 0) {
-    uint64_t c = 0;
-#pragma unroll
-    for (int j = 0; j < PF; ++j) {
-      const uint64_t mj = ((m >> j) & 1u) ? x : 0ULL;
-      const uint64_t p = planes[(uint32_t)j * stride];
-      planes[(uint32_t)j * stride] = p ^ mj ^ c;
-      c = (p & mj) | (c & (p ^ mj));
-    }
-  } else {
-    add_weighted(planes, stride, P, x, m);
-  }
-}
-
 // 2 rows in flight at a 12-blocks-per-SM register budget: 21.9 ms against
 // 23.6 ms for 4 rows at 6 blocks (2 M reads of the 2000-genome workload);
 // more rows in flight cost occupancy and were slower (8 rows: 44-50 ms)
@@ -153,7 +131,6 @@ constexpr int kColorBlocksPerSm = SBWT_COLORS_BLOCKS_PER_SM;
 // 32 ids at a time: each lane ORs its id's bit into the row word it falls in
 // (stage: the warp's 32 * WL zeroed words in shared memory), then every lane
 // adds its own staged words and zeroes them again.
-template <int PF>
 __device__ __forceinline__ void add_sparse(const ColorsView &cv, uint64_t *planes,
                                            uint64_t *stage, uint32_t stride, uint32_t P,
                                            uint32_t WL, uint32_t wbase, uint32_t lane,
@@ -175,7 +152,7 @@ __device__ __forceinline__ void add_sparse(const ColorsView &cv, uint64_t *plane
       const uint64_t x = stage[li];
       if (x) {
         stage[li] = 0;
-        add_rows<PF>(planes + li, stride, P, x, m);
+        add_weighted(planes + li, stride, P, x, m);
       }
     }
     __syncwarp();
@@ -189,10 +166,8 @@ __device__ __forceinline__ void add_sparse(const ColorsView &cv, uint64_t *plane
 // its distinct records once with their multiplicity (__match_any_sync), rows
 // kRowsInFlight at a time.  Counts are sums, so the order and grouping of the
 // adds does not change them.
-// mode 0: pass bitmask + count per read; mode 1: full counts.  PF: 8 when
-// the counters have exactly 8 planes (reads of at most 255 k-mers; branch-
-// free adds), else 0 (any plane count).
-template <int MODE, bool DIRECT, int PF>
+// mode 0: pass bitmask + count per read; mode 1: full counts.
+template <int MODE, bool DIRECT>
 __global__ void __launch_bounds__(32 * kColorWarps, kColorBlocksPerSm)
     colors_kernel(ColorsView cv, ColorsJob job, uint32_t *err) {
   constexpr uint32_t FULL = 0xFFFFFFFFu;
@@ -265,13 +240,13 @@ __global__ void __launch_bounds__(32 * kColorWarps, kColorBlocksPerSm)
                          : 0;
 #pragma unroll
             for (int u = 0; u < kRowsInFlight; ++u)
-              if (x[u]) add_rows<PF>(planes + local, stride, P, x[u], wt[u]);
+              if (x[u]) add_weighted(planes + local, stride, P, x[u], wt[u]);
           }
 #pragma unroll
           for (int u = 0; u < kRowsInFlight; ++u)
             if (wt[u] && !(rr[u] & 1ULL))
-              add_sparse<PF>(cv, planes, stage, stride, P, WL, wbase, lane,
-                             rec_start(rr[u]), rec_len(rr[u]), wt[u]);
+              add_sparse(cv, planes, stage, stride, P, WL, wbase, lane, rec_start(rr[u]),
+                         rec_len(rr[u]), wt[u]);
         }
       }
     }
@@ -661,7 +636,7 @@ void ColorsImpl::launch(const u64 *d_vals, const u64 *d_offs, const u64 *d_nf,
   job.tau = tau;
   job.include_not_found = (flags & SBWT_INCLUDE_NOT_FOUND) ? 1 : 0;
   job.include_invalid = (flags & SBWT_INCLUDE_INVALID) ? 1 : 0;
-  job.planes = planes_for(max_kmers) <= 8 ? 8u : planes_for(max_kmers);
+  job.planes = planes_for(max_kmers);
   if (mode == 0 && view.tiles > 1)  // tiles of a read add their passing counts
     SBWT_CUDA(cudaMemsetAsync(d_pass_count, 0, n_reads * 4, st));
   job.pass_bits = d_pass_bits;
@@ -678,15 +653,10 @@ void ColorsImpl::launch(const u64 *d_vals, const u64 *d_offs, const u64 *d_nf,
                                    (int)smem));
     kernel<<<(unsigned)blocks, 32 * kColorWarps, smem, st>>>(view, job, d_err);
   };
-  const bool p8 = job.planes == 8;
-  if (mode == 0 && p8)
-    direct ? go(colors_kernel<0, true, 8>) : go(colors_kernel<0, false, 8>);
-  else if (mode == 0)
-    direct ? go(colors_kernel<0, true, 0>) : go(colors_kernel<0, false, 0>);
-  else if (p8)
-    direct ? go(colors_kernel<1, true, 8>) : go(colors_kernel<1, false, 8>);
+  if (mode == 0)
+    direct ? go(colors_kernel<0, true>) : go(colors_kernel<0, false>);
   else
-    direct ? go(colors_kernel<1, true, 0>) : go(colors_kernel<1, false, 0>);
+    direct ? go(colors_kernel<1, true>) : go(colors_kernel<1, false>);
   SBWT_CUDA(cudaGetLastError());
 }
 
@@ -716,12 +686,10 @@ void ColorsImpl::enqueue_pseudoalign(const u64 *d_vals, const u64 *d_offs, u64 n
 }
 
 void ColorsImpl::prepare_launch(u64 max_kmers) const {
-  const uint32_t P = planes_for(max_kmers) <= 8 ? 8u : planes_for(max_kmers);
+  const uint32_t P = planes_for(max_kmers);
   const size_t smem = (size_t)kColorWarps * (P + 1) * 32 * view.words_per_lane * 8;
-  for (auto kernel : {colors_kernel<0, true, 8>, colors_kernel<0, false, 8>,
-                      colors_kernel<1, true, 8>, colors_kernel<1, false, 8>,
-                      colors_kernel<0, true, 0>, colors_kernel<0, false, 0>,
-                      colors_kernel<1, true, 0>, colors_kernel<1, false, 0>})
+  for (auto kernel : {colors_kernel<0, true>, colors_kernel<0, false>, colors_kernel<1, true>,
+                      colors_kernel<1, false>})
     SBWT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
 }

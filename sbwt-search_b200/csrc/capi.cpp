@@ -200,7 +200,7 @@ int sbwt_index_set_kmer_table(sbwt_index_t *index, int enable, uint64_t *table_b
       x.build_kmer_table();
     }
     x.device_bytes = x.presearch.size() + x.hot.size() + x.key_buf.size() + x.l0_all.size() +
-                     x.kmer_table.size() + x.kmer_filter.size() + x.lmer_filter.size();
+                     x.kmer_table.size() + x.kmer_filter.size();
     if (table_bytes) *table_bytes = x.kmer_table.size();
   });
 }
@@ -336,8 +336,8 @@ int sbwt_set_probe_length(uint32_t probe_len) {
 // kernel staging 8/16 slots, 18 the same with the filter and 16 slots,
 // negative = the library default.  Results do not depend on it.
 int sbwt_set_table_kernel(int mode) {
-  if (mode > 20) {
-    set_last_error("table kernel mode must be 0..20 (or negative for the default)");
+  if (mode > 19) {
+    set_last_error("table kernel mode must be 0..19 (or negative for the default)");
     return SBWT_E_INVALID;
   }
   default_launch_config().table_kernel = mode < 0 ? kDefaultTableKernel : (uint32_t)mode;

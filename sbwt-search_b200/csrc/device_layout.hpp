@@ -52,11 +52,6 @@ struct SbwtView {
   uint64_t kmer_table_mask;    // slots - 1
   const uint64_t *kmer_filter; // blocked Bloom filter of the table's keys, or nullptr
   uint64_t filter_words;       // 64-bit words of kmer_filter
-  // blocked Bloom filter of every L-mer inside the table's keys (L =
-  // lmer_len), or nullptr: an L-mer it rejects occurs in no SBWT k-mer
-  const uint64_t *lmer_filter;
-  uint64_t lmer_words;         // 64-bit words of lmer_filter
-  uint32_t lmer_len;           // L
   uint64_t num_bits;
   uint32_t k;
   uint32_t p;      // presearch depth used by this call

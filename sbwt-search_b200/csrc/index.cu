@@ -1275,7 +1275,7 @@ __global__ void __launch_bounds__(256, SBWT_TABLE_MIN_BLOCKS)
 // k-mer slots (tiles are multiples of 4 slots) when the output is 32-byte
 // aligned.
 enum : uint32_t { WK_NEW = 0, WK_STREAM = 1, WK_STEP = 2, WK_SG = 3, WK_FILTER = 4, WK_HASH = 5,
-                  WK_DONE = 6, WK_LMER = 7 };
+                  WK_DONE = 6 };
 constexpr uint32_t kFilterBatch = 4;
 
 __device__ __forceinline__ uint64_t load_u64_nc(const uint64_t *p) {
@@ -1327,17 +1327,8 @@ __device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_
 // G consecutive results (G * 8 bytes, a full 128-byte line for G = 16).
 // G: slots staged per walk before they are stored (4, 8 or 16); without
 // LEAN, results leave as 32-byte stores of 4 slots per lane.
-// LSKIP (with LEAN, without LFILTER): after a failed stream step (k-mer
-// x[s..e] absent after a found one) the walk probes the L-mer filter
-// (WK_LMER) for the L-mer ending at e; if it is rejected, the k-mers
-// starting up to e - L + 1 are -1 without a lookup (a run, like the runs of
-// -2, cut where a k-mer would hold an invalid char), and at e - L + 2 it
-// probes the L-mer starting at e, which covers the k-mers starting up to e.
-// A rejection is exact (the filter has every L-mer of every SBWT k-mer), so
-// results do not change; an L-mer the filter passes sends the walk to the
-// table as before.
 template <int W, int MINB, bool COUNT, bool LEAN = false, bool LFILTER = false,
-          bool LSTAGE = false, int G = 4, bool LSKIP = false>
+          bool LSTAGE = false, int G = 4>
 __global__ void __launch_bounds__(256, MINB)
     search_walks_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
                         unsigned long long *counters) {
@@ -1367,25 +1358,16 @@ __global__ void __launch_bounds__(256, MINB)
   uint32_t *const out32 = rv.out32;
   const bool vec_out32 = ((uintptr_t)out32 & 15) == 0;
   uint64_t n_table = 0, n_block = 0, n_sg = 0, n_filter = 0, n_iter = 0, n_lane = 0,
-           n_known = 0, n_searched = 0, n_stream = 0, n_step = 0, n_distinct = 0, n_lmer = 0,
-           n_skip = 0;
+           n_known = 0, n_searched = 0, n_stream = 0, n_step = 0, n_distinct = 0;
   I slot[W], slot_end[W], r[W], r_next[W], pos[W], last_inv1[W], v[W], x[W], hslot[W];
   I obase[W];
   uint32_t mode[W], ubit[W], nb[W], omask[W];
-  // LSKIP: the last char e of the k-mer whose stream step failed, the probe
-  // stage (0 none, 1 the L-mer ending at e, 2 the L-mer starting at e), and
-  // one past the last k-mer start proven absent
-  I lm_e[W], absent_end[W];
-  uint32_t lm_stage[W];
-  const uint32_t L = LSKIP ? s.lmer_len : 0u;
   CharWin<I> cw[W];
 #pragma unroll
   for (int w = 0; w < W; ++w) {
     slot[w] = slot_end[w] = r[w] = r_next[w] = pos[w] = last_inv1[w] = x[w] = hslot[w] = 0;
     v[w] = NONE;
     obase[w] = 0;
-    lm_e[w] = absent_end[w] = 0;
-    lm_stage[w] = 0;
     mode[w] = WK_NEW;
     ubit[w] = 63;
     nb[w] = 0;
@@ -1502,15 +1484,13 @@ __global__ void __launch_bounds__(256, MINB)
         }
       }
     }
-    // ---- phase 1 (per walk): the next k-mer, runs of -2 (and of -1), the
-    // walk's mode
+    // ---- phase 1 (per walk): the next k-mer, runs of -2, the walk's mode
     I run_slot[W];
-    uint32_t run_n[W], run_code[W];  // run_code: the 32-bit result code of the run
+    uint32_t run_n[W];
 #pragma unroll
     for (int w = 0; w < W; ++w) {
       run_slot[w] = 0;
       run_n[w] = 0;
-      run_code[w] = 0xFFFFFFFEu;
       if (mode[w] != WK_NEW) continue;
       bool ready = false;
       while (true) {
@@ -1526,7 +1506,6 @@ __global__ void __launch_bounds__(256, MINB)
           cw[w].move_to(rv.packed, rv.invalid, pos[w]);
           last_inv1[w] = cw[w].last_invalid1(pos[w], pos[w] + k - 1);
           v[w] = NONE;
-          if (LSKIP) absent_end[w] = lm_stage[w] = 0;
         } else if (slot[w] == r_next[w]) {  // next read
           do {
             r_next[w] = (I)__ldg(rv.kmer_off + (++r[w]) + 1);
@@ -1535,36 +1514,11 @@ __global__ void __launch_bounds__(256, MINB)
           cw[w].move_to(rv.packed, rv.invalid, pos[w]);
           last_inv1[w] = cw[w].last_invalid1(pos[w], pos[w] + k - 1);
           v[w] = NONE;
-          if (LSKIP) absent_end[w] = lm_stage[w] = 0;
         }
         const I newc = pos[w] + k - 1;
         cw[w].move_to(rv.packed, rv.invalid, pos[w]);
         if (cw[w].invalid_at(newc)) last_inv1[w] = newc + 1;
         if (last_inv1[w] <= pos[w]) {
-          if (LSKIP && v[w] == NONE && pos[w] < absent_end[w]) {
-            if (run_n[w]) break;  // one run per walk per iteration
-            // k-mers pos .. absent_end - 1 hold a rejected L-mer: a run of -1
-            // up to the read / tile end and to the last k-mer whose chars
-            // are all valid and inside the char window (the current k-mer's
-            // are: the first invalid char past newc bounds the run)
-            const uint32_t o1 = pos[w] + k - 32 * cw[w].wbase;  // <= 62
-            const uint64_t later = cw[w].inv >> o1;
-            const I c_inv = later ? pos[w] + k + (I)(__ffsll((long long)later) - 1)
-                                  : 32 * cw[w].wbase + 64;
-            const I n = min(min(absent_end[w] - pos[w], c_inv - newc),
-                            min(r_next[w], slot_end[w]) - slot[w]);
-            run_slot[w] = slot[w];
-            run_n[w] = (uint32_t)n;
-            run_code[w] = 0xFFFFFFFFu;
-            if (COUNT) n_skip += n;
-            slot[w] += n;
-            pos[w] += n;
-            if (slot[w] < min(r_next[w], slot_end[w])) {
-              cw[w].move_to(rv.packed, rv.invalid, pos[w]);
-              last_inv1[w] = cw[w].last_invalid1(pos[w], pos[w] + k - 1);
-            }
-            continue;
-          }
           ready = true;
           break;
         }
@@ -1574,7 +1528,6 @@ __global__ void __launch_bounds__(256, MINB)
         const I n = min(last_inv1[w] - pos[w], min(r_next[w], slot_end[w]) - slot[w]);
         run_slot[w] = slot[w];
         run_n[w] = (uint32_t)n;
-        run_code[w] = 0xFFFFFFFEu;
         if (COUNT) n_known += n;
         v[w] = NONE;
         slot[w] += n;
@@ -1591,12 +1544,7 @@ __global__ void __launch_bounds__(256, MINB)
         } else if (LEAN && LFILTER) {
           nb[w] = 1;
           mode[w] = WK_FILTER;
-        } else if (LEAN && LSKIP && s.lmer_filter &&
-                   ((lm_stage[w] == 1 && pos[w] + k == lm_e[w] + 2) ||
-                    (lm_stage[w] == 2 && pos[w] + L == lm_e[w] + 2))) {
-          mode[w] = WK_LMER;  // the k-mer right after the failed one, or after the first run
         } else if (LEAN) {
-          if (LSKIP) lm_stage[w] = 0;
           hslot[w] = (I)kmer_table_bucket(cw[w].prefix(pos[w], k), s.kmer_table_mask);
           mode[w] = WK_HASH;
         } else {
@@ -1620,17 +1568,12 @@ __global__ void __launch_bounds__(256, MINB)
         const int q = __ffs(runs) - 1;
         const I q_slot = __shfl_sync(0xFFFFFFFFu, run_slot[w], q);
         const uint32_t q_n = __shfl_sync(0xFFFFFFFFu, run_n[w], q);
-        const uint32_t q_code =
-            LSKIP ? __shfl_sync(0xFFFFFFFFu, run_code[w], q) : 0xFFFFFFFEu;
-        const unsigned long long q_val = q_code == 0xFFFFFFFFu
-                                             ? (unsigned long long)SBWT_NOT_FOUND
-                                             : (unsigned long long)SBWT_INVALID;
         for (uint32_t j = lane; j < q_n; j += 32) {
           if (q_slot + j >= out_cap) continue;
           if (out32)
-            __stcs(out32 + q_slot + j, q_code);
+            __stcs(out32 + q_slot + j, 0xFFFFFFFEu);
           else
-            __stcs(rv.out + q_slot + j, q_val);
+            __stcs(rv.out + q_slot + j, (unsigned long long)SBWT_INVALID);
         }
       }
     }
@@ -1688,13 +1631,6 @@ __global__ void __launch_bounds__(256, MINB)
       } else if (mode[w] == WK_HASH) {
         A[w] = load_block_hint(reinterpret_cast<const Block *>(s.kmer_table + 2 * (uint64_t)hslot[w]),
                                pol_first);
-      } else if (LSKIP && mode[w] == WK_LMER) {
-        // stage 1: the L chars ending at e; stage 2: the L chars from e
-        // (both inside the current k-mer)
-        const I st = lm_stage[w] == 1 ? lm_e[w] + 1 - L : lm_e[w];
-        const uint64_t z = kmer_mix(cw[w].prefix(st, L));
-        fz[w] = z;
-        A[w].w0 = load_u64_hint(s.lmer_filter + kmer_filter_word(z, s.lmer_words), pol_first);
       } else if (mode[w] == WK_FILTER) {
         uint64_t z = kmer_mix(cw[w].prefix(pos[w], k));
         fz[w] = z;
@@ -1725,7 +1661,6 @@ __global__ void __launch_bounds__(256, MINB)
         n_block += md == WK_STREAM || md == WK_STEP;
         n_sg += md == WK_SG;
         n_filter += md == WK_FILTER ? nb[w] : 0;
-        n_lmer += md == WK_LMER;
         n_stream += md == WK_STREAM;
         n_step += md == WK_STEP;
       }
@@ -1754,19 +1689,6 @@ __global__ void __launch_bounds__(256, MINB)
           ++pos[w];
         }
         if (j == nb[w]) mode[w] = WK_NEW;  // v stays NONE
-        continue;
-      }
-      if (LSKIP && md == WK_LMER) {
-        const uint64_t bits = kmer_filter_bits(fz[w]);
-        if ((A[w].w0 & bits) != bits) {  // the L-mer is in no SBWT k-mer
-          absent_end[w] = lm_stage[w] == 1 ? lm_e[w] + 2 - L : lm_e[w] + 1;
-          lm_stage[w] = lm_stage[w] == 1 ? 2u : 0u;
-          mode[w] = WK_NEW;  // v stays NONE: the run starts next iteration
-        } else {
-          lm_stage[w] = 0;
-          hslot[w] = (I)kmer_table_bucket(cw[w].prefix(pos[w], k), s.kmer_table_mask);
-          mode[w] = WK_HASH;
-        }
         continue;
       }
       if (md != WK_STREAM && md != WK_STEP && md != WK_SG && md != WK_HASH) continue;
@@ -1816,10 +1738,6 @@ __global__ void __launch_bounds__(256, MINB)
       }
       if (emitted) {
         if (COUNT) ++n_searched;
-        if (LSKIP && res == NONE && md != WK_HASH) {  // a failed stream step
-          lm_e[w] = pos[w] + k - 1;
-          lm_stage[w] = 1;
-        }
         v[w] = res;
         emit(w, slot[w], res);
         ++slot[w];
@@ -1847,9 +1765,7 @@ __global__ void __launch_bounds__(256, MINB)
     atomicAdd(counters + 10, (unsigned long long)n_step);    // steps at a group start
     atomicAdd(counters + 11, (unsigned long long)n_sg);      // group scan words
     atomicAdd(counters + 12, (unsigned long long)n_table);   // table lookups
-    atomicAdd(counters + 13, (unsigned long long)n_lmer);    // L-mer filter words
     atomicAdd(counters + 14, (unsigned long long)n_distinct);
-    atomicAdd(counters + 15, (unsigned long long)n_skip);    // k-mers -1 by L-mer runs
   }
 }
 
@@ -2345,7 +2261,7 @@ static void launch_one_wave(void (*kernel)(KArgs...), int grid, int threads, cud
 // lean walks kernel (1 walk) with staged stores, without and with the
 // one-k-mer filter; 15 = the k-mers kernel with consecutive slots per lane;
 // 16, 17 = 13 staging 8 or 16 slots per store group; 18 = 14 staging 16;
-// 19 = 6 without the filter; 20 = 17 with the L-mer skips (LSKIP).
+// 19 = 6 without the filter.
 // Results never depend on it.
 // Whether launch_search_kernel runs the walks kernel (the only one that can
 // write 32-bit results, ReadsView::out32).
@@ -2446,15 +2362,6 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
       launch_ex(search_walks_kernel<W_, B_, false, true, F_, true, G_>, grid, threads, st, \
                 la, sv, rv, tile_read, ctr);                                               \
   } while (0)
-#define SBWT_LEANSK(W_, B_, G_)                                                            \
-  do {                                                                                     \
-    if (ctr)                                                                               \
-      launch_ex(search_walks_kernel<W_, B_, true, true, false, true, G_, true>, grid,      \
-                threads, st, la, sv, rv, tile_read, ctr);                                  \
-    else                                                                                   \
-      launch_ex(search_walks_kernel<W_, B_, false, true, false, true, G_, true>, grid,     \
-                threads, st, la, sv, rv, tile_read, ctr);                                  \
-  } while (0)
 #define SBWT_WALKS(W_, B_)                                                                 \
   do {                                                                                     \
     if (ctr)                                                                               \
@@ -2481,7 +2388,6 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
     else if (kernel_mode == 16) SBWT_LEANSG(1, 5, false, 8);
     else if (kernel_mode == 17) SBWT_LEANSG(1, 6, false, 16);
     else if (kernel_mode == 18) SBWT_LEANSG(1, 5, true, 16);
-    else if (kernel_mode == 20) SBWT_LEANSK(1, 5, 16);
     else if (kernel_mode == 14) SBWT_LEANS(1, 5, true);
     else if (kernel_mode == 11 && ctr)
       launch_one_wave(search_kmers_kernel<2, true>,
@@ -2511,7 +2417,6 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
 #undef SBWT_LEAN
 #undef SBWT_LEANS
 #undef SBWT_LEANSG
-#undef SBWT_LEANSK
   } else if (table) {
     if (ctr)
       launch_ex(search_table_kernel<true>, grid, threads, st, la, sv, rv, tile_read, ctr);
@@ -2696,7 +2601,7 @@ IndexImpl::IndexImpl(const u64 *const acgt[4], u64 num_bits_, u32 k_,
   SBWT_CUDA(cudaDeviceSynchronize());
   build_kmer_table();
   device_bytes = presearch.size() + hot.size() + key_buf.size() + l0_all.size() +
-                 kmer_table.size() + kmer_filter.size() + lmer_filter.size();
+                 kmer_table.size() + kmer_filter.size();
 }
 
 SbwtView IndexImpl::view_for(u32 p) const {

@@ -75,7 +75,7 @@ struct IndexImpl {
   u64 device_bytes = 0;
   SbwtView view{};
   DeviceBuffer hot;  // rank blocks of A/C/G/T + suffix-group words, contiguous
-  DeviceBuffer l0_all, presearch, key_buf, kmer_table, kmer_filter, lmer_filter;
+  DeviceBuffer l0_all, presearch, key_buf, kmer_table, kmer_filter;
   u64 table_kmers = 0;
   u64 window_bytes = 0;   // L2 access-policy window over `hot`
 };

@@ -28,14 +28,6 @@
 // structure inside the GPU's address-translation reach and mostly in L2,
 // and only k-mers the filter passes pay a table lookup.  A filter answer of
 // "absent" is exact (no false negatives), so results do not change.
-//
-// L-mer filter: the same kind of filter over every L-mer (L = (k + 2) / 2)
-// inside the table's keys.  An L-mer it rejects occurs in no SBWT k-mer, so
-// every read k-mer that contains it is absent: after a failed stream step
-// (k-mer x[s..e] absent, x[s-1..e-1] present) the L-mer ending at e proves
-// the k-mers starting in [s, e - L + 1] absent and the L-mer starting at e
-// those starting in [e + L - k, e] (2L >= k + 1: the two ranges meet), with
-// two filter probes instead of a table lookup per k-mer.
 #include <cuda_runtime.h>
 
 #include <cub/cub.cuh>
@@ -144,22 +136,6 @@ __global__ void filter_insert_kernel(const uint64_t *key, const uint8_t *alive, 
   }
 }
 
-// Every L-mer of every key (first char on top, like the keys).
-__global__ void lmer_insert_kernel(const uint64_t *key, const uint8_t *alive, uint64_t n,
-                                   uint32_t k, uint32_t L, unsigned long long *filter,
-                                   uint64_t n_words) {
-  const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t mask = (1ULL << (2 * L)) - 1;
-  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += step) {
-    if (!alive[v]) continue;
-    const uint64_t kk = key[v];
-    for (uint32_t j = 0; j + L <= k; ++j) {
-      const uint64_t z = kmer_mix((kk >> (2 * (k - L - j))) & mask);
-      atomicOr(filter + kmer_filter_word(z, n_words), (unsigned long long)kmer_filter_bits(z));
-    }
-  }
-}
-
 unsigned grid_of(uint64_t n) {
   return (unsigned)std::max<uint64_t>(std::min<uint64_t>((n + 255) / 256, 148 * 32), 1);
 }
@@ -220,9 +196,6 @@ bool IndexImpl::build_kmer_table() {
   if (slots > (1ULL << 32) || slots * 16 > kKmerTableMaxBytes ||
       slots * 16 + filter_words * 8 > free_b / 4)
     return false;
-  // the L-mer filter (same size as the k-mer filter) when it fits as well
-  const u32 lmer_len = (k + 2) / 2;
-  const bool with_lmers = k >= 4 && slots * 16 + 2 * filter_words * 8 <= free_b / 4;
   kmer_table.resize(slots * 16);
   SBWT_CUDA(cudaMemset(kmer_table.get(), 0xFF, slots * 16));
   DeviceBuffer d_err(4);
@@ -243,17 +216,6 @@ bool IndexImpl::build_kmer_table() {
                                             kmer_filter.get<unsigned long long>(),
                                             filter_words);
   SBWT_CUDA(cudaGetLastError());
-  if (with_lmers) {
-    lmer_filter.resize(filter_words * 8);
-    SBWT_CUDA(cudaMemset(lmer_filter.get(), 0, filter_words * 8));
-    lmer_insert_kernel<<<grid_of(n), 256>>>(key.get<u64>(), alive.get<uint8_t>(), n, k,
-                                            lmer_len, lmer_filter.get<unsigned long long>(),
-                                            filter_words);
-    SBWT_CUDA(cudaGetLastError());
-    view.lmer_filter = lmer_filter.get<u64>();
-    view.lmer_words = filter_words;
-    view.lmer_len = lmer_len;
-  }
   view.kmer_table = kmer_table.get<u64>();
   view.kmer_table_mask = slots - 1;
   view.kmer_filter = kmer_filter.get<u64>();
@@ -266,14 +228,10 @@ void IndexImpl::drop_kmer_table() {
   DeviceGuard g(device);
   kmer_table.release();
   kmer_filter.release();
-  lmer_filter.release();
   view.kmer_table = nullptr;
   view.kmer_table_mask = 0;
   view.kmer_filter = nullptr;
   view.filter_words = 0;
-  view.lmer_filter = nullptr;
-  view.lmer_words = 0;
-  view.lmer_len = 0;
   table_kmers = 0;
 }
 

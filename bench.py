@@ -754,7 +754,7 @@ KERNELS = {0: "search_reads_kernel", 1: "search_table_kernel", 2: "search_walks_
            10: "search_walks_kernel", 11: "search_kmers_kernel", 12: "search_kmers_kernel",
            13: "search_walks_kernel", 14: "search_walks_kernel", 15: "search_kmers_seq_kernel",
            16: "search_walks_kernel", 17: "search_walks_kernel", 18: "search_walks_kernel",
-           19: "search_kmers_kernel", 20: "search_walks_kernel", 21: "search_walks_kernel"}
+           19: "search_kmers_kernel"}
 DEFAULT_KERNEL_MODE = 7
 KMERS_KERNEL_MAX_BYTES = 256 << 20  # mode 7 picks the k-mers kernel up to this
 

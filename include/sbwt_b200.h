@@ -411,10 +411,9 @@ int sbwt_set_probe_length(uint32_t probe_len);
  *       k-mer slots per lane (one char window, one 32-byte result store);
  *       16, 17 = 13 with 8 or 16 slots staged per store group; 18 = 14 with
  *       16 slots; 19 = 6 without the filter (every valid k-mer to the
- *       table); 20, 21 = 17 with stream-step-only iterations between the
- *       full ones while at least 16 / 24 lanes of a warp can take one;
+ *       table);
  *   negative = the default.
- * Results never depend on it.  Returns SBWT_E_INVALID above 21. */
+ * Results never depend on it.  Returns SBWT_E_INVALID above 19. */
 int sbwt_set_table_kernel(int mode);
 /* The process-wide launch configuration (set by sbwt_set_launch_config,
  * sbwt_set_table_kernel, sbwt_autotune); any pointer may be NULL. */

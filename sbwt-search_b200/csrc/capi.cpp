@@ -336,8 +336,8 @@ int sbwt_set_probe_length(uint32_t probe_len) {
 // kernel staging 8/16 slots, 18 the same with the filter and 16 slots,
 // negative = the library default.  Results do not depend on it.
 int sbwt_set_table_kernel(int mode) {
-  if (mode > 21) {
-    set_last_error("table kernel mode must be 0..21 (or negative for the default)");
+  if (mode > 19) {
+    set_last_error("table kernel mode must be 0..19 (or negative for the default)");
     return SBWT_E_INVALID;
   }
   default_launch_config().table_kernel = mode < 0 ? kDefaultTableKernel : (uint32_t)mode;

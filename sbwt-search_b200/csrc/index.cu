@@ -1327,16 +1327,8 @@ __device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_
 // G consecutive results (G * 8 bytes, a full 128-byte line for G = 16).
 // G: slots staged per walk before they are stored (4, 8 or 16); without
 // LEAN, results leave as 32-byte stores of 4 slots per lane.
-// FASTMIN (with LEAN and LSTAGE, W = 1, > 0): after each full iteration the
-// warp runs stream steps only, for the lanes whose walk stands at a k-mer
-// that one stream step resolves without other work (previous k-mer found,
-// same read and tile, next char valid and in the char window, its staging
-// row open), for as long as at least FASTMIN lanes are such; the other
-// lanes wait for the next full iteration.  A stream step costs a few dozen
-// instructions there instead of the full iteration's union of every lane
-// mode's path.
 template <int W, int MINB, bool COUNT, bool LEAN = false, bool LFILTER = false,
-          bool LSTAGE = false, int G = 4, int FASTMIN = 0>
+          bool LSTAGE = false, int G = 4>
 __global__ void __launch_bounds__(256, MINB)
     search_walks_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
                         unsigned long long *counters) {
@@ -1440,38 +1432,6 @@ __global__ void __launch_bounds__(256, MINB)
     omask[w] |= 1u << (sl & (G - 1));
     if (omask[w] == GFULL) flush(w);
     }
-  };
-
-  // the warp stores the staged rows of complete or left groups (COOP)
-  auto coop_flush = [&]() {
-   if constexpr (COOP) {
-     constexpr int P = 32 / G;  // rows per store instruction
-     const int sub = (int)lane / G, q = (int)lane % G;
-#pragma unroll
-     for (int w = 0; w < W; ++w) {
-      const bool nf = omask[w] && (mode[w] == WK_DONE || omask[w] == GFULL ||
-                                   (slot[w] & ~I(G - 1)) != obase[w]);
-      for (unsigned fm = __ballot_sync(0xFFFFFFFFu, nf); fm;) {
-        int src = -1;
-#pragma unroll
-        for (int i = 0; i < P; ++i) {  // the sub-th lane left in fm
-          if (i == sub && fm) src = __ffs(fm) - 1;
-          fm &= fm - 1;
-        }
-        const int from = src < 0 ? (int)lane : src;
-        const I gb = __shfl_sync(0xFFFFFFFFu, obase[w], from);
-        const uint32_t gm = __shfl_sync(0xFFFFFFFFu, omask[w], from);
-        if (src >= 0 && ((gm >> q) & 1u) && gb + (I)q < out_cap) {
-          const uint32_t val = sh_row[w * 256 + (threadIdx.x & ~31u) + (unsigned)src][q];
-          if (out32)
-            __stcs(out32 + gb + q, val);
-          else
-            __stcs(rv.out + gb + q, (unsigned long long)widen_node(val));
-        }
-      }
-      if (nf) omask[w] = 0;
-     }
-   }
   };
 
   while (true) {
@@ -1617,7 +1577,34 @@ __global__ void __launch_bounds__(256, MINB)
         }
       }
     }
-    if (COOP) coop_flush();  // ---- the warp stores the rows of complete or left groups
+    if (COOP) {  // ---- the warp stores the rows of complete or left groups
+     constexpr int P = 32 / G;  // rows per store instruction
+     const int sub = (int)lane / G, q = (int)lane % G;
+#pragma unroll
+     for (int w = 0; w < W; ++w) {
+      const bool nf = omask[w] && (mode[w] == WK_DONE || omask[w] == GFULL ||
+                                   (slot[w] & ~I(G - 1)) != obase[w]);
+      for (unsigned fm = __ballot_sync(0xFFFFFFFFu, nf); fm;) {
+        int src = -1;
+#pragma unroll
+        for (int i = 0; i < P; ++i) {  // the sub-th lane left in fm
+          if (i == sub && fm) src = __ffs(fm) - 1;
+          fm &= fm - 1;
+        }
+        const int from = src < 0 ? (int)lane : src;
+        const I gb = __shfl_sync(0xFFFFFFFFu, obase[w], from);
+        const uint32_t gm = __shfl_sync(0xFFFFFFFFu, omask[w], from);
+        if (src >= 0 && ((gm >> q) & 1u) && gb + (I)q < out_cap) {
+          const uint32_t val = sh_row[w * 256 + (threadIdx.x & ~31u) + (unsigned)src][q];
+          if (out32)
+            __stcs(out32 + gb + q, val);
+          else
+            __stcs(rv.out + gb + q, (unsigned long long)widen_node(val));
+        }
+      }
+      if (nf) omask[w] = 0;
+     }
+    }
     bool all_done = true;
 #pragma unroll
     for (int w = 0; w < W; ++w) all_done &= mode[w] == WK_DONE;
@@ -1756,41 +1743,6 @@ __global__ void __launch_bounds__(256, MINB)
         ++slot[w];
         ++pos[w];
         mode[w] = WK_NEW;
-      }
-    }
-    if constexpr (FASTMIN > 0 && COOP && W == 1) {  // ---- stream steps only
-      coop_flush();
-      while (true) {
-        const bool f = mode[0] == WK_NEW && v[0] != NONE &&
-                       slot[0] < min(r_next[0], slot_end[0]) &&
-                       (pos[0] >> 5) == cw[0].wbase && !cw[0].invalid_at(pos[0] + k - 1) &&
-                       (omask[0] == 0 || (slot[0] & ~I(G - 1)) == obase[0]);
-        if (__popc(__ballot_sync(0xFFFFFFFFu, f)) < FASTMIN) break;
-        if (f) {
-          const uint32_t c = cw[0].char_at(pos[0] + k - 1);
-          const I b = block_idx(v[0]);
-          const Block B = load_block_hint(s.blocks0 + (uint64_t)c * s.block_stride + b, pol_last);
-          const uint32_t q = v[0] - b * kBlockBits;
-          if (COUNT) {
-            ++n_block;
-            ++n_stream;
-            ++n_lane;
-          }
-          if (block_bit(B, q)) {
-            const I res = sh_cmap[c] + (I)block_rank(B, q);
-            if (COUNT) ++n_searched;
-            v[0] = res;
-            emit(0, slot[0], res);
-            ++slot[0];
-            ++pos[0];
-          } else {  // no edge at v itself: the group scan in the next full iteration
-            x[0] = v[0] >> 6;
-            ubit[0] = v[0] & 63;
-            mode[0] = WK_SG;
-          }
-        }
-        if (COUNT) n_iter += lane == 0;
-        coop_flush();
       }
     }
   }
@@ -2309,8 +2261,7 @@ static void launch_one_wave(void (*kernel)(KArgs...), int grid, int threads, cud
 // lean walks kernel (1 walk) with staged stores, without and with the
 // one-k-mer filter; 15 = the k-mers kernel with consecutive slots per lane;
 // 16, 17 = 13 staging 8 or 16 slots per store group; 18 = 14 staging 16;
-// 19 = 6 without the filter; 20, 21 = 17 with stream-step-only inner
-// iterations while at least 16 / 24 lanes can take one (FASTMIN).
+// 19 = 6 without the filter.
 // Results never depend on it.
 // Whether launch_search_kernel runs the walks kernel (the only one that can
 // write 32-bit results, ReadsView::out32).
@@ -2411,15 +2362,6 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
       launch_ex(search_walks_kernel<W_, B_, false, true, F_, true, G_>, grid, threads, st, \
                 la, sv, rv, tile_read, ctr);                                               \
   } while (0)
-#define SBWT_LEANSF(B_, F_)                                                                \
-  do {                                                                                     \
-    if (ctr)                                                                               \
-      launch_ex(search_walks_kernel<1, B_, true, true, false, true, 16, F_>, grid, threads, \
-                st, la, sv, rv, tile_read, ctr);                                           \
-    else                                                                                   \
-      launch_ex(search_walks_kernel<1, B_, false, true, false, true, 16, F_>, grid,        \
-                threads, st, la, sv, rv, tile_read, ctr);                                  \
-  } while (0)
 #define SBWT_WALKS(W_, B_)                                                                 \
   do {                                                                                     \
     if (ctr)                                                                               \
@@ -2446,8 +2388,6 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
     else if (kernel_mode == 16) SBWT_LEANSG(1, 5, false, 8);
     else if (kernel_mode == 17) SBWT_LEANSG(1, 6, false, 16);
     else if (kernel_mode == 18) SBWT_LEANSG(1, 5, true, 16);
-    else if (kernel_mode == 20) SBWT_LEANSF(6, 16);
-    else if (kernel_mode == 21) SBWT_LEANSF(6, 24);
     else if (kernel_mode == 14) SBWT_LEANS(1, 5, true);
     else if (kernel_mode == 11 && ctr)
       launch_one_wave(search_kmers_kernel<2, true>,
@@ -2477,7 +2417,6 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
 #undef SBWT_LEAN
 #undef SBWT_LEANS
 #undef SBWT_LEANSG
-#undef SBWT_LEANSF
   } else if (table) {
     if (ctr)
       launch_ex(search_table_kernel<true>, grid, threads, st, la, sv, rv, tile_read, ctr);

@@ -173,8 +173,7 @@ def set_table_kernel(mode: int = TABLE_KERNEL_DEFAULT) -> None:
     walks), 10 the same with 1 walk and a one-k-mer filter, 11/12 k-mers
     kernel with 2/8 k-mers per lane, 13/14 = 8/10 with staged stores,
     15 k-mers kernel over consecutive slots, 16/17 = 13 staging 8/16 slots,
-    18 = 14 staging 16 slots, 19 k-mers kernel without the filter, 20/21 =
-    17 with stream-step-only iterations (at least 16/24 lanes), -1 the
+    18 = 14 staging 16 slots, 19 k-mers kernel without the filter, -1 the
     library default (sbwt_set_table_kernel).  Results never depend on it."""
     check(lib().sbwt_set_table_kernel(int(mode)))
 

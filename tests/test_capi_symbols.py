@@ -37,13 +37,13 @@ def test_version_and_error_without_gpu():
 
 
 def test_table_kernel_mode_range_without_gpu():
-    """Modes 0..21 set the read search kernel (no device call); 22 and above
+    """Modes 0..19 set the read search kernel (no device call); 20 and above
     are SBWT_E_INVALID; a negative mode restores the default."""
     lib = S.lib()
     try:
-        for mode in (0, 7, 17, 21):
+        for mode in (0, 7, 17, 19):
             assert lib.sbwt_set_table_kernel(mode) == 0
-        assert lib.sbwt_set_table_kernel(22) == S.E_INVALID
-        assert b"0..21" in lib.sbwt_last_error()
+        assert lib.sbwt_set_table_kernel(20) == S.E_INVALID
+        assert b"0..19" in lib.sbwt_last_error()
     finally:
         assert lib.sbwt_set_table_kernel(-1) == 0

@@ -18,7 +18,7 @@ DEFAULT_TABLE_KERNEL = S.TABLE_KERNEL_DEFAULT
 # walks kernel as (walks per lane, blocks per SM) = (1, 5), (2, 4), (2, 3),
 # (4, 2), the k-mers kernel, automatic, the lean walks kernel with 1 and 2
 # walks per lane
-KERNEL_MODES = list(range(22))
+KERNEL_MODES = list(range(20))
 
 
 @pytest.fixture(scope="module")

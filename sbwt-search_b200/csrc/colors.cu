@@ -167,14 +167,16 @@ __device__ __forceinline__ void add_sparse(const ColorsView &cv, uint64_t *plane
 // kRowsInFlight at a time.  Counts are sums, so the order and grouping of the
 // adds does not change them.
 // mode 0: pass bitmask + count per read; mode 1: full counts.  WLC: the row
-// words per lane when known at compile time (1: up to 2048 colors), else 0.
-template <int MODE, bool DIRECT, int WLC>
+// words per lane when known at compile time (1: up to 2048 colors), else 0;
+// PC: the counter planes when known (8: reads of at most 255 k-mers), else 0.
+template <int MODE, bool DIRECT, int WLC, int PC>
 __global__ void __launch_bounds__(32 * kColorWarps, kColorBlocksPerSm)
     colors_kernel(ColorsView cv, ColorsJob job, uint32_t *err) {
   constexpr uint32_t FULL = 0xFFFFFFFFu;
   extern __shared__ uint64_t smem[];
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const uint32_t WL = WLC ? (uint32_t)WLC : cv.words_per_lane, P = job.planes, T = cv.tiles;
+  const uint32_t WL = WLC ? (uint32_t)WLC : cv.words_per_lane;
+  const uint32_t P = PC ? (uint32_t)PC : job.planes, T = cv.tiles;
   // per warp: P planes x (32 * WL) words, plane-major so lanes are contiguous,
   // then 32 * WL staging words for the sparse lists
   const uint32_t stride = 32 * WL;
@@ -637,7 +639,7 @@ void ColorsImpl::launch(const u64 *d_vals, const u64 *d_offs, const u64 *d_nf,
   job.tau = tau;
   job.include_not_found = (flags & SBWT_INCLUDE_NOT_FOUND) ? 1 : 0;
   job.include_invalid = (flags & SBWT_INCLUDE_INVALID) ? 1 : 0;
-  job.planes = planes_for(max_kmers);
+  job.planes = planes_for(max_kmers) <= 8 ? 8u : planes_for(max_kmers);
   if (mode == 0 && view.tiles > 1)  // tiles of a read add their passing counts
     SBWT_CUDA(cudaMemsetAsync(d_pass_count, 0, n_reads * 4, st));
   job.pass_bits = d_pass_bits;
@@ -654,15 +656,15 @@ void ColorsImpl::launch(const u64 *d_vals, const u64 *d_offs, const u64 *d_nf,
                                    (int)smem));
     kernel<<<(unsigned)blocks, 32 * kColorWarps, smem, st>>>(view, job, d_err);
   };
-  const bool wl1 = view.words_per_lane == 1;
-  if (mode == 0 && wl1)
-    direct ? go(colors_kernel<0, true, 1>) : go(colors_kernel<0, false, 1>);
+  const bool wl1 = view.words_per_lane == 1, p8 = job.planes == 8;
+  if (mode == 0 && wl1 && p8)
+    direct ? go(colors_kernel<0, true, 1, 8>) : go(colors_kernel<0, false, 1, 8>);
   else if (mode == 0)
-    direct ? go(colors_kernel<0, true, 0>) : go(colors_kernel<0, false, 0>);
-  else if (wl1)
-    direct ? go(colors_kernel<1, true, 1>) : go(colors_kernel<1, false, 1>);
+    direct ? go(colors_kernel<0, true, 0, 0>) : go(colors_kernel<0, false, 0, 0>);
+  else if (wl1 && p8)
+    direct ? go(colors_kernel<1, true, 1, 8>) : go(colors_kernel<1, false, 1, 8>);
   else
-    direct ? go(colors_kernel<1, true, 0>) : go(colors_kernel<1, false, 0>);
+    direct ? go(colors_kernel<1, true, 0, 0>) : go(colors_kernel<1, false, 0, 0>);
   SBWT_CUDA(cudaGetLastError());
 }
 
@@ -692,12 +694,12 @@ void ColorsImpl::enqueue_pseudoalign(const u64 *d_vals, const u64 *d_offs, u64 n
 }
 
 void ColorsImpl::prepare_launch(u64 max_kmers) const {
-  const uint32_t P = planes_for(max_kmers);
+  const uint32_t P = planes_for(max_kmers) <= 8 ? 8u : planes_for(max_kmers);
   const size_t smem = (size_t)kColorWarps * (P + 1) * 32 * view.words_per_lane * 8;
-  for (auto kernel : {colors_kernel<0, true, 1>, colors_kernel<0, false, 1>,
-                      colors_kernel<1, true, 1>, colors_kernel<1, false, 1>,
-                      colors_kernel<0, true, 0>, colors_kernel<0, false, 0>,
-                      colors_kernel<1, true, 0>, colors_kernel<1, false, 0>})
+  for (auto kernel : {colors_kernel<0, true, 1, 8>, colors_kernel<0, false, 1, 8>,
+                      colors_kernel<1, true, 1, 8>, colors_kernel<1, false, 1, 8>,
+                      colors_kernel<0, true, 0, 0>, colors_kernel<0, false, 0, 0>,
+                      colors_kernel<1, true, 0, 0>, colors_kernel<1, false, 0, 0>})
     SBWT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
 }

@@ -113,14 +113,15 @@ __device__ __forceinline__ void add_weighted(uint64_t *planes, uint32_t stride, 
   }
 }
 
-// 2 rows in flight at a 12-blocks-per-SM register budget: 21.9 ms against
-// 23.6 ms for 4 rows at 6 blocks (2 M reads of the 2000-genome workload);
-// more rows in flight cost occupancy and were slower (8 rows: 44-50 ms)
+// 2 rows in flight at a 14-blocks-per-SM register budget (32 registers):
+// 17.6 ms against 17.9 ms at 12 blocks, 19.5 ms for 4 rows at 10 blocks
+// (2 M reads of the 2000-genome workload); more rows in flight cost
+// occupancy and were slower (8 rows: 2x)
 #ifndef SBWT_COLORS_ROWS_IN_FLIGHT
 #define SBWT_COLORS_ROWS_IN_FLIGHT 2
 #endif
 #ifndef SBWT_COLORS_BLOCKS_PER_SM
-#define SBWT_COLORS_BLOCKS_PER_SM 12
+#define SBWT_COLORS_BLOCKS_PER_SM 14
 #endif
 constexpr int kRowsInFlight = SBWT_COLORS_ROWS_IN_FLIGHT;  // dense rows loaded before the adds
 constexpr int kWindows = 4;  // windows of 32 k-mers whose lookups overlap

@@ -1328,7 +1328,7 @@ __device__ __forceinline__ void store_sector_cs(uint64_t *p, uint64_t a, uint64_
 // G: slots staged per walk before they are stored (4, 8 or 16); without
 // LEAN, results leave as 32-byte stores of 4 slots per lane.
 template <int W, int MINB, bool COUNT, bool LEAN = false, bool LFILTER = false,
-          bool LSTAGE = false, int G = 4>
+          bool LSTAGE = false, int G = 4, int KC = 0>
 __global__ void __launch_bounds__(256, MINB)
     search_walks_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
                         unsigned long long *counters) {
@@ -1347,7 +1347,7 @@ __global__ void __launch_bounds__(256, MINB)
   constexpr uint32_t GFULL = (1u << G) - 1u;
   if (threadIdx.x < 4) sh_cmap[threadIdx.x] = (uint32_t)s.c_map[threadIdx.x];
   __syncthreads();
-  const uint32_t k = s.k;
+  const uint32_t k = KC ? (uint32_t)KC : s.k;  // KC: k known at compile time
   const uint32_t lane = threadIdx.x & 31;
   const I n_kmers = (I)(rv.n_kmers_dev ? *rv.n_kmers_dev : rv.n_kmers);
   const I tsize = (I)rv.tile;
@@ -1787,14 +1787,14 @@ constexpr uint64_t kTableL2ResidentBytes = 96ULL << 20;
 // all loads of a lane are independent.  FILT = false skips the filter: every
 // valid k-mer goes to the table (one round trip fewer; for a table that stays
 // in L2 an absent k-mer's probe costs about what its filter word does).
-template <int PER, bool COUNT, bool FILT = true>
+template <int PER, bool COUNT, bool FILT = true, int KC = 0>
 __global__ void __launch_bounds__(256)
     search_kmers_kernel(SbwtView s, ReadsView rv, const uint64_t *__restrict__ tile_read,
                         unsigned long long *counters) {
   using I = uint32_t;
   constexpr I CH = 32 * PER;
   constexpr int MR = 5;  // reads of a chunk resolved from one round of loads
-  const uint32_t k = s.k;
+  const uint32_t k = KC ? (uint32_t)KC : s.k;  // KC: k known at compile time
   const uint32_t lane = threadIdx.x & 31;
   const I n_kmers = (I)(rv.n_kmers_dev ? *rv.n_kmers_dev : rv.n_kmers);
   const I n_reads = (I)rv.n_reads;
@@ -2386,9 +2386,21 @@ static void launch_search_kernel(bool stream, const SbwtView &sv, const ReadsVie
                       grid, threads, st, la, sv, rv, tile_read, ctr);
     else if (kernel_mode == 13) SBWT_LEANS(1, 5, false);
     else if (kernel_mode == 16) SBWT_LEANSG(1, 5, false, 8);
+    else if (kernel_mode == 17 && sv.k == 31 && ctr)
+      launch_ex(search_walks_kernel<1, 6, true, true, false, true, 16, 31>, grid, threads, st,
+                la, sv, rv, tile_read, ctr);
+    else if (kernel_mode == 17 && sv.k == 31)
+      launch_ex(search_walks_kernel<1, 6, false, true, false, true, 16, 31>, grid, threads, st,
+                la, sv, rv, tile_read, ctr);
     else if (kernel_mode == 17) SBWT_LEANSG(1, 6, false, 16);
     else if (kernel_mode == 18) SBWT_LEANSG(1, 5, true, 16);
     else if (kernel_mode == 14) SBWT_LEANS(1, 5, true);
+    else if (kernel_mode == 11 && sv.k == 31 && ctr)
+      launch_one_wave(search_kmers_kernel<2, true, true, 31>,
+                      grid, threads, st, la, sv, rv, tile_read, ctr);
+    else if (kernel_mode == 11 && sv.k == 31)
+      launch_one_wave(search_kmers_kernel<2, false, true, 31>,
+                      grid, threads, st, la, sv, rv, tile_read, ctr);
     else if (kernel_mode == 11 && ctr)
       launch_one_wave(search_kmers_kernel<2, true>,
                       grid, threads, st, la, sv, rv, tile_read, ctr);

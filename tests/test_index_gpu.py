@@ -394,3 +394,38 @@ def test_table_kernel_device_pointers_and_capacity(kernel, shift):
     assert (got[:shift] == -7).all()
     assert np.array_equal(got[shift:shift + len(exp)].view(np.uint64), exp)
     assert (got[shift + len(exp):] == -7).all()
+
+
+@pytest.mark.parametrize("kernel", [DEFAULT_TABLE_KERNEL, 1, 11, 17])
+def test_device_pointers_bad_read_ends(kernel):
+    """Device-pointer calls queue the search right after the scan, with no
+    host check in between: read ends that decrease or pass n_chars scan to
+    zero k-mers, nothing is written, the call returns SBWT_E_INVALID, and the
+    next call on the handle is unaffected."""
+    import torch
+    g, path, sb = synthetic(4, 2, 4000, 31, 1, 0.02)
+    idx = S.SbwtIndex.open(path)
+    assert idx.set_kmer_table(True) > 0
+    chars, ends = mixed_reads(g, 21, 3000)
+    exp = oracle_results(oracle_index(path, 8), chars, ends)
+    d_chars = torch.from_numpy(chars.copy()).cuda()
+    decreasing = ends.copy()
+    decreasing[len(ends) // 2] = decreasing[len(ends) // 2 - 1] - 1
+    past_end = ends.copy()
+    past_end[-1] = len(chars) + 100
+    S.set_table_kernel(kernel)
+    try:
+        for bad in (decreasing, past_end):
+            d_bad = torch.from_numpy(bad.view(np.int64).copy()).cuda()
+            out = torch.full((len(exp) + 8,), -7, dtype=torch.int64, device="cuda")
+            with pytest.raises(S.SbwtError) as e:
+                idx.search_reads(d_chars, d_bad, out=out)
+            assert e.value.code == S.E_INVALID
+            assert (out.cpu().numpy() == -7).all()
+        d_ends = torch.from_numpy(ends.view(np.int64).copy()).cuda()
+        out = torch.empty(len(exp), dtype=torch.int64, device="cuda")
+        assert idx.search_reads(d_chars, d_ends, out=out) == len(exp)
+        assert np.array_equal(out.cpu().numpy().view(np.uint64), exp)
+    finally:
+        S.set_table_kernel(DEFAULT_TABLE_KERNEL)
+    idx.close()

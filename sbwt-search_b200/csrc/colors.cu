@@ -124,7 +124,10 @@ __device__ __forceinline__ void add_weighted(uint64_t *planes, uint32_t stride, 
 #define SBWT_COLORS_BLOCKS_PER_SM 14
 #endif
 constexpr int kRowsInFlight = SBWT_COLORS_ROWS_IN_FLIGHT;  // dense rows loaded before the adds
-constexpr int kWindows = 4;  // windows of 32 k-mers whose lookups overlap
+#ifndef SBWT_COLORS_WINDOWS
+#define SBWT_COLORS_WINDOWS 4
+#endif
+constexpr int kWindows = SBWT_COLORS_WINDOWS;  // windows of 32 k-mers whose lookups overlap
 constexpr int kColorBlocksPerSm = SBWT_COLORS_BLOCKS_PER_SM;
 
 // Adds m copies of the sparse color list sparse[start, start + len) to this

@@ -1631,7 +1631,7 @@ __global__ void __launch_bounds__(256, MINB)
       } else if (mode[w] == WK_HASH) {
         A[w] = load_block_hint(reinterpret_cast<const Block *>(s.kmer_table + 2 * (uint64_t)hslot[w]),
                                pol_first);
-      } else if (mode[w] == WK_FILTER) {
+      } else if ((!LEAN || LFILTER) && mode[w] == WK_FILTER) {  // no filter: never
         uint64_t z = kmer_mix(cw[w].prefix(pos[w], k));
         fz[w] = z;
         A[w].w0 = load_u64_hint(s.kmer_filter + kmer_filter_word(z, s.filter_words), pol_first);
@@ -1671,7 +1671,7 @@ __global__ void __launch_bounds__(256, MINB)
 #pragma unroll
     for (int w = 0; w < W; ++w) {
       const uint32_t md = mode[w];
-      if (md == WK_FILTER) {
+      if ((!LEAN || LFILTER) && md == WK_FILTER) {
         // k-mers the filter rejects are absent; the first it passes is looked up
         uint32_t j = 0;
         for (; j < nb[w]; ++j) {

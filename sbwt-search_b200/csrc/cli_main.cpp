@@ -19,6 +19,8 @@
 // stream through the host reader in batches of 256 M chars.
 #include <cuda_runtime.h>
 
+#include <sys/stat.h>
+
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -154,16 +156,95 @@ u64 device_text_budget(int device) {
   return (u64)(0.8 * (double)free_b / 40.0);
 }
 
+struct Event {
+  cudaEvent_t e = nullptr;
+  Event() { check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)); }
+  ~Event() { cudaEventDestroy(e); }
+};
+
+// Host <-> device streaming through two pinned buffers of kStageBytes: one is
+// filled (or written out) by the host while the other's copy runs, so no
+// pinned buffer of the whole file or output is allocated.
+constexpr u64 kStageBytes = 64ULL << 20;
+struct Staging {
+  HostMem buf[2]{HostMem(kStageBytes), HostMem(kStageBytes)};
+  Event done[2];
+};
+
+// The size of a plain (not gzip) file, or -1 (gzip, unreadable).
+long long plain_file_size(const std::string &path) {
+  FILE *f = std::fopen(path.c_str(), "rb");
+  if (!f) return -1;
+  unsigned char m[2] = {0, 0};
+  const size_t got = std::fread(m, 1, 2, f);
+  std::fclose(f);
+  if (got == 2 && m[0] == 0x1f && m[1] == 0x8b) return -1;
+  struct stat st{};
+  if (::stat(path.c_str(), &st) != 0) return -1;
+  return (long long)st.st_size;
+}
+
+// Reads a plain file of n bytes into d_text (device), chunk by chunk.
+void read_file_to_device(const std::string &path, u64 n, char *d_text, Staging &sg,
+                         cudaStream_t st) {
+  FILE *f = std::fopen(path.c_str(), "rb");
+  if (!f) throw std::runtime_error("Unable to open file " + path);
+  u64 off = 0;
+  for (int i = 0; off < n; ++i) {
+    const int b = i & 1;
+    if (i >= 2) check_cuda(cudaEventSynchronize(sg.done[b].e));  // its last copy is done
+    const u64 len = std::min<u64>(kStageBytes, n - off);
+    if (std::fread(sg.buf[b].p, 1, len, f) != len) {
+      std::fclose(f);
+      throw std::runtime_error("read error in sequence file");
+    }
+    check_cuda(cudaMemcpyAsync(d_text + off, sg.buf[b].p, len, cudaMemcpyHostToDevice, st));
+    check_cuda(cudaEventRecord(sg.done[b].e, st));
+    off += len;
+  }
+  std::fclose(f);
+}
+
+// Writes nb device bytes to w, chunk by chunk (the copy of chunk i runs
+// while chunk i - 1 is written).
+void write_device_bytes(const char *d_bytes, u64 nb, IndexResultsWriter &w, Staging &sg,
+                        cudaStream_t st) {
+  u64 prev_len = 0;
+  int prev = -1;
+  for (u64 off = 0, i = 0; off < nb; ++i) {
+    const int b = (int)(i & 1);
+    const u64 len = std::min<u64>(kStageBytes, nb - off);
+    check_cuda(cudaMemcpyAsync(sg.buf[b].p, d_bytes + off, len, cudaMemcpyDeviceToHost, st));
+    check_cuda(cudaEventRecord(sg.done[b].e, st));
+    if (prev >= 0) {
+      check_cuda(cudaEventSynchronize(sg.done[prev].e));
+      w.write_raw(static_cast<const char *>(sg.buf[prev].p), prev_len);
+    }
+    prev = b;
+    prev_len = len;
+    off += len;
+  }
+  if (prev >= 0) {
+    check_cuda(cudaEventSynchronize(sg.done[prev].e));
+    w.write_raw(static_cast<const char *>(sg.buf[prev].p), prev_len);
+  }
+}
+
 // One whole query text through the GPU: parse, search, format; the formatted
-// bytes are appended to w.
+// bytes are appended to w.  The text is either in host memory (`text`) or
+// read from the plain file `path` of n bytes.
 void index_text_on_device(sbwt_index_t *ix, const sbwt_index_info_t &info, uint32_t flags,
-                          const std::vector<char> &text, int format, IndexResultsWriter &w) {
-  const u64 n = text.size();
+                          const std::vector<char> *text, const std::string &path, u64 n,
+                          int format, IndexResultsWriter &w) {
   if (n == 0) return;
   Stream st;
+  Staging sg;
   const uint32_t dp = SBWT_DEVICE_POINTERS;
   DevMem d_text(n), d_chars(n);
-  check_cuda(cudaMemcpyAsync(d_text.p, text.data(), n, cudaMemcpyHostToDevice, st.s));
+  if (text)
+    check_cuda(cudaMemcpyAsync(d_text.p, text->data(), n, cudaMemcpyHostToDevice, st.s));
+  else
+    read_file_to_device(path, n, d_text.get<char>(), sg, st.s);
   u64 nc = 0, nr = 0;
   int rc = sbwt_fastx_parse(d_text.get<char>(), n, d_chars.get<char>(), n, nullptr, 0, &nc,
                             &nr, dp, info.device, st.s);
@@ -183,10 +264,7 @@ void index_text_on_device(sbwt_index_t *ix, const sbwt_index_info_t &info, uint3
   DevMem d_out(nb);
   check(sbwt_format_index_results(d_res.get<u64>(), d_ends.get<u64>(), nr, info.k, format,
                                   d_out.get<char>(), nb, &nb, dp, info.device, st.s));
-  HostMem h_out(nb);
-  check_cuda(cudaMemcpyAsync(h_out.p, d_out.p, nb, cudaMemcpyDeviceToHost, st.s));
-  check_cuda(cudaStreamSynchronize(st.s));
-  w.write_raw(static_cast<const char *>(h_out.p), nb);
+  write_device_bytes(d_out.get<char>(), nb, w, sg, st.s);
 }
 
 int run_index(const Args &a) {
@@ -219,6 +297,14 @@ int run_index(const Args &a) {
   std::vector<u64> results;
   std::vector<char> text;
   for (size_t f = 0; f < ins.size(); ++f) {
+    // a plain file that fits goes to the device as it is read; a gzip file
+    // that fits is inflated on the host first
+    const long long plain = plain_file_size(ins[f]);
+    if (plain >= 0 && (u64)plain <= budget) {
+      IndexResultsWriter w(outs[f], fmt, headers);
+      index_text_on_device(ix, info, flags, nullptr, ins[f], (u64)plain, format, w);
+      continue;
+    }
     bool whole = false;
     try {
       whole = read_whole_file(ins[f], budget, text);
@@ -228,7 +314,7 @@ int run_index(const Args &a) {
     }
     if (whole) {
       IndexResultsWriter w(outs[f], fmt, headers);
-      index_text_on_device(ix, info, flags, text, format, w);
+      index_text_on_device(ix, info, flags, &text, std::string(), text.size(), format, w);
       continue;
     }
     text = std::vector<char>();

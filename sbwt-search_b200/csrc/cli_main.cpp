@@ -146,15 +146,33 @@ struct Stream {
   ~Stream() { cudaStreamDestroy(s); }
 };
 
-// Largest query text handled on the device in one piece: text, chars, read
-// ends, one u64 result and up to 22 formatted bytes per char stay within 80 %
-// of the free device memory.
+// Largest query text handled on the device in one piece: per char of text at
+// most 33 bytes stay within 80 % of the free device memory (text and chars
+// 1 each, read ends 8 per read and a read takes at least 4 chars of text,
+// one u64 result per k-mer, at most 21 formatted bytes per k-mer).
 u64 device_text_budget(int device) {
   size_t free_b = 0, total_b = 0;
   check_cuda(cudaSetDevice(device));
   check_cuda(cudaMemGetInfo(&free_b, &total_b));
-  return (u64)(0.8 * (double)free_b / 40.0);
+  return (u64)(0.8 * (double)free_b / 33.0);
 }
+
+// A device buffer that grows to the largest size asked for.
+struct GrowMem {
+  void *p = nullptr;
+  u64 cap = 0;
+  ~GrowMem() { cudaFree(p); }
+  template <class T>
+  T *get(u64 n) {
+    if (n > cap || !p) {
+      cudaFree(p);
+      p = nullptr;
+      check_cuda(cudaMalloc(&p, n ? n : 1));
+      cap = n;
+    }
+    return static_cast<T *>(p);
+  }
+};
 
 struct Event {
   cudaEvent_t e = nullptr;
@@ -267,6 +285,35 @@ void index_text_on_device(sbwt_index_t *ix, const sbwt_index_info_t &info, uint3
   write_device_bytes(d_out.get<char>(), nb, w, sg, st.s);
 }
 
+// One host-parsed batch (chars and cumulative read ends) through the GPU:
+// search, format, and the formatted bytes appended to w.
+struct DeviceBatch {
+  GrowMem chars, ends, res, out;
+};
+void index_batch_on_device(sbwt_index_t *ix, const sbwt_index_info_t &info, uint32_t flags,
+                           const ReadBatch &b, int format, IndexResultsWriter &w,
+                           DeviceBatch &db, Staging &sg, cudaStream_t st) {
+  const u64 nc = b.chars.size(), nr = b.ends.size();
+  if (nr == 0) return;
+  const uint32_t dp = SBWT_DEVICE_POINTERS;
+  char *d_chars = db.chars.get<char>(nc + 16);
+  u64 *d_ends = db.ends.get<u64>(nr * 8);
+  check_cuda(cudaMemcpyAsync(d_chars, b.chars.data(), nc, cudaMemcpyHostToDevice, st));
+  check_cuda(cudaMemcpyAsync(d_ends, b.ends.data(), nr * 8, cudaMemcpyHostToDevice, st));
+  const u64 cap = std::max<u64>(nc, 1);
+  u64 *d_res = db.res.get<u64>(cap * 8);
+  u64 nk = 0;
+  check(sbwt_search_reads(ix, d_chars, nc, d_ends, nr, d_res, cap, &nk, flags | dp, st));
+  u64 nb = 0;
+  const int rc = sbwt_format_index_results(d_res, d_ends, nr, info.k, format, nullptr, 0, &nb,
+                                           dp, info.device, st);
+  if (rc != SBWT_E_CAPACITY) check(rc);
+  char *d_out = db.out.get<char>(nb);
+  check(sbwt_format_index_results(d_res, d_ends, nr, info.k, format, d_out, nb, &nb, dp,
+                                  info.device, st));
+  write_device_bytes(d_out, nb, w, sg, st);
+}
+
 int run_index(const Args &a) {
   if (a.flags.count("help")) {
     std::printf("%s", kIndexHelp);
@@ -294,7 +341,6 @@ int run_index(const Args &a) {
   const u64 batch_chars = 256ULL << 20;
   const int format = fmt == IndexFormat::Ascii ? 0 : fmt == IndexFormat::Binary ? 1 : 2;
   const u64 budget = device_text_budget(info.device);
-  std::vector<u64> results;
   std::vector<char> text;
   for (size_t f = 0; f < ins.size(); ++f) {
     // a plain file that fits goes to the device as it is read; a gzip file
@@ -317,19 +363,19 @@ int run_index(const Args &a) {
       index_text_on_device(ix, info, flags, &text, std::string(), text.size(), format, w);
       continue;
     }
+    // larger than one device piece: parsed on the host batch by batch, each
+    // batch searched and formatted on the device
     text = std::vector<char>();
     std::unique_ptr<FastxReader> rd = std::make_unique<FastxReader>(ins[f]);
     IndexResultsWriter w(outs[f], fmt, headers);
+    Stream st;
+    Staging sg;
+    DeviceBatch db;
     ReadBatch b;
     while (true) {
       b.clear();
       if (!rd->next_batch(b, batch_chars, ~0ULL)) break;
-      const u64 nk = sbwt_count_kmers(b.ends.data(), b.ends.size(), info.k);
-      results.resize(std::max<u64>(nk, 1));
-      u64 n = 0;
-      check(sbwt_search_reads(ix, b.chars.data(), b.chars.size(), b.ends.data(), b.ends.size(),
-                              results.data(), results.size(), &n, flags, nullptr));
-      w.write(results.data(), b.ends.data(), b.ends.size(), info.k);
+      index_batch_on_device(ix, info, flags, b, format, w, db, sg, st.s);
     }
   }
   sbwt_index_free(ix);

@@ -150,11 +150,16 @@ struct Stream {
 // most 33 bytes stay within 80 % of the free device memory (text and chars
 // 1 each, read ends 8 per read and a read takes at least 4 chars of text,
 // one u64 result per k-mer, at most 21 formatted bytes per k-mer).
+// SBWT_CLI_DEVICE_PIECE_BYTES (environment) lowers it, e.g. to test the
+// batched path on small files.
 u64 device_text_budget(int device) {
   size_t free_b = 0, total_b = 0;
   check_cuda(cudaSetDevice(device));
   check_cuda(cudaMemGetInfo(&free_b, &total_b));
-  return (u64)(0.8 * (double)free_b / 33.0);
+  u64 b = (u64)(0.8 * (double)free_b / 33.0);
+  if (const char *e = std::getenv("SBWT_CLI_DEVICE_PIECE_BYTES"))
+    b = std::min<u64>(b, std::strtoull(e, nullptr, 10));
+  return b;
 }
 
 // A device buffer that grows to the largest size asked for.

@@ -1,6 +1,7 @@
 """The reference-compatible CLI (`sbwt_search index|colors`) end to end on
 the GPU: the reference's own index fixtures reproduce byte for byte, and the
 colors step matches the oracle."""
+import os
 import struct
 import subprocess
 
@@ -16,8 +17,8 @@ pytestmark = pytest.mark.gpu
 CLI = str(S.HERE / "_build" / "sbwt_search")
 
 
-def run(*args):
-    r = subprocess.run([CLI, *map(str, args)], capture_output=True, text=True)
+def run(*args, env=None):
+    r = subprocess.run([CLI, *map(str, args)], capture_output=True, text=True, env=env)
     assert r.returncode == 0, r.stdout + r.stderr
     return r
 
@@ -44,13 +45,20 @@ def decode_index_file(path, mode):
     return rows
 
 
+@pytest.mark.parametrize("piece", [None, "1"])
 @pytest.mark.parametrize("mode", ["ascii", "binary", "bool"])
-def test_index_cli_on_reference_fixtures(mode, tmp_path):
+def test_index_cli_on_reference_fixtures(mode, piece, tmp_path):
+    """piece "1": every query file is larger than the device piece, so the
+    CLI parses it on the host in batches and searches and formats each batch
+    on the device; None: whole files go to the device as they are read."""
     ins = tmp_path / "in.list"
     outs = tmp_path / "out.list"
     ins.write_text("\n".join(str(GOLDEN / "index_search" / n) for n in FIXTURE_FILES) + "\n")
     outs.write_text("\n".join(str(tmp_path / n.split(".")[0]) for n in FIXTURE_FILES) + "\n")
-    run("index", "-i", golden_sbwt_path(), "-q", ins, "-o", outs, "-p", mode)
+    env = None
+    if piece is not None:
+        env = dict(os.environ, SBWT_CLI_DEVICE_PIECE_BYTES=piece)
+    run("index", "-i", golden_sbwt_path(), "-q", ins, "-o", outs, "-p", mode, env=env)
     ext = {"ascii": ".txt", "binary": ".bin", "bool": ".bool"}[mode]
     for n in FIXTURE_FILES:
         stem = n.split(".")[0]

@@ -1910,10 +1910,9 @@ __global__ void __launch_bounds__(256)
     // table probes of the keys the filter passed, one round of loads at a time
     while (true) {
       bool any = false;
-      Block A[PER];
+      Block A[PER];  // read only where look[t]
 #pragma unroll
       for (int t = 0; t < PER; ++t) {
-        A[t] = Block{0, 0, 0, 0};
         if (look[t]) {
           A[t] = load_block_hint(
               reinterpret_cast<const Block *>(s.kmer_table + 2 * (uint64_t)hs[t]), pol_table);

@@ -3,6 +3,7 @@
 #include <cstring>
 #include <fstream>
 #include <stdexcept>
+#include <thread>
 
 #include "../../include/sbwt_b200.h"
 #include "host_io.hpp"
@@ -168,6 +169,48 @@ void ColorResultsWriter::write_raw(const char *bytes, u64 n) {
   if (n && std::fwrite(bytes, 1, n, f_) != n) throw std::runtime_error("write failed");
 }
 
+// The ascii body of an index results file, bytes [a, b) (whole lines, or the
+// file's unterminated tail): found values back to back and per read its
+// found count, -1 count and -2 count; a read ends at '\n', and an
+// unterminated tail with tokens is one more read.
+struct AsciiPart {
+  std::vector<u64> found, n_found, nf, inv;
+};
+static void parse_ascii_part(const char *data, size_t a, size_t b, AsciiPart &o) {
+  u64 nf = 0, inv = 0, f0 = 0;
+  bool open_read = false;
+  auto end_read = [&]() {
+    o.n_found.push_back(o.found.size() - f0);
+    o.nf.push_back(nf);
+    o.inv.push_back(inv);
+    f0 = o.found.size();
+    nf = inv = 0;
+  };
+  size_t i = a;
+  while (i < b) {
+    const char c = data[i];
+    if (c == '\n') {
+      end_read();
+      open_read = false;
+      ++i;
+    } else if (c == '-') {  // -1 / -2 (other negatives are skipped)
+      if (i + 1 < b && data[i + 1] == '1') ++nf;
+      else if (i + 1 < b && data[i + 1] == '2') ++inv;
+      ++i;
+      while (i < b && data[i] >= '0') ++i;
+      open_read = true;
+    } else if (c >= '0' && c <= '9') {
+      u64 v = 0;
+      while (i < b && data[i] >= '0' && data[i] <= '9') v = v * 10 + (u64)(data[i++] - '0');
+      o.found.push_back(v);
+      open_read = true;
+    } else {
+      ++i;
+    }
+  }
+  if (open_read) end_read();  // only the file's last part can end inside a read
+}
+
 IndexResults read_index_results(const std::string &path) {
   std::ifstream in(path, std::ios::binary);
   if (!in) throw std::runtime_error("Unable to open file " + path);
@@ -183,7 +226,14 @@ IndexResults read_index_results(const std::string &path) {
   if (fmt != "ascii" && fmt != "binary")
     throw std::runtime_error("Unknown index file format '" + fmt + "'");
   if (get_str() != "v1.0") throw std::runtime_error("The file has an incompatible version number");
-  std::vector<char> data((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+  // the body in one read (its size from the stream's end)
+  const std::streampos body = in.tellg();
+  in.seekg(0, std::ios::end);
+  const std::streamoff n_body = in.tellg() - body;
+  in.seekg(body);
+  std::vector<char> data((size_t)std::max<std::streamoff>(n_body, 0));
+  if (!data.empty() && !in.read(data.data(), (std::streamsize)data.size()))
+    throw std::runtime_error("read error in index results file");
   IndexResults out;
   out.offsets.push_back(0);
   u64 nf = 0, inv = 0;
@@ -195,29 +245,41 @@ IndexResults read_index_results(const std::string &path) {
   };
   bool open_read = false;
   if (fmt == "ascii") {
-    size_t i = 0;
+    // parts of whole lines parsed on host threads, then joined in order
     const size_t n = data.size();
-    while (i < n) {
-      const char c = data[i];
-      if (c == '\n') {
-        end_read();
-        open_read = false;
-        ++i;
-      } else if (c == '-') {  // -1 / -2 (other negatives are skipped)
-        if (i + 1 < n && data[i + 1] == '1') ++nf;
-        else if (i + 1 < n && data[i + 1] == '2') ++inv;
-        ++i;
-        while (i < n && data[i] >= '0') ++i;
-        open_read = true;
-      } else if (c >= '0' && c <= '9') {
-        u64 v = 0;
-        while (i < n && data[i] >= '0' && data[i] <= '9') v = v * 10 + (u64)(data[i++] - '0');
-        out.found.push_back(v);
-        open_read = true;
-      } else {
-        ++i;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t T = std::min<size_t>(std::min<size_t>(hw, 32), std::max<size_t>(n >> 24, 1));
+    std::vector<size_t> cut(T + 1, n);
+    cut[0] = 0;
+    for (size_t t = 1; t < T; ++t) {  // just past a newline at or after n * t / T
+      size_t c = std::max(cut[t - 1], n * t / T);
+      while (c < n && data[c] != '\n') ++c;
+      cut[t] = c < n ? c + 1 : n;
+    }
+    std::vector<AsciiPart> parts(T);
+    std::vector<std::thread> th;
+    for (size_t t = 1; t < T; ++t)
+      th.emplace_back(parse_ascii_part, data.data(), cut[t], cut[t + 1], std::ref(parts[t]));
+    parse_ascii_part(data.data(), cut[0], cut[1], parts[0]);
+    for (auto &x : th) x.join();
+    size_t n_found = 0, n_reads = 0;
+    for (const auto &q : parts) {
+      n_found += q.found.size();
+      n_reads += q.nf.size();
+    }
+    out.found.reserve(n_found);
+    out.offsets.reserve(n_reads + 1);
+    out.not_found.reserve(n_reads);
+    out.invalid.reserve(n_reads);
+    for (auto &q : parts) {
+      out.found.insert(out.found.end(), q.found.begin(), q.found.end());
+      for (size_t r = 0; r < q.nf.size(); ++r) {
+        out.offsets.push_back(out.offsets.back() + q.n_found[r]);
+        out.not_found.push_back(q.nf[r]);
+        out.invalid.push_back(q.inv[r]);
       }
     }
+    return out;
   } else {
     const size_t nw = data.size() / 8;
     for (size_t w = 0; w < nw; ++w) {

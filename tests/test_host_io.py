@@ -141,3 +141,56 @@ def test_fastx_reader_matches_oracle_on_random_text(seed, tmp_path):
     reads = O.parse_fastx(text)
     assert chars == b"".join(reads)
     assert ends.tolist() == np.cumsum([len(r) for r in reads]).tolist()
+
+
+@pytest.mark.parametrize("tail_newline", [True, False])
+def test_index_file_reader_large_file_in_parts(tail_newline):
+    """A file over 16 MB is parsed in parts of whole lines on host threads:
+    the joined result equals the rows written (values, -1 and -2 counts,
+    empty rows, and an unterminated last row)."""
+    rng = np.random.default_rng(5)
+    n_rows = 600_000
+    lens = rng.integers(0, 40, n_rows)
+    lens[rng.random(n_rows) < 0.05] = 0
+    lens[-2] = 0
+    if tail_newline:
+        lens[-1] = 0  # trailing empty rows
+    vals = rng.integers(0, 1 << 40, int(lens.sum()))
+    kinds = rng.random(len(vals))
+    vals[kinds < 0.1] = -1
+    vals[(kinds >= 0.1) & (kinds < 0.15)] = -2
+    starts = np.concatenate([[0], np.cumsum(lens)])
+    lines = [" ".join(map(str, vals[starts[r]:starts[r + 1]])) for r in range(n_rows)]
+    if not tail_newline:
+        lines[-1] = lines[-1] or "5"
+    body = "\n".join(lines) + ("\n" if tail_newline else "")
+    path = TMP / f"big_index_results_{int(tail_newline)}.txt"
+    path.write_bytes(struct.pack("<Q", 5) + b"ascii" + struct.pack("<Q", 4) + b"v1.0" +
+                     body.encode())
+    assert path.stat().st_size > 40 << 20  # several parts
+    L = lib()
+    ptrs = [C.c_void_p() for _ in range(4)]
+    n = C.c_uint64()
+    S.check(L.sbwt_read_index_results(str(path).encode(), *[C.byref(p) for p in ptrs],
+                                      C.byref(n)))
+    try:
+        assert n.value == n_rows
+        offs = np.ctypeslib.as_array(C.cast(ptrs[1], U64P), (n_rows + 1,)).copy()
+        found = np.ctypeslib.as_array(C.cast(ptrs[0], U64P), (max(int(offs[-1]), 1),))
+        nf = np.ctypeslib.as_array(C.cast(ptrs[2], U64P), (n_rows,))
+        inv = np.ctypeslib.as_array(C.cast(ptrs[3], U64P), (n_rows,))
+        if not tail_newline and lens[-1] == 0:
+            lens = lens.copy()
+            lens[-1] = 1
+            vals = np.concatenate([vals, [5]])
+        pos = vals >= 0
+        row = np.repeat(np.arange(n_rows), lens)
+        exp_found_per_row = np.bincount(row[pos], minlength=n_rows)
+        exp_nf = np.bincount(row[vals == -1], minlength=n_rows)
+        exp_inv = np.bincount(row[vals == -2], minlength=n_rows)
+        assert np.array_equal(np.diff(offs), exp_found_per_row)
+        assert np.array_equal(nf, exp_nf) and np.array_equal(inv, exp_inv)
+        assert np.array_equal(found[:int(offs[-1])], vals[pos].astype(np.uint64))
+    finally:
+        for p in ptrs:
+            L.sbwt_free(p)

@@ -298,6 +298,59 @@ def bench_batched_full(args, idx, S, torch, dev):
                       "chars assembled on the device outside the timed calls"}
 
 
+def colors_cli_file_to_file(sp, cp, chars, ends, tau, tmpdir):
+    """The reference's two command lines on all reads of the colors workload,
+    file to file: `sbwt_search index` (FASTQ -> ascii index results) then
+    `sbwt_search colors` (index results -> ascii color ids), each timed with
+    its process start and index load (an empty query measures those)."""
+    cli = str(REPO / "sbwt-search_b200" / "_build" / "sbwt_search")
+    fq = os.path.join(tmpdir, "colors_reads.fq")
+    with open(fq, "wb") as f:
+        for lo in range(0, len(ends), 1_000_000):
+            hi = min(len(ends), lo + 1_000_000)
+            base = int(ends[lo - 1]) if lo else 0
+            f.write(fastq_text(chars[base:int(ends[hi - 1])], ends[lo:hi] - base).tobytes())
+    idx_out, col_out = os.path.join(tmpdir, "colors_idx"), os.path.join(tmpdir, "colors_ids")
+    empty = os.path.join(tmpdir, "colors_empty.fq")
+    open(empty, "wb").close()
+
+    def timed(argv):
+        t0 = time.perf_counter()
+        r = subprocess.run([cli, *argv], capture_output=True)
+        return time.perf_counter() - t0, r.returncode
+
+    t_idx_load, rc0 = timed(["index", "-i", sp, "-q", empty, "-o", idx_out + "_e"])
+    t_idx, rc1 = timed(["index", "-i", sp, "-q", fq, "-o", idx_out])
+    idx_bytes = os.path.getsize(idx_out + ".txt") if rc1 == 0 else 0
+    os.remove(fq)
+    # the colors step's empty query: an index results file of no reads
+    with open(idx_out + "_e.txt", "rb") as f:
+        hdr = f.read()
+    with open(os.path.join(tmpdir, "colors_empty_idx.txt"), "wb") as f:
+        f.write(hdr)
+    t_col_load, rc2 = timed(["colors", "-k", cp, "-q", os.path.join(tmpdir, "colors_empty_idx.txt"),
+                             "-o", col_out + "_e", "-t", str(tau)])
+    t_col, rc3 = timed(["colors", "-k", cp, "-q", idx_out + ".txt", "-o", col_out, "-t",
+                        str(tau)])
+    col_bytes = os.path.getsize(col_out + ".txt") if rc3 == 0 else 0
+    for x in (idx_out + ".txt", col_out + ".txt"):
+        try:
+            os.remove(x)
+        except OSError:
+            pass
+    n = len(ends)
+    return {"commands": "sbwt_search index -i <colors .sbwt> -q <reads FASTQ> -o <idx>; "
+                        "sbwt_search colors -k <.tcolors> -q <idx>.txt -o <ids> -t 0.7 "
+                        "(ascii in and out)",
+            "reads": int(n), "rc": [rc0, rc1, rc2, rc3],
+            "index_results_bytes": int(idx_bytes), "color_ids_bytes": int(col_bytes),
+            "index_step_s": t_idx, "index_step_load_s": t_idx_load,
+            "colors_step_s": t_col, "colors_step_load_s": t_col_load,
+            "reads_per_s_both_steps_file_to_file":
+                n / max(t_idx - t_idx_load + t_col - t_col_load, 1e-9),
+            "reads_per_s_both_steps_incl_loads": n / max(t_idx + t_col, 1e-9)}
+
+
 def bench_colors_and_serving(args, S, torch, dev, tmpdir, rank, resident_index=None):
     """Pseudoalignment reads/s (colors step, device-resident), the fused
     reads -> colors pipeline (host in, host out), the CPU oracle on a sample,
@@ -448,6 +501,12 @@ def bench_colors_and_serving(args, S, torch, dev, tmpdir, rank, resident_index=N
                   "plain": "the reference's flow: per batch of 100000 reads the R x C counts "
                            "(sbwt_color_counts) copied to the host, threshold on the host",
                   "fused": "sbwt_pseudoalign: counts and threshold on the device, sorted ids"}}
+    if args.cli_full:
+        try:  # never lets this extra run take the bench line down
+            colors["cli_file_to_file"] = colors_cli_file_to_file(sp, cp, chars, ends, c["tau"],
+                                                                 tmpdir)
+        except Exception as e:  # reported, not raised
+            colors["cli_file_to_file"] = {"error": repr(e)}
     del d_res, d_found, d_ids, found_mask, res2
     torch.cuda.empty_cache()
     # fused reads -> colors pipeline from host memory (CUDA graph per batch)

@@ -420,8 +420,8 @@ int run_colors(const Args &a) {
       continue;
     }
     const u64 n = r.not_found.size();
-    std::vector<u64> offs(n + 1, 0);
-    std::vector<uint32_t> ids(std::max<u64>(r.found.size(), 1));
+    U64Array offs(n + 1);
+    std::vector<uint32_t, NoInitAlloc<uint32_t>> ids(std::max<u64>(r.found.size(), 1));
     int rc = sbwt_pseudoalign(ci, r.found.data(), r.offsets.data(), r.not_found.data(),
                               r.invalid.data(), n, tau, flags, ids.data(), ids.size(),
                               offs.data(), nullptr);

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace sbwt {
@@ -97,10 +98,32 @@ class ColorResultsWriter {
 // (src/IndexFileParser/AsciiIndexFileParser.cpp:33-98,
 //  BinaryIndexFileParser.cpp:33-69): per read the found indexes, and the
 // counts of -1 and -2 tokens.
+// A vector whose resize leaves new elements uninitialised (they are all
+// written next), so multi-GB result arrays are not cleared first.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <class U>
+  NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
+  template <class U>
+  void construct(U *p) noexcept {
+    ::new (static_cast<void *>(p)) U;
+  }
+  template <class U, class... A>
+  void construct(U *p, A &&...a) {
+    ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
+  }
+};
+using U64Array = std::vector<u64, NoInitAlloc<u64>>;
+
 struct IndexResults {
-  std::vector<u64> found;    // all reads back to back
-  std::vector<u64> offsets;  // n_reads + 1
-  std::vector<u64> not_found, invalid;
+  U64Array found;    // all reads back to back
+  U64Array offsets;  // n_reads + 1
+  U64Array not_found, invalid;
 };
 IndexResults read_index_results(const std::string &path);
 

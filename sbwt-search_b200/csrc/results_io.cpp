@@ -2,6 +2,9 @@
 #include <charconv>
 #include <cstring>
 #include <fstream>
+#include <unistd.h>
+
+#include <atomic>
 #include <stdexcept>
 #include <thread>
 
@@ -170,70 +173,91 @@ void ColorResultsWriter::write_raw(const char *bytes, u64 n) {
 }
 
 // The ascii body of an index results file, bytes [a, b) (whole lines, or the
-// file's unterminated tail): found values back to back and per read its
-// found count, -1 count and -2 count; a read ends at '\n', and an
-// unterminated tail with tokens is one more read.
-struct AsciiPart {
-  std::vector<u64> found, n_found, nf, inv;
-};
-static void parse_ascii_part(const char *data, size_t a, size_t b, AsciiPart &o) {
-  u64 nf = 0, inv = 0, f0 = 0;
+// file's unterminated tail), token by token: value(v) for a found index,
+// nf() / inv() for a -1 / -2, end() at each read's end ('\n', and an
+// unterminated tail with tokens is one more read).
+template <class V, class NF, class INV, class END>
+static void scan_ascii(const char *data, size_t a, size_t b, V &&value, NF &&nf, INV &&inv,
+                       END &&end) {
   bool open_read = false;
-  auto end_read = [&]() {
-    o.n_found.push_back(o.found.size() - f0);
-    o.nf.push_back(nf);
-    o.inv.push_back(inv);
-    f0 = o.found.size();
-    nf = inv = 0;
-  };
   size_t i = a;
   while (i < b) {
     const char c = data[i];
     if (c == '\n') {
-      end_read();
+      end();
       open_read = false;
       ++i;
     } else if (c == '-') {  // -1 / -2 (other negatives are skipped)
-      if (i + 1 < b && data[i + 1] == '1') ++nf;
-      else if (i + 1 < b && data[i + 1] == '2') ++inv;
+      if (i + 1 < b && data[i + 1] == '1') nf();
+      else if (i + 1 < b && data[i + 1] == '2') inv();
       ++i;
       while (i < b && data[i] >= '0') ++i;
       open_read = true;
     } else if (c >= '0' && c <= '9') {
       u64 v = 0;
       while (i < b && data[i] >= '0' && data[i] <= '9') v = v * 10 + (u64)(data[i++] - '0');
-      o.found.push_back(v);
+      value(v);
       open_read = true;
     } else {
       ++i;
     }
   }
-  if (open_read) end_read();  // only the file's last part can end inside a read
+  if (open_read) end();  // only the file's last part can end inside a read
 }
 
 IndexResults read_index_results(const std::string &path) {
-  std::ifstream in(path, std::ios::binary);
+  FILE *in = std::fopen(path.c_str(), "rb");
   if (!in) throw std::runtime_error("Unable to open file " + path);
+  std::unique_ptr<FILE, int (*)(FILE *)> closer(in, std::fclose);
   auto get_str = [&]() {
     u64 n = 0;
-    in.read(reinterpret_cast<char *>(&n), 8);
-    if (!in || n > 64) throw std::runtime_error("The file has an incompatible format");
+    if (std::fread(&n, 8, 1, in) != 1 || n > 64)
+      throw std::runtime_error("The file has an incompatible format");
     std::string s(n, '\0');
-    in.read(s.data(), (std::streamsize)n);
+    if (n && std::fread(s.data(), 1, n, in) != n)
+      throw std::runtime_error("The file has an incompatible format");
     return s;
   };
   const std::string fmt = get_str();
   if (fmt != "ascii" && fmt != "binary")
     throw std::runtime_error("Unknown index file format '" + fmt + "'");
   if (get_str() != "v1.0") throw std::runtime_error("The file has an incompatible version number");
-  // the body in one read (its size from the stream's end)
-  const std::streampos body = in.tellg();
-  in.seekg(0, std::ios::end);
-  const std::streamoff n_body = in.tellg() - body;
-  in.seekg(body);
-  std::vector<char> data((size_t)std::max<std::streamoff>(n_body, 0));
-  if (!data.empty() && !in.read(data.data(), (std::streamsize)data.size()))
-    throw std::runtime_error("read error in index results file");
+  // the body in one read (its size from the file's end), not cleared first
+  const long body = std::ftell(in);
+  std::fseek(in, 0, SEEK_END);
+  const long end_pos = std::ftell(in);
+  std::fseek(in, body, SEEK_SET);
+  const size_t nbody = end_pos > body ? (size_t)(end_pos - body) : 0;
+  std::unique_ptr<char[]> buf(new char[std::max<size_t>(nbody, 1)]);
+  {  // in pieces of 64 MiB on host threads (the page-cache copies and the
+     // buffer's first touches run in parallel)
+    const int fd = fileno(in);
+    const size_t piece = 64ULL << 20, n_pieces = (nbody + piece - 1) / piece;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t T = std::min<size_t>(std::min<size_t>(hw, 16), std::max<size_t>(n_pieces, 1));
+    std::atomic<size_t> next{0};
+    std::atomic<bool> failed{false};
+    auto work = [&]() {
+      for (size_t p; (p = next.fetch_add(1)) < n_pieces;) {
+        const size_t off = p * piece, len = std::min(piece, nbody - off);
+        size_t got = 0;
+        while (got < len) {
+          const ssize_t r = ::pread(fd, buf.get() + off + got, len - got, body + (off_t)(off + got));
+          if (r <= 0) {
+            failed = true;
+            return;
+          }
+          got += (size_t)r;
+        }
+      }
+    };
+    std::vector<std::thread> th;
+    for (size_t t = 1; t < T; ++t) th.emplace_back(work);
+    work();
+    for (auto &x : th) x.join();
+    if (failed) throw std::runtime_error("read error in index results file");
+  }
+  const char *data = buf.get();
   IndexResults out;
   out.offsets.push_back(0);
   u64 nf = 0, inv = 0;
@@ -245,10 +269,12 @@ IndexResults read_index_results(const std::string &path) {
   };
   bool open_read = false;
   if (fmt == "ascii") {
-    // parts of whole lines parsed on host threads, then joined in order
-    const size_t n = data.size();
+    // parts of whole lines on host threads: one pass counts each part's
+    // reads and found values, the second writes them straight to their
+    // places in the output
+    const size_t n = nbody;
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t T = std::min<size_t>(std::min<size_t>(hw, 32), std::max<size_t>(n >> 24, 1));
+    const size_t T = std::min<size_t>(std::min<size_t>(hw, 32), std::max<size_t>(n >> 22, 1));
     std::vector<size_t> cut(T + 1, n);
     cut[0] = 0;
     for (size_t t = 1; t < T; ++t) {  // just past a newline at or after n * t / T
@@ -256,35 +282,53 @@ IndexResults read_index_results(const std::string &path) {
       while (c < n && data[c] != '\n') ++c;
       cut[t] = c < n ? c + 1 : n;
     }
-    std::vector<AsciiPart> parts(T);
-    std::vector<std::thread> th;
-    for (size_t t = 1; t < T; ++t)
-      th.emplace_back(parse_ascii_part, data.data(), cut[t], cut[t + 1], std::ref(parts[t]));
-    parse_ascii_part(data.data(), cut[0], cut[1], parts[0]);
-    for (auto &x : th) x.join();
-    size_t n_found = 0, n_reads = 0;
-    for (const auto &q : parts) {
-      n_found += q.found.size();
-      n_reads += q.nf.size();
+    std::vector<u64> part_found(T + 1, 0), part_reads(T + 1, 0);
+    auto run = [&](auto &&work) {
+      std::vector<std::thread> th;
+      for (size_t t = 1; t < T; ++t) th.emplace_back(work, t);
+      work(0);
+      for (auto &x : th) x.join();
+    };
+    run([&](size_t t) {
+      u64 nv = 0, nr = 0;
+      scan_ascii(data, cut[t], cut[t + 1], [&](u64) { ++nv; }, [] {}, [] {}, [&] { ++nr; });
+      part_found[t] = nv;
+      part_reads[t] = nr;
+    });
+    u64 total_found = 0, total_reads = 0;
+    for (size_t t = 0; t < T; ++t) {  // exclusive prefix sums
+      const u64 f = part_found[t], r = part_reads[t];
+      part_found[t] = total_found;
+      part_reads[t] = total_reads;
+      total_found += f;
+      total_reads += r;
     }
-    out.found.reserve(n_found);
-    out.offsets.reserve(n_reads + 1);
-    out.not_found.reserve(n_reads);
-    out.invalid.reserve(n_reads);
-    for (auto &q : parts) {
-      out.found.insert(out.found.end(), q.found.begin(), q.found.end());
-      for (size_t r = 0; r < q.nf.size(); ++r) {
-        out.offsets.push_back(out.offsets.back() + q.n_found[r]);
-        out.not_found.push_back(q.nf[r]);
-        out.invalid.push_back(q.inv[r]);
-      }
-    }
+    out.found.resize(total_found);
+    out.offsets.resize(total_reads + 1);
+    out.not_found.resize(total_reads);
+    out.invalid.resize(total_reads);
+    out.offsets[0] = 0;
+    run([&](size_t t) {
+      u64 fv = part_found[t], r = part_reads[t], pnf = 0, pinv = 0;
+      u64 *found = out.found.data(), *offs = out.offsets.data();
+      u64 *onf = out.not_found.data(), *oinv = out.invalid.data();
+      scan_ascii(
+          data, cut[t], cut[t + 1], [&](u64 v) { found[fv++] = v; }, [&] { ++pnf; },
+          [&] { ++pinv; },
+          [&] {
+            offs[r + 1] = fv;
+            onf[r] = pnf;
+            oinv[r] = pinv;
+            ++r;
+            pnf = pinv = 0;
+          });
+    });
     return out;
   } else {
-    const size_t nw = data.size() / 8;
+    const size_t nw = nbody / 8;
     for (size_t w = 0; w < nw; ++w) {
       u64 v;
-      std::memcpy(&v, data.data() + 8 * w, 8);
+      std::memcpy(&v, data + 8 * w, 8);
       if (v == (u64)-1) {
         ++nf;
         open_read = true;
@@ -375,7 +419,7 @@ int sbwt_read_index_results(const char *path, uint64_t **found, uint64_t **offse
   }
   return guarded([&] {
     IndexResults r = read_index_results(path);
-    auto dup = [](const std::vector<u64> &v) {
+    auto dup = [](const U64Array &v) {
       auto *p = static_cast<uint64_t *>(std::malloc(std::max<size_t>(v.size(), 1) * 8));
       if (!p) throw std::bad_alloc();
       std::memcpy(p, v.data(), v.size() * 8);

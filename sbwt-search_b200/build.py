@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-I", str(REPO / "include")]
 
 LIB_SOURCES = ["index.cu", "colors.cu", "measure.cu", "pipeline.cu", "fastx_device.cu", "format_device.cu", "build_device.cu", "kmer_table.cu",
-               "capi.cpp", "formats.cpp", "fastx.cpp", "results_io.cpp"]
+               "capi.cpp", "colors_host.cpp", "formats.cpp", "fastx.cpp", "results_io.cpp"]
 CLI_SOURCES = ["cli_main.cpp"]
 TOOLS_SOURCES = ["tools/sbwt_build.cpp", "formats.cpp"]
 

@@ -851,7 +851,10 @@ void build_colored_device(const char *chars, u64 n_chars, const u64 *ends, u64 C
     }
   }
   t.dense_arrays.num_bits = dense_total;
-  t.dense_arrays.words = to_host<u64>(dense_words, (dense_total + 63) / 64);
+  {
+    const std::vector<u64> w = to_host<u64>(dense_words, (dense_total + 63) / 64);
+    t.dense_arrays.words.assign(w.begin(), w.end());
+  }
   t.dense_arrays_intervals.assign(dense_iv, width_for(dense_iv.back()));
   t.sparse_arrays.assign(to_host<u64>(sparse_vals, sparse_total), width_for(C - 1));
   t.sparse_arrays_intervals.assign(sparse_iv, width_for(sparse_iv.back()));

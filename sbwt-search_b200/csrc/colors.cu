@@ -36,14 +36,6 @@ namespace sbwt {
 
 constexpr int kColorWarps = 4;  // warps (reads in flight) per block
 
-// Packed set record: start (42 bits) | len (21 bits) | dense (1 bit).  len is
-// row words for a dense set, ids for a sparse one; start indexes the dense
-// words or the sparse ids.
-constexpr uint64_t kRecNone = ~0ULL;
-constexpr int kRecLenBits = 21;
-__host__ __device__ __forceinline__ uint64_t make_rec(uint64_t start, uint64_t len, bool dense) {
-  return (start << (kRecLenBits + 1)) | (len << 1) | (dense ? 1ULL : 0ULL);
-}
 __device__ __forceinline__ uint64_t rec_start(uint64_t rec) { return rec >> (kRecLenBits + 1); }
 __device__ __forceinline__ uint32_t rec_len(uint64_t rec) {
   return (uint32_t)(rec >> 1) & ((1u << kRecLenBits) - 1);
@@ -81,6 +73,27 @@ __device__ __forceinline__ uint64_t set_record(const ColorsView &cv, uint64_t v)
   if (j >= cv.n_keys) return kRecNone;
   const uint32_t s = __ldg(cv.csi + j);
   return s < cv.n_sets ? __ldg(cv.recs + s) : kRecNone;
+}
+
+// out[i] = entry i of an sdsl int vector of `width` bits per entry (LSB-first
+// in 64-bit words); entries >= limit set *err and read as 0.
+__global__ void unpack_set_indexes_kernel(const uint64_t *words, uint64_t n, uint32_t width,
+                                          uint64_t limit, uint32_t *out, uint32_t *err) {
+  const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t mask = width >= 64 ? ~0ULL : (1ULL << width) - 1;
+  uint32_t bad = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += step) {
+    const uint64_t bit = i * width, w = bit >> 6, o = bit & 63;
+    uint64_t v = words[w] >> o;
+    if (o + width > 64) v |= words[w + 1] << (64 - o);
+    v &= mask;
+    if (v >= limit) {
+      bad = 1;
+      v = 0;
+    }
+    out[i] = (uint32_t)v;
+  }
+  if (__any_sync(0xFFFFFFFFu, bad) && (threadIdx.x & 31) == 0) atomicOr(err, 1u);
 }
 
 // node_rec[v] = set_record(v) for every v < key_bits.
@@ -481,57 +494,7 @@ ColorsImpl::ColorsImpl(const TColorsFile &t, int device_) {
     throw Error(SBWT_E_FORMAT, "number of colors out of range");
   const u64 n_sets = t.is_dense_marks.num_bits;
   const u64 n_keys = t.color_set_idxs.size();
-  // per-set packed records + dense rows (aligned) + u32 sparse ids
-  std::vector<u64> recs(std::max<u64>(n_sets, 1));
-  std::vector<u64> dense_words;
-  std::vector<uint32_t> sparse(std::max<u64>(t.sparse_arrays.size(), 1));
-  for (u64 i = 0; i < t.sparse_arrays.size(); ++i) {
-    const u64 v = t.sparse_arrays.get(i);
-    if (v >= num_colors) throw Error(SBWT_E_FORMAT, "sparse color id out of range");
-    sparse[i] = (uint32_t)v;
-  }
-  u64 n_dense = 0, n_sparse = 0;
-  bool sparse_sorted = true;  // every sparse list strictly ascending
-  const u64 n_dense_iv = t.dense_arrays_intervals.size();
-  const u64 n_sparse_iv = t.sparse_arrays_intervals.size();
-  for (u64 s = 0; s < n_sets; ++s) {
-    if (t.is_dense_marks.get(s)) {
-      if (n_dense + 1 >= n_dense_iv) throw Error(SBWT_E_FORMAT, "dense intervals too short");
-      const u64 st = t.dense_arrays_intervals.get(n_dense);
-      const u64 en = t.dense_arrays_intervals.get(n_dense + 1);
-      if (en < st || en > t.dense_arrays.num_bits || en - st > num_colors)
-        throw Error(SBWT_E_FORMAT, "dense interval out of range");
-      const u64 nbits = en - st, nw = (nbits + 63) / 64;
-      // a row starts on a 64-byte boundary (on its own size when smaller),
-      // so it spans the fewest sectors and DRAM bursts
-      const u64 align = nw >= 8 ? 8 : nw >= 4 ? 4 : nw >= 2 ? 2 : 1;
-      const u64 at = (dense_words.size() + align - 1) / align * align;
-      dense_words.resize(at + nw, 0);
-      for (u64 c = 0; c < nbits; ++c)
-        if (t.dense_arrays.get(st + c)) dense_words[at + c / 64] |= 1ULL << (c % 64);
-      recs[s] = make_rec(at, nw, true);
-      ++n_dense;
-    } else {
-      if (n_sparse + 1 >= n_sparse_iv) throw Error(SBWT_E_FORMAT, "sparse intervals too short");
-      const u64 st = t.sparse_arrays_intervals.get(n_sparse);
-      const u64 en = t.sparse_arrays_intervals.get(n_sparse + 1);
-      if (en < st || en > t.sparse_arrays.size())
-        throw Error(SBWT_E_FORMAT, "sparse interval out of range");
-      if (en - st >= (1ULL << kRecLenBits)) throw Error(SBWT_E_FORMAT, "sparse color set too long");
-      for (u64 i = st + 1; i < en && sparse_sorted; ++i) sparse_sorted = sparse[i - 1] < sparse[i];
-      recs[s] = make_rec(st, en - st, false);
-      ++n_sparse;
-    }
-  }
-  if (dense_words.empty()) dense_words.push_back(0);
-  if (std::max<u64>(dense_words.size(), t.sparse_arrays.size()) >= (1ULL << (63 - kRecLenBits)))
-    throw Error(SBWT_E_FORMAT, "color arrays too large");
-  std::vector<uint32_t> csi(std::max<u64>(n_keys, 1));
-  for (u64 j = 0; j < n_keys; ++j) {
-    const u64 v = t.color_set_idxs.get(j);
-    if (v >= n_sets) throw Error(SBWT_E_FORMAT, "color set index out of range");
-    csi[j] = (uint32_t)v;
-  }
+  const HostColorSets h = prepare_color_sets(t);
   std::vector<Block> kb;
   std::vector<u64> kl0;
   u64 total_keys = 0;
@@ -545,10 +508,26 @@ ColorsImpl::ColorsImpl(const TColorsFile &t, int device_) {
   };
   up(key_blocks, kb.data(), kb.size() * sizeof(Block));
   up(key_l0, kl0.data(), kl0.size() * 8);
-  up(csi_buf, csi.data(), csi.size() * 4);
-  up(recs_buf, recs.data(), recs.size() * 8);
-  up(dense_buf, dense_words.data(), dense_words.size() * 8);
-  up(sparse_buf, sparse.data(), sparse.size() * 4);
+  up(recs_buf, h.recs.data(), h.recs.size() * 8);
+  up(dense_buf, h.dense_words.data(), h.dense_words.size() * 8);
+  up(sparse_buf, h.sparse.data(), h.sparse.size() * 4);
+  // color set indexes: the packed int vector goes up as it is and is widened
+  // to u32 on the device
+  csi_buf.resize(std::max<u64>(n_keys, 1) * 4);
+  if (n_keys) {
+    DeviceBuffer packed, err;
+    up(packed, t.color_set_idxs.words.data(), t.color_set_idxs.words.size() * 8);
+    err.resize(4);
+    SBWT_CUDA(cudaMemset(err.get(), 0, 4));
+    const u64 blocks = std::min<u64>((n_keys + 255) / 256, 148 * 16);
+    unpack_set_indexes_kernel<<<(unsigned)blocks, 256>>>(
+        packed.get<u64>(), n_keys, t.color_set_idxs.width, n_sets, csi_buf.get<uint32_t>(),
+        err.get<uint32_t>());
+    SBWT_CUDA(cudaGetLastError());
+    uint32_t bad = 0;
+    SBWT_CUDA(cudaMemcpy(&bad, err.get(), 4, cudaMemcpyDeviceToHost));
+    if (bad) throw Error(SBWT_E_FORMAT, "color set index out of range");
+  }
   view = ColorsView{};
   view.key_blocks = key_blocks.get<Block>();
   view.key_l0 = key_l0.get<u64>();
@@ -564,7 +543,7 @@ ColorsImpl::ColorsImpl(const TColorsFile &t, int device_) {
   // color tiles of at most 32 lanes x 4 words (8192 colors) per warp
   view.words_per_lane = std::min<uint32_t>((view.row_words + 31) / 32, 4);
   view.tiles = (view.row_words + 32 * view.words_per_lane - 1) / (32 * view.words_per_lane);
-  view.sparse_sorted = sparse_sorted ? 1 : 0;
+  view.sparse_sorted = h.sparse_sorted ? 1 : 0;
   set_node_table(true);
 }
 

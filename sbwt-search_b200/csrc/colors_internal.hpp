@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "common.hpp"
 #include "device_layout.hpp"
 #include "formats.hpp"
@@ -10,6 +12,28 @@
 namespace sbwt {
 
 constexpr u64 kNodeTableMaxBytes = 16ULL << 30;  // per-node record table cap
+
+// Packed set record: start (42 bits) | len (21 bits) | dense (1 bit).  len is
+// row words for a dense set, ids for a sparse one; start indexes the dense
+// words or the sparse ids.
+constexpr uint64_t kRecNone = ~0ULL;
+constexpr int kRecLenBits = 21;
+__host__ __device__ __forceinline__ uint64_t make_rec(uint64_t start, uint64_t len, bool dense) {
+  return (start << (kRecLenBits + 1)) | (len << 1) | (dense ? 1ULL : 0ULL);
+}
+
+// Host images of the color set arrays the device keeps: one record per color
+// set, the dense rows (each on its own alignment, gaps zero) and the sparse
+// ids as u32.
+struct HostColorSets {
+  std::vector<u64> recs;
+  std::vector<u64> dense_words;
+  std::vector<uint32_t> sparse;
+  bool sparse_sorted = true;  // every sparse list strictly ascending
+};
+// Checks and lays out the color sets of t (host threads); throws Error
+// (SBWT_E_FORMAT) on malformed intervals or ids.
+HostColorSets prepare_color_sets(const TColorsFile &t);
 
 // Device view of the color index.
 struct ColorsView {

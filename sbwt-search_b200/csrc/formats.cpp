@@ -1,20 +1,34 @@
 #include "formats.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <stdexcept>
+#include <thread>
+#include <vector>
+
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 namespace sbwt {
 
 namespace {
 
+// Sequential reader over a file descriptor; arrays above 32 MiB are
+// read in parallel pieces (pread on host threads).
 class Reader {
  public:
-  explicit Reader(const std::string &path) : f_(path, std::ios::binary) {
-    if (!f_) throw std::runtime_error("Unable to open file " + path);
+  explicit Reader(const std::string &path) : fd_(::open(path.c_str(), O_RDONLY)) {
+    if (fd_ < 0) throw std::runtime_error("Unable to open file " + path);
+    struct stat st {};
+    size_ = ::fstat(fd_, &st) == 0 ? (u64)st.st_size : 0;
   }
+  ~Reader() { ::close(fd_); }
+  Reader(const Reader &) = delete;
+  Reader &operator=(const Reader &) = delete;
   u64 u64v() {
     u64 v = 0;
     read(&v, 8);
@@ -33,11 +47,36 @@ class Reader {
     return s;
   }
   void read(void *dst, u64 n) {
-    f_.read(static_cast<char *>(dst), static_cast<std::streamsize>(n));
-    if (static_cast<u64>(f_.gcount()) != n)
-      throw std::runtime_error("unexpected end of file");
+    if (n > size_ || pos_ > size_ - n) throw std::runtime_error("unexpected end of file");
+    char *out = static_cast<char *>(dst);
+    constexpr u64 kPiece = 32ULL << 20;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const u64 parts = std::min<u64>(std::min(hw, 16u), (n + kPiece - 1) / kPiece);
+    std::atomic<bool> ok{true};
+    auto piece = [&](u64 a, u64 b) {
+      while (a < b) {
+        const ssize_t got = ::pread(fd_, out + a, b - a, (off_t)(pos_ + a));
+        if (got <= 0) {
+          ok = false;
+          return;
+        }
+        a += (u64)got;
+      }
+    };
+    if (parts <= 1) {
+      piece(0, n);
+    } else {
+      std::vector<std::thread> th;
+      for (u64 p = 0; p < parts; ++p) th.emplace_back(piece, n * p / parts, n * (p + 1) / parts);
+      for (auto &t : th) t.join();
+    }
+    if (!ok) throw std::runtime_error("unexpected end of file");
+    pos_ += n;
   }
-  void skip(u64 n) { f_.seekg(static_cast<std::streamoff>(n), std::ios::cur); }
+  void skip(u64 n) {
+    if (n > size_ || pos_ > size_ - n) throw std::runtime_error("unexpected end of file");
+    pos_ += n;
+  }
   BitVector bitvector() {
     BitVector b;
     b.num_bits = u64v();
@@ -53,6 +92,7 @@ class Reader {
     IntVector v;
     v.num_bits = u64v();
     v.width = u8v();
+    if (v.width > 64) throw std::runtime_error("corrupt int vector width");
     v.words.resize((v.num_bits + 63) / 64);
     read(v.words.data(), v.words.size() * 8);
     return v;
@@ -64,7 +104,8 @@ class Reader {
   }
 
  private:
-  std::ifstream f_;
+  int fd_;
+  u64 size_ = 0, pos_ = 0;
 };
 
 class Writer {

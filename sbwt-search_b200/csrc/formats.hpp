@@ -11,7 +11,10 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace sbwt {
@@ -20,9 +23,31 @@ using u64 = uint64_t;
 using u32 = uint32_t;
 using u8 = uint8_t;
 
+// A vector whose resize leaves new elements uninitialised (they are all
+// written next), so multi-GB arrays read from files are not cleared first.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <class U>
+  NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
+  template <class U>
+  void construct(U *p) noexcept {
+    ::new (static_cast<void *>(p)) U;
+  }
+  template <class U, class... A>
+  void construct(U *p, A &&...a) {
+    ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
+  }
+};
+using U64Array = std::vector<u64, NoInitAlloc<u64>>;
+
 struct BitVector {
   u64 num_bits = 0;
-  std::vector<u64> words;  // ceil(num_bits / 64) words, LSB-first bits
+  U64Array words;  // ceil(num_bits / 64) words, LSB-first bits
   bool get(u64 i) const { return (words[i / 64] >> (i % 64)) & 1ULL; }
   void set(u64 i) { words[i / 64] |= 1ULL << (i % 64); }
   void resize(u64 bits) {
@@ -34,7 +59,7 @@ struct BitVector {
 struct IntVector {  // sdsl int_vector<> (variable width), LSB-first packing
   u64 num_bits = 0;
   u8 width = 64;
-  std::vector<u64> words;
+  U64Array words;
   u64 size() const { return width ? num_bits / width : 0; }
   u64 get(u64 idx) const;
   void assign(const std::vector<u64> &values, u8 width);

@@ -11,6 +11,8 @@
 #include <utility>
 #include <vector>
 
+#include "formats.hpp"
+
 namespace sbwt {
 
 using u64 = uint64_t;
@@ -98,28 +100,6 @@ class ColorResultsWriter {
 // (src/IndexFileParser/AsciiIndexFileParser.cpp:33-98,
 //  BinaryIndexFileParser.cpp:33-69): per read the found indexes, and the
 // counts of -1 and -2 tokens.
-// A vector whose resize leaves new elements uninitialised (they are all
-// written next), so multi-GB result arrays are not cleared first.
-template <class T>
-struct NoInitAlloc : std::allocator<T> {
-  template <class U>
-  struct rebind {
-    using other = NoInitAlloc<U>;
-  };
-  NoInitAlloc() = default;
-  template <class U>
-  NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
-  template <class U>
-  void construct(U *p) noexcept {
-    ::new (static_cast<void *>(p)) U;
-  }
-  template <class U, class... A>
-  void construct(U *p, A &&...a) {
-    ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
-  }
-};
-using U64Array = std::vector<u64, NoInitAlloc<u64>>;
-
 struct IndexResults {
   U64Array found;    // all reads back to back
   U64Array offsets;  // n_reads + 1

@@ -77,30 +77,34 @@ class Reader {
     if (n > size_ || pos_ > size_ - n) throw std::runtime_error("unexpected end of file");
     pos_ += n;
   }
+  // words of a vector of `bits` bits, checked against the rest of the file
+  // before anything is allocated for them
+  u64 words_for(u64 bits) const {
+    const u64 nw = bits / 64 + (bits % 64 ? 1 : 0);
+    if (nw > (size_ - pos_) / 8) throw std::runtime_error("unexpected end of file");
+    return nw;
+  }
   BitVector bitvector() {
     BitVector b;
     b.num_bits = u64v();
-    b.words.resize((b.num_bits + 63) / 64);
+    b.words.resize(words_for(b.num_bits));
     read(b.words.data(), b.words.size() * 8);
     return b;
   }
-  void skip_bitvector() {
-    u64 bits = u64v();
-    skip(((bits + 63) / 64) * 8);
-  }
+  void skip_bitvector() { skip(words_for(u64v()) * 8); }
   IntVector intvector() {
     IntVector v;
     v.num_bits = u64v();
     v.width = u8v();
     if (v.width > 64) throw std::runtime_error("corrupt int vector width");
-    v.words.resize((v.num_bits + 63) / 64);
+    v.words.resize(words_for(v.num_bits));
     read(v.words.data(), v.words.size() * 8);
     return v;
   }
   void skip_intvector() {
-    u64 bits = u64v();
+    const u64 bits = u64v();
     u8v();
-    skip(((bits + 63) / 64) * 8);
+    skip(words_for(bits) * 8);
   }
 
  private:

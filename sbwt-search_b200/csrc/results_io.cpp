@@ -205,6 +205,29 @@ static void scan_ascii(const char *data, size_t a, size_t b, V &&value, NF &&nf,
   if (open_read) end();  // only the file's last part can end inside a read
 }
 
+// The binary body of an index results file, words [a, b) (whole reads, or
+// the file's unterminated tail), with the callbacks of scan_ascii: a read
+// ends at each -3 word, -1 / -2 are not-found / invalid.
+template <class V, class NF, class INV, class END>
+static void scan_binary(const char *data, size_t a, size_t b, V &&value, NF &&nf, INV &&inv,
+                        END &&end) {
+  bool open_read = false;
+  for (size_t w = a; w < b; ++w) {
+    u64 v;
+    std::memcpy(&v, data + 8 * w, 8);
+    if (v == (u64)-3) {
+      end();
+      open_read = false;
+      continue;
+    }
+    if (v == (u64)-1) nf();
+    else if (v == (u64)-2) inv();
+    else value(v);
+    open_read = true;
+  }
+  if (open_read) end();  // only the file's last part can end inside a read
+}
+
 IndexResults read_index_results(const std::string &path) {
   FILE *in = std::fopen(path.c_str(), "rb");
   if (!in) throw std::runtime_error("Unable to open file " + path);
@@ -258,93 +281,73 @@ IndexResults read_index_results(const std::string &path) {
     if (failed) throw std::runtime_error("read error in index results file");
   }
   const char *data = buf.get();
-  IndexResults out;
-  out.offsets.push_back(0);
-  u64 nf = 0, inv = 0;
-  auto end_read = [&]() {
-    out.offsets.push_back(out.found.size());
-    out.not_found.push_back(nf);
-    out.invalid.push_back(inv);
-    nf = inv = 0;
+  // Parts of whole reads on host threads (cut just past a newline, or a -3
+  // word): one pass counts each part's reads and found values, the second
+  // writes them straight to their places in the output.
+  const bool ascii = fmt == "ascii";
+  const size_t n = ascii ? nbody : nbody / 8;  // bytes or words (a partial word is ignored)
+  auto word = [&](size_t w) {
+    u64 v;
+    std::memcpy(&v, data + 8 * w, 8);
+    return v;
   };
-  bool open_read = false;
-  if (fmt == "ascii") {
-    // parts of whole lines on host threads: one pass counts each part's
-    // reads and found values, the second writes them straight to their
-    // places in the output
-    const size_t n = nbody;
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t T = std::min<size_t>(std::min<size_t>(hw, 32), std::max<size_t>(n >> 22, 1));
-    std::vector<size_t> cut(T + 1, n);
-    cut[0] = 0;
-    for (size_t t = 1; t < T; ++t) {  // just past a newline at or after n * t / T
-      size_t c = std::max(cut[t - 1], n * t / T);
+  auto scan = [&](size_t a, size_t b, auto &&value, auto &&nf, auto &&inv, auto &&end) {
+    if (ascii) scan_ascii(data, a, b, value, nf, inv, end);
+    else scan_binary(data, a, b, value, nf, inv, end);
+  };
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t T = std::min<size_t>(std::min<size_t>(hw, 32), std::max<size_t>(nbody >> 22, 1));
+  std::vector<size_t> cut(T + 1, n);
+  cut[0] = 0;
+  for (size_t t = 1; t < T; ++t) {  // just past a read's end at or after n * t / T
+    size_t c = std::max(cut[t - 1], n * t / T);
+    if (ascii)
       while (c < n && data[c] != '\n') ++c;
-      cut[t] = c < n ? c + 1 : n;
-    }
-    std::vector<u64> part_found(T + 1, 0), part_reads(T + 1, 0);
-    auto run = [&](auto &&work) {
-      std::vector<std::thread> th;
-      for (size_t t = 1; t < T; ++t) th.emplace_back(work, t);
-      work(0);
-      for (auto &x : th) x.join();
-    };
-    run([&](size_t t) {
-      u64 nv = 0, nr = 0;
-      scan_ascii(data, cut[t], cut[t + 1], [&](u64) { ++nv; }, [] {}, [] {}, [&] { ++nr; });
-      part_found[t] = nv;
-      part_reads[t] = nr;
-    });
-    u64 total_found = 0, total_reads = 0;
-    for (size_t t = 0; t < T; ++t) {  // exclusive prefix sums
-      const u64 f = part_found[t], r = part_reads[t];
-      part_found[t] = total_found;
-      part_reads[t] = total_reads;
-      total_found += f;
-      total_reads += r;
-    }
-    out.found.resize(total_found);
-    out.offsets.resize(total_reads + 1);
-    out.not_found.resize(total_reads);
-    out.invalid.resize(total_reads);
-    out.offsets[0] = 0;
-    run([&](size_t t) {
-      u64 fv = part_found[t], r = part_reads[t], pnf = 0, pinv = 0;
-      u64 *found = out.found.data(), *offs = out.offsets.data();
-      u64 *onf = out.not_found.data(), *oinv = out.invalid.data();
-      scan_ascii(
-          data, cut[t], cut[t + 1], [&](u64 v) { found[fv++] = v; }, [&] { ++pnf; },
-          [&] { ++pinv; },
-          [&] {
-            offs[r + 1] = fv;
-            onf[r] = pnf;
-            oinv[r] = pinv;
-            ++r;
-            pnf = pinv = 0;
-          });
-    });
-    return out;
-  } else {
-    const size_t nw = nbody / 8;
-    for (size_t w = 0; w < nw; ++w) {
-      u64 v;
-      std::memcpy(&v, data + 8 * w, 8);
-      if (v == (u64)-1) {
-        ++nf;
-        open_read = true;
-      } else if (v == (u64)-2) {
-        ++inv;
-        open_read = true;
-      } else if (v == (u64)-3) {
-        end_read();
-        open_read = false;
-      } else {
-        out.found.push_back(v);
-        open_read = true;
-      }
-    }
+    else
+      while (c < n && word(c) != (u64)-3) ++c;
+    cut[t] = c < n ? c + 1 : n;
   }
-  if (open_read) end_read();  // unterminated last read
+  std::vector<u64> part_found(T + 1, 0), part_reads(T + 1, 0);
+  auto run = [&](auto &&work) {
+    std::vector<std::thread> th;
+    for (size_t t = 1; t < T; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto &x : th) x.join();
+  };
+  run([&](size_t t) {
+    u64 nv = 0, nr = 0;
+    scan(cut[t], cut[t + 1], [&](u64) { ++nv; }, [] {}, [] {}, [&] { ++nr; });
+    part_found[t] = nv;
+    part_reads[t] = nr;
+  });
+  u64 total_found = 0, total_reads = 0;
+  for (size_t t = 0; t < T; ++t) {  // exclusive prefix sums
+    const u64 f = part_found[t], r = part_reads[t];
+    part_found[t] = total_found;
+    part_reads[t] = total_reads;
+    total_found += f;
+    total_reads += r;
+  }
+  IndexResults out;
+  out.found.resize(total_found);
+  out.offsets.resize(total_reads + 1);
+  out.not_found.resize(total_reads);
+  out.invalid.resize(total_reads);
+  out.offsets[0] = 0;
+  run([&](size_t t) {
+    u64 fv = part_found[t], r = part_reads[t], pnf = 0, pinv = 0;
+    u64 *found = out.found.data(), *offs = out.offsets.data();
+    u64 *onf = out.not_found.data(), *oinv = out.invalid.data();
+    scan(
+        cut[t], cut[t + 1], [&](u64 v) { found[fv++] = v; }, [&] { ++pnf; }, [&] { ++pinv; },
+        [&] {
+          offs[r + 1] = fv;
+          onf[r] = pnf;
+          oinv[r] = pinv;
+          ++r;
+          pnf = pinv = 0;
+        });
+  });
   return out;
 }
 

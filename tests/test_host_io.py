@@ -143,11 +143,13 @@ def test_fastx_reader_matches_oracle_on_random_text(seed, tmp_path):
     assert ends.tolist() == np.cumsum([len(r) for r in reads]).tolist()
 
 
+@pytest.mark.parametrize("binary", [False, True])
 @pytest.mark.parametrize("tail_newline", [True, False])
-def test_index_file_reader_large_file_in_parts(tail_newline):
-    """A file over 16 MB is parsed in parts of whole lines on host threads:
-    the joined result equals the rows written (values, -1 and -2 counts,
-    empty rows, and an unterminated last row)."""
+def test_index_file_reader_large_file_in_parts(tail_newline, binary):
+    """A file over 16 MB is parsed in parts of whole reads on host threads
+    (ascii lines, or binary reads ended by -3 words): the joined result
+    equals the rows written (values, -1 and -2 counts, empty rows, and an
+    unterminated last row)."""
     rng = np.random.default_rng(5)
     n_rows = 600_000
     lens = rng.integers(0, 40, n_rows)
@@ -160,13 +162,23 @@ def test_index_file_reader_large_file_in_parts(tail_newline):
     vals[kinds < 0.1] = -1
     vals[(kinds >= 0.1) & (kinds < 0.15)] = -2
     starts = np.concatenate([[0], np.cumsum(lens)])
-    lines = [" ".join(map(str, vals[starts[r]:starts[r + 1]])) for r in range(n_rows)]
-    if not tail_newline:
-        lines[-1] = lines[-1] or "5"
-    body = "\n".join(lines) + ("\n" if tail_newline else "")
-    path = TMP / f"big_index_results_{int(tail_newline)}.txt"
-    path.write_bytes(struct.pack("<Q", 5) + b"ascii" + struct.pack("<Q", 4) + b"v1.0" +
-                     body.encode())
+    path = TMP / f"big_index_results_{int(tail_newline)}_{int(binary)}.txt"
+    if binary:
+        words = np.full(len(vals) + n_rows, np.uint64(2**64 - 3))
+        words[np.arange(len(vals)) + np.repeat(np.arange(n_rows), lens)] = vals.astype(np.uint64)
+        if not tail_newline:
+            words = words[:-1]
+            if lens[-1] == 0:
+                words = np.concatenate([words, np.array([5], np.uint64)])
+        path.write_bytes(struct.pack("<Q", 6) + b"binary" + struct.pack("<Q", 4) + b"v1.0" +
+                         words.tobytes())
+    else:
+        lines = [" ".join(map(str, vals[starts[r]:starts[r + 1]])) for r in range(n_rows)]
+        if not tail_newline:
+            lines[-1] = lines[-1] or "5"
+        body = "\n".join(lines) + ("\n" if tail_newline else "")
+        path.write_bytes(struct.pack("<Q", 5) + b"ascii" + struct.pack("<Q", 4) + b"v1.0" +
+                         body.encode())
     assert path.stat().st_size > 40 << 20  # several parts
     L = lib()
     ptrs = [C.c_void_p() for _ in range(4)]

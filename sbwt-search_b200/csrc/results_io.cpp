@@ -2,6 +2,7 @@
 #include <charconv>
 #include <cstring>
 #include <fstream>
+#include <emmintrin.h>
 #include <unistd.h>
 
 #include <atomic>
@@ -172,6 +173,49 @@ void ColorResultsWriter::write_raw(const char *bytes, u64 n) {
   if (n && std::fwrite(bytes, 1, n, f_) != n) throw std::runtime_error("write failed");
 }
 
+// Length of the run of decimal digits that starts 8 bytes x (first char in
+// the low byte), 0..8.  Per byte without carries between bytes: the byte's
+// low 7 bits compared with '0' and ':' by adding to the high bit, and the
+// high bit itself clear.
+static inline unsigned digit_run8(u64 x) {
+  constexpr u64 kHigh = 0x8080808080808080ULL, kLow7 = 0x7F7F7F7F7F7F7F7FULL;
+  const u64 low = x & kLow7;
+  const u64 ge0 = (low + 0x5050505050505050ULL) & kHigh;    // low >= 0x30
+  const u64 gt9 = (low + 0x4646464646464646ULL) & kHigh;    // low >= 0x3A
+  const u64 digit = ge0 & ~gt9 & ~x & kHigh;
+  const u64 other = ~digit & kHigh;
+  return other ? (unsigned)__builtin_ctzll(other) / 8 : 8u;
+}
+
+// Value of the first len (0..8) digit chars of x: the digits moved to the
+// top bytes (zeros below are leading zeros), then pairs, quads and the
+// eight combined by multiply-and-shift (the published SWAR eight-digit
+// conversion).
+static inline u64 digits_value8(u64 x, unsigned len) {
+  u64 d = (x & 0x0F0F0F0F0F0F0F0FULL) << ((8 * (8 - len)) & 63);
+  d = (d * 10 + (d >> 8)) & 0x00FF00FF00FF00FFULL;
+  d = (d * 100 + (d >> 16)) & 0x0000FFFF0000FFFFULL;
+  d = (d * 10000 + (d >> 32)) & 0x00000000FFFFFFFFULL;
+  return len ? d : 0;
+}
+
+// The decimal number whose digits start at data[i] (i < b), modulo 2^64;
+// i moves past its digits.  Up to 8 digits from one 8-byte load, the rest
+// one by one.  (Two loads for up to 16 digits without a branch on the
+// length were slower on the index workload's 8-9 digit numbers.)
+static inline u64 parse_digits(const char *data, size_t &i, size_t b) {
+  u64 v = 0;
+  if (i + 8 <= b) {
+    u64 x;
+    std::memcpy(&x, data + i, 8);
+    const unsigned len = digit_run8(x);
+    v = digits_value8(x, len);
+    i += len;
+  }
+  while (i < b && data[i] >= '0' && data[i] <= '9') v = v * 10 + (u64)(data[i++] - '0');
+  return v;
+}
+
 // The ascii body of an index results file, bytes [a, b) (whole lines, or the
 // file's unterminated tail), token by token: value(v) for a found index,
 // nf() / inv() for a -1 / -2, end() at each read's end ('\n', and an
@@ -194,15 +238,110 @@ static void scan_ascii(const char *data, size_t a, size_t b, V &&value, NF &&nf,
       while (i < b && data[i] >= '0') ++i;
       open_read = true;
     } else if (c >= '0' && c <= '9') {
-      u64 v = 0;
-      while (i < b && data[i] >= '0' && data[i] <= '9') v = v * 10 + (u64)(data[i++] - '0');
-      value(v);
+      value(parse_digits(data, i, b));
       open_read = true;
     } else {
       ++i;
     }
   }
   if (open_read) end();  // only the file's last part can end inside a read
+}
+
+// Bytes [i, i + 64) of an ascii body that ends at b, one bit per byte and
+// class (bytes at b and past it read as spaces); bad = none of digit,
+// space, newline, '-'.
+struct Block64 {
+  u64 digit, sep, nl, minus, one, two, bad;
+};
+static inline Block64 classify64(const char *data, size_t i, size_t b) {
+  alignas(16) char tmp[64];
+  const char *p = data + i;
+  if (b - i < 64) {
+    std::memcpy(tmp, p, b - i);
+    std::memset(tmp + (b - i), ' ', 64 - (b - i));
+    p = tmp;
+  }
+  const __m128i k0 = _mm_set1_epi8('0'), k9 = _mm_set1_epi8(9), ksp = _mm_set1_epi8(' '),
+                knl = _mm_set1_epi8('\n'), kmi = _mm_set1_epi8('-'), k1 = _mm_set1_epi8('1'),
+                k2 = _mm_set1_epi8('2');
+  Block64 c{0, 0, 0, 0, 0, 0, 0};
+  for (int q = 0; q < 4; ++q) {
+    const __m128i x = _mm_loadu_si128(reinterpret_cast<const __m128i *>(p + 16 * q));
+    const __m128i d = _mm_sub_epi8(x, k0);
+    auto bits = [q](__m128i m) { return (u64)(unsigned)_mm_movemask_epi8(m) << (16 * q); };
+    const __m128i nl = _mm_cmpeq_epi8(x, knl);
+    c.digit |= bits(_mm_cmpeq_epi8(_mm_min_epu8(d, k9), d));  // x - '0' <= 9 unsigned
+    c.nl |= bits(nl);
+    c.sep |= bits(_mm_or_si128(_mm_cmpeq_epi8(x, ksp), nl));
+    c.minus |= bits(_mm_cmpeq_epi8(x, kmi));
+    c.one |= bits(_mm_cmpeq_epi8(x, k1));
+    c.two |= bits(_mm_cmpeq_epi8(x, k2));
+  }
+  c.bad = ~(c.digit | c.sep | c.minus);
+  return c;
+}
+
+// Whether a read is open (a token since the last newline) after block c.
+static inline bool open_after(const Block64 &c, bool open) {
+  const u64 tok = c.digit | c.minus;
+  if (!c.nl) return open || tok != 0;
+  const int last = 63 - __builtin_clzll(c.nl);
+  return last < 63 && (tok >> (last + 1)) != 0;
+}
+
+// On a body of digits, spaces, newlines and '-' only, scan_ascii's tokens
+// follow from byte classes 64 bytes at a time: a number starts at a digit
+// after a space or newline (or at a, a line start), -1 / -2 are a '-'
+// followed by '1' / '2' (its digits never start a number), a read ends at
+// each newline and at b when a token came after the last one.
+// count_plain_ascii gives scan_ascii's counts of values and reads, or false
+// (counts unset) when [a, b) holds another byte; scan_plain_ascii then makes
+// scan_ascii's calls in the same order.
+static bool count_plain_ascii(const char *data, size_t a, size_t b, u64 &values, u64 &reads) {
+  u64 nv = 0, nr = 0, carry = 1;
+  bool open = false;
+  for (size_t i = a; i < b; i += 64) {
+    const Block64 c = classify64(data, i, b);
+    if (c.bad) return false;
+    nv += (u64)__builtin_popcountll(c.digit & ((c.sep << 1) | carry));
+    carry = c.sep >> 63;
+    nr += (u64)__builtin_popcountll(c.nl);
+    open = open_after(c, open);
+  }
+  values = nv;
+  reads = nr + (open ? 1 : 0);
+  return true;
+}
+
+template <class V, class NF, class INV, class END>
+static void scan_plain_ascii(const char *data, size_t a, size_t b, V &&value, NF &&nf, INV &&inv,
+                             END &&end) {
+  u64 carry = 1;
+  bool open = false;
+  for (size_t i = a; i < b; i += 64) {
+    const Block64 c = classify64(data, i, b);
+    const u64 start = c.digit & ((c.sep << 1) | carry);
+    carry = c.sep >> 63;
+    const char next = i + 64 < b ? data[i + 64] : ' ';  // the byte after the block
+    const u64 m1 = c.minus & ((c.one >> 1) | (next == '1' ? 1ULL << 63 : 0));
+    const u64 m2 = c.minus & ((c.two >> 1) | (next == '2' ? 1ULL << 63 : 0));
+    for (u64 ev = start | c.nl | m1 | m2; ev; ev &= ev - 1) {
+      const int bit = __builtin_ctzll(ev);
+      const u64 mb = 1ULL << bit;
+      if (start & mb) {
+        size_t j = i + (size_t)bit;
+        value(parse_digits(data, j, b));
+      } else if (c.nl & mb) {
+        end();
+      } else if (m1 & mb) {
+        nf();
+      } else {
+        inv();
+      }
+    }
+    open = open_after(c, open);
+  }
+  if (open) end();
 }
 
 // The binary body of an index results file, words [a, b) (whole reads, or
@@ -314,9 +453,13 @@ IndexResults read_index_results(const std::string &path) {
     work(0);
     for (auto &x : th) x.join();
   };
+  std::vector<char> plain(T, 0);  // part t holds only digits, spaces, newlines, '-'
   run([&](size_t t) {
     u64 nv = 0, nr = 0;
-    scan(cut[t], cut[t + 1], [&](u64) { ++nv; }, [] {}, [] {}, [&] { ++nr; });
+    if (ascii && count_plain_ascii(data, cut[t], cut[t + 1], nv, nr))
+      plain[t] = 1;
+    else
+      scan(cut[t], cut[t + 1], [&](u64) { ++nv; }, [] {}, [] {}, [&] { ++nr; });
     part_found[t] = nv;
     part_reads[t] = nr;
   });
@@ -338,15 +481,20 @@ IndexResults read_index_results(const std::string &path) {
     u64 fv = part_found[t], r = part_reads[t], pnf = 0, pinv = 0;
     u64 *found = out.found.data(), *offs = out.offsets.data();
     u64 *onf = out.not_found.data(), *oinv = out.invalid.data();
-    scan(
-        cut[t], cut[t + 1], [&](u64 v) { found[fv++] = v; }, [&] { ++pnf; }, [&] { ++pinv; },
-        [&] {
-          offs[r + 1] = fv;
-          onf[r] = pnf;
-          oinv[r] = pinv;
-          ++r;
-          pnf = pinv = 0;
-        });
+    auto value = [&](u64 v) { found[fv++] = v; };
+    auto nf = [&] { ++pnf; };
+    auto inv = [&] { ++pinv; };
+    auto end = [&] {
+      offs[r + 1] = fv;
+      onf[r] = pnf;
+      oinv[r] = pinv;
+      ++r;
+      pnf = pinv = 0;
+    };
+    if (plain[t])
+      scan_plain_ascii(data, cut[t], cut[t + 1], value, nf, inv, end);
+    else
+      scan(cut[t], cut[t + 1], value, nf, inv, end);
   });
   return out;
 }

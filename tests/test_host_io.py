@@ -206,3 +206,102 @@ def test_index_file_reader_large_file_in_parts(tail_newline, binary):
     finally:
         for p in ptrs:
             L.sbwt_free(p)
+
+
+def scan_index_body(body: bytes):
+    """The ascii index-results body token by token, as the reader specifies
+    it: a newline ends a read; '-' counts a not-found / invalid when the next
+    byte is '1' / '2' and skips the bytes from '0' up to 0x7f after it; a
+    digit run is a found value modulo 2^64; other bytes are skipped; a tail
+    with tokens after the last newline is one more read."""
+    found, offs, nf, inv = [], [0], [], []
+    c_nf = c_inv = 0
+    open_read = False
+    i, n = 0, len(body)
+    while i < n:
+        c = body[i]
+        if c == 10:
+            offs.append(len(found)); nf.append(c_nf); inv.append(c_inv)
+            c_nf = c_inv = 0
+            open_read = False
+            i += 1
+        elif c == 45:
+            if i + 1 < n and body[i + 1] == 49:
+                c_nf += 1
+            elif i + 1 < n and body[i + 1] == 50:
+                c_inv += 1
+            i += 1
+            while i < n and 48 <= body[i] < 128:
+                i += 1
+            open_read = True
+        elif 48 <= c <= 57:
+            v = 0
+            while i < n and 48 <= body[i] <= 57:
+                v = (v * 10 + body[i] - 48) % (1 << 64)
+                i += 1
+            found.append(v)
+            open_read = True
+        else:
+            i += 1
+    if open_read:
+        offs.append(len(found)); nf.append(c_nf); inv.append(c_inv)
+    return found, offs, nf, inv
+
+
+def random_index_body(rng, n_bytes: int, other: bytes = b"") -> bytes:
+    """Lines of numbers of 1..21 digits, -1 / -2 / other negatives, runs of
+    spaces, empty lines and stray '-', cut at n_bytes; `other` bytes are
+    sprinkled in when given."""
+    parts = []
+    size = 0
+    while size < n_bytes:
+        r = rng.random()
+        if r < 0.55:
+            t = str(int(rng.integers(0, 10 ** int(rng.integers(1, 10)))))
+            if rng.random() < 0.05:
+                t = "".join(map(str, rng.integers(0, 10, int(rng.integers(10, 22)))))
+        elif r < 0.65:
+            t = ["-1", "-2", "-3", "-12", "--1", "-", "-21"][int(rng.integers(0, 7))]
+        elif r < 0.8:
+            t = " " * int(rng.integers(1, 4))
+        elif r < 0.9:
+            t = "\n"
+        else:
+            t = " "
+        if other and rng.random() < 0.01:
+            t += chr(other[int(rng.integers(0, len(other)))])
+        parts.append(t)
+        size += len(t)
+    return "".join(parts).encode("latin-1")[:n_bytes]
+
+
+@pytest.mark.parametrize("case", [(1, 3000, b""), (2, 5000, b""), (3, 777, b"x\r"),
+                                  (4, 12 << 20, b""), (5, 9 << 20, b"\r\t")])
+def test_index_file_reader_matches_scanner_rules(case):
+    """The reader (a byte-class fast path for bodies of digits, spaces,
+    newlines and '-', the byte-by-byte scanner otherwise, parts on host
+    threads) equals the token rules on random bodies."""
+    seed, n_bytes, other = case
+    rng = np.random.default_rng(seed)
+    body = random_index_body(rng, n_bytes, other)
+    path = TMP / f"index_body_{seed}.txt"
+    path.write_bytes(struct.pack("<Q", 5) + b"ascii" + struct.pack("<Q", 4) + b"v1.0" + body)
+    found, offs, nf, inv = scan_index_body(body)
+    L = lib()
+    ptrs = [C.c_void_p() for _ in range(4)]
+    n = C.c_uint64()
+    S.check(L.sbwt_read_index_results(str(path).encode(), *[C.byref(p) for p in ptrs],
+                                      C.byref(n)))
+    try:
+        nr = n.value
+        assert nr == len(nf)
+        got_offs = np.ctypeslib.as_array(C.cast(ptrs[1], U64P), (nr + 1,))
+        assert got_offs.tolist() == offs
+        got_found = np.ctypeslib.as_array(C.cast(ptrs[0], U64P), (max(len(found), 1),))
+        assert got_found[:len(found)].tolist() == found
+        if nr:
+            assert np.ctypeslib.as_array(C.cast(ptrs[2], U64P), (nr,)).tolist() == nf
+            assert np.ctypeslib.as_array(C.cast(ptrs[3], U64P), (nr,)).tolist() == inv
+    finally:
+        for p in ptrs:
+            L.sbwt_free(p)

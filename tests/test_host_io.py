@@ -305,3 +305,38 @@ def test_index_file_reader_matches_scanner_rules(case):
     finally:
         for p in ptrs:
             L.sbwt_free(p)
+
+
+def _read_results(path):
+    L = lib()
+    ptrs = [C.c_void_p() for _ in range(4)]
+    n = C.c_uint64()
+    rc = L.sbwt_read_index_results(str(path).encode(), *[C.byref(p) for p in ptrs], C.byref(n))
+    if rc == S.OK:
+        for p in ptrs:
+            L.sbwt_free(p)
+    return rc, n.value
+
+
+def test_index_file_reader_errors():
+    """Missing files are SBWT_E_IO; bad headers are SBWT_E_FORMAT; a header
+    with an empty body is zero reads (no GPU involved)."""
+    hdr = lambda fmt, ver=b"v1.0": (struct.pack("<Q", len(fmt)) + fmt +
+                                     struct.pack("<Q", len(ver)) + ver)
+    assert _read_results(TMP / "no_such_results.txt")[0] == S.E_IO
+    cases = {
+        "empty": b"",
+        "short_len": b"\x05\x00\x00",
+        "long_name": struct.pack("<Q", 1 << 40) + b"ascii",
+        "unknown_format": hdr(b"fasta") + b"1 2 3\n",
+        "bad_version": hdr(b"ascii", b"v9.9") + b"1 2 3\n",
+        "cut_name": struct.pack("<Q", 6) + b"bin",
+    }
+    for name, data in cases.items():
+        p = TMP / f"bad_results_{name}.txt"
+        p.write_bytes(data)
+        assert _read_results(p)[0] == S.E_FORMAT, name
+    for fmt in (b"ascii", b"binary"):
+        p = TMP / f"empty_results_{fmt.decode()}.txt"
+        p.write_bytes(hdr(fmt))
+        assert _read_results(p) == (S.OK, 0)

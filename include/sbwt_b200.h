@@ -82,6 +82,8 @@ typedef struct {
  * the reference's 12), else 1..14 (deeper tables replace more search steps;
  * results are the same; the depth-14 pyramid takes 2.9 GB, 5.7 GB for 2^32
  * or more nodes).
+ * SBWT_E_IO when a file cannot be opened; SBWT_E_FORMAT for a bad magic or
+ * version string, a truncated file or a length the file cannot hold.
  * Replaces SbwtBuilder::get_cpu_sbwt + CpuSbwtContainer::to_gpu +
  * Presearcher::presearch (src/SbwtBuilder/SbwtBuilder.cpp:41-56,
  * src/SbwtContainer/CpuSbwtContainer.cpp:23-35,
@@ -205,7 +207,11 @@ typedef struct sbwt_colors sbwt_colors_t;
 
 /* Loads a Themisto "sdsl-hybrid-v4" .tcolors file onto `device`
  * (src/ColorIndexBuilder/ColorIndexBuilder.cpp:23-86,
- *  src/ColorIndexContainer/GpuColorIndexContainer.cpp:13-86). */
+ *  src/ColorIndexContainer/GpuColorIndexContainer.cpp:13-86).
+ * SBWT_E_IO when the file cannot be opened; SBWT_E_FORMAT for a bad magic
+ * string, a truncated file, a length the file cannot hold (checked before
+ * anything is allocated for it), an int vector wider than 64 bits, or a
+ * color set index, sparse color id or dense interval past its array. */
 int sbwt_colors_open(const char *tcolors_path, int device, sbwt_colors_t **out);
 void sbwt_colors_free(sbwt_colors_t *colors);
 uint64_t sbwt_colors_num_colors(const sbwt_colors_t *colors);
@@ -366,7 +372,8 @@ int sbwt_write_index_results(const char *out_prefix, int format,
 /* Reads an ascii or binary index-results file back (the colors step's input,
  * src/IndexFileParser/AsciiIndexFileParser.cpp:33-98,
  * BinaryIndexFileParser.cpp:33-69): found indexes per read + -1 / -2 counts.
- * Arrays are malloc'ed (sbwt_free). */
+ * Arrays are malloc'ed (sbwt_free).  SBWT_E_IO when the file cannot be
+ * opened, SBWT_E_FORMAT for a bad header.  No GPU involved. */
 int sbwt_read_index_results(const char *path, uint64_t **found,
                             uint64_t **offsets, uint64_t **not_found,
                             uint64_t **invalid, uint64_t *n_reads);

@@ -9,33 +9,12 @@
 // by sparse_arrays_intervals, is_dense_marks tells which kind set s is).
 #include <algorithm>
 #include <atomic>
-#include <thread>
 #include <vector>
 
 #include "colors_internal.hpp"
+#include "host_threads.hpp"
 
 namespace sbwt {
-
-namespace {
-
-// Runs f(lo, hi) over [0, n) in contiguous parts on up to 32 host threads
-// (one part below `grain` items).
-template <class F>
-void parallel_parts(u64 n, u64 grain, F &&f) {
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const u64 parts = std::min<u64>(std::min(hw, 32u), std::max<u64>(n / grain, 1));
-  if (parts <= 1) {
-    f(u64{0}, n);
-    return;
-  }
-  std::vector<std::thread> th;
-  th.reserve(parts);
-  for (u64 p = 0; p < parts; ++p)
-    th.emplace_back([&, p] { f(n * p / parts, n * (p + 1) / parts); });
-  for (auto &t : th) t.join();
-}
-
-}  // namespace
 
 HostColorSets prepare_color_sets(const TColorsFile &t) {
   const u64 num_colors = t.num_colors();
@@ -45,7 +24,7 @@ HostColorSets prepare_color_sets(const TColorsFile &t) {
   h.recs.resize(std::max<u64>(n_sets, 1));
   h.sparse.resize(std::max<u64>(n_ids, 1));
   std::atomic<bool> bad_id{false};
-  parallel_parts(n_ids, 1 << 20, [&](u64 lo, u64 hi) {
+  run_parts(n_ids, host_threads(n_ids, 1 << 20, 32), [&](u64 lo, u64 hi) {
     bool bad = false;
     for (u64 i = lo; i < hi; ++i) {
       const u64 v = t.sparse_arrays.get(i);
@@ -100,7 +79,7 @@ HostColorSets prepare_color_sets(const TColorsFile &t) {
   h.dense_words.assign(std::max<u64>(n_words, 1), 0);
   const u64 *src = t.dense_arrays.words.data();
   const u64 src_words = t.dense_arrays.words.size();
-  parallel_parts(rows.size(), 1 << 14, [&](u64 lo, u64 hi) {
+  run_parts(rows.size(), host_threads(rows.size(), 1 << 14, 32), [&](u64 lo, u64 hi) {
     for (u64 r = lo; r < hi; ++r) {
       const Row &row = rows[r];
       u64 *out = h.dense_words.data() + row.at;
@@ -116,7 +95,7 @@ HostColorSets prepare_color_sets(const TColorsFile &t) {
 
   // Every sparse list strictly ascending?
   std::atomic<bool> unsorted{false};
-  parallel_parts(lists.size() / 2, 1 << 14, [&](u64 lo, u64 hi) {
+  run_parts(lists.size() / 2, host_threads(lists.size() / 2, 1 << 14, 32), [&](u64 lo, u64 hi) {
     for (u64 l = lo; l < hi && !unsorted.load(std::memory_order_relaxed); ++l)
       for (u64 i = lists[2 * l] + 1; i < lists[2 * l + 1]; ++i)
         if (h.sparse[i - 1] >= h.sparse[i]) {

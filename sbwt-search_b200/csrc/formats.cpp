@@ -6,12 +6,13 @@
 #include <cstring>
 #include <fstream>
 #include <stdexcept>
-#include <thread>
 #include <vector>
 
 #include <fcntl.h>
 #include <sys/stat.h>
 #include <unistd.h>
+
+#include "host_threads.hpp"
 
 namespace sbwt {
 
@@ -49,11 +50,8 @@ class Reader {
   void read(void *dst, u64 n) {
     if (n > size_ || pos_ > size_ - n) throw std::runtime_error("unexpected end of file");
     char *out = static_cast<char *>(dst);
-    constexpr u64 kPiece = 32ULL << 20;
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const u64 parts = std::min<u64>(std::min(hw, 16u), (n + kPiece - 1) / kPiece);
     std::atomic<bool> ok{true};
-    auto piece = [&](u64 a, u64 b) {
+    run_parts(n, host_threads(n + (32ULL << 20) - 1, 32ULL << 20, 16), [&](u64 a, u64 b) {
       while (a < b) {
         const ssize_t got = ::pread(fd_, out + a, b - a, (off_t)(pos_ + a));
         if (got <= 0) {
@@ -62,14 +60,7 @@ class Reader {
         }
         a += (u64)got;
       }
-    };
-    if (parts <= 1) {
-      piece(0, n);
-    } else {
-      std::vector<std::thread> th;
-      for (u64 p = 0; p < parts; ++p) th.emplace_back(piece, n * p / parts, n * (p + 1) / parts);
-      for (auto &t : th) t.join();
-    }
+    });
     if (!ok) throw std::runtime_error("unexpected end of file");
     pos_ += n;
   }

@@ -7,10 +7,10 @@
 
 #include <atomic>
 #include <stdexcept>
-#include <thread>
 
 #include "../../include/sbwt_b200.h"
 #include "host_io.hpp"
+#include "host_threads.hpp"
 
 namespace sbwt {
 
@@ -395,11 +395,9 @@ IndexResults read_index_results(const std::string &path) {
      // buffer's first touches run in parallel)
     const int fd = fileno(in);
     const size_t piece = 64ULL << 20, n_pieces = (nbody + piece - 1) / piece;
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t T = std::min<size_t>(std::min<size_t>(hw, 16), std::max<size_t>(n_pieces, 1));
     std::atomic<size_t> next{0};
     std::atomic<bool> failed{false};
-    auto work = [&]() {
+    run_threads(host_threads(n_pieces, 1, 16), [&](size_t) {
       for (size_t p; (p = next.fetch_add(1)) < n_pieces;) {
         const size_t off = p * piece, len = std::min(piece, nbody - off);
         size_t got = 0;
@@ -412,11 +410,7 @@ IndexResults read_index_results(const std::string &path) {
           got += (size_t)r;
         }
       }
-    };
-    std::vector<std::thread> th;
-    for (size_t t = 1; t < T; ++t) th.emplace_back(work);
-    work();
-    for (auto &x : th) x.join();
+    });
     if (failed) throw std::runtime_error("read error in index results file");
   }
   const char *data = buf.get();
@@ -434,8 +428,7 @@ IndexResults read_index_results(const std::string &path) {
     if (ascii) scan_ascii(data, a, b, value, nf, inv, end);
     else scan_binary(data, a, b, value, nf, inv, end);
   };
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const size_t T = std::min<size_t>(std::min<size_t>(hw, 32), std::max<size_t>(nbody >> 22, 1));
+  const size_t T = host_threads(nbody, 1 << 22, 32);
   std::vector<size_t> cut(T + 1, n);
   cut[0] = 0;
   for (size_t t = 1; t < T; ++t) {  // just past a read's end at or after n * t / T
@@ -447,12 +440,7 @@ IndexResults read_index_results(const std::string &path) {
     cut[t] = c < n ? c + 1 : n;
   }
   std::vector<u64> part_found(T + 1, 0), part_reads(T + 1, 0);
-  auto run = [&](auto &&work) {
-    std::vector<std::thread> th;
-    for (size_t t = 1; t < T; ++t) th.emplace_back(work, t);
-    work(0);
-    for (auto &x : th) x.join();
-  };
+  auto run = [&](auto &&work) { run_threads(T, work); };
   std::vector<char> plain(T, 0);  // part t holds only digits, spaces, newlines, '-'
   run([&](size_t t) {
     u64 nv = 0, nr = 0;

@@ -173,10 +173,10 @@ void ColorResultsWriter::write_raw(const char *bytes, u64 n) {
   if (n && std::fwrite(bytes, 1, n, f_) != n) throw std::runtime_error("write failed");
 }
 
-// Length of the run of decimal digits that starts 8 bytes x (first char in
-// the low byte), 0..8.  Per byte without carries between bytes: the byte's
-// low 7 bits compared with '0' and ':' by adding to the high bit, and the
-// high bit itself clear.
+// Length (0..8) of the run of decimal digits at the start of the 8 bytes x
+// (first char in the low byte).  Per byte, without carries between bytes:
+// the byte's low 7 bits compared with '0' and ':' by adding to the high
+// bit, and the high bit itself clear.
 static inline unsigned digit_run8(u64 x) {
   constexpr u64 kHigh = 0x8080808080808080ULL, kLow7 = 0x7F7F7F7F7F7F7F7FULL;
   const u64 low = x & kLow7;

@@ -8,7 +8,8 @@
 // Flags and defaults follow src/ArgumentParser/IndexSearchArgumentParser.cpp
 // :29-241 and ColorSearchArgumentParser.cpp:29-177.  The memory / stream flags
 // (-u -m -c -g -r -s) are accepted; this build sizes its batches from free
-// device memory itself.  A missing required flag prints the help and exits 1
+// device memory itself, but -c, -g and -t outside [0, 1] exit 1 with the
+// reference's messages.  A missing required flag prints the help and exits 1
 // (src/ArgumentParser/ArgumentParser.cpp:20-22); an unreadable input file is
 // reported and skipped (src/SequenceFileParser/
 // ContinuousSequenceFileParser.cpp:114-133).
@@ -55,7 +56,7 @@ const char *kIndexHelp =
     "  -p, --print-mode arg            ascii | binary | bool (default: ascii)\n"
     "  -k, --colors-file arg           .tcolors file: report the next key k-mer (d > 1)\n"
     "      --no-headers                do not write the format/version header\n"
-    "  -u, -m, -c, -r, -g, -s          memory / stream sizing (accepted, unused)\n"
+    "  -u, -m, -c, -r, -g, -s          memory / stream sizing (unused; -c, -g in [0, 1])\n"
     "  -h, --help                      print this help\n";
 const char *kColorsHelp =
     "Usage: sbwt_search colors [OPTION...]\n"
@@ -67,7 +68,7 @@ const char *kColorsHelp =
     "      --include-not-found         count not-found k-mers in the read size\n"
     "      --include-invalid           count invalid k-mers in the read size\n"
     "      --no-headers                do not write the format/version header\n"
-    "  -u, -m, -c, -r, -g, -s          memory / stream sizing (accepted, unused)\n"
+    "  -u, -m, -c, -r, -g, -s          memory / stream sizing (unused; -c, -g in [0, 1])\n"
     "  -h, --help                      print this help\n";
 
 Args parse(int argc, char **argv, int first) {
@@ -114,6 +115,26 @@ int missing(const Args &a, const std::vector<std::string> &req, const char *help
       return 1;
     }
   return 0;
+}
+
+// A fraction flag outside [0, 1] (or not a number): the reference prints
+// `message` to stderr and exits 1 before any work
+// (IndexSearchArgumentParser.cpp:203-222, ColorSearchArgumentParser.cpp:202-235).
+int bad_fraction(const Args &a, const std::string &name, const char *message) {
+  if (!a.has(name)) return 0;
+  const std::string v = a.get(name);
+  char *end = nullptr;
+  const double x = std::strtod(v.c_str(), &end);
+  if (end != v.c_str() && *end == '\0' && x >= 0 && x <= 1) return 0;
+  std::fprintf(stderr, "%s\n", message);
+  return 1;
+}
+
+int bad_sizing(const Args &a) {
+  return bad_fraction(a, "cpu-memory-percentage",
+                      "Invalid value for cpu-memory-percentage. Must be between 0 and 1.") ||
+         bad_fraction(a, "gpu-memory-percentage",
+                      "Invalid value for gpu-memory-percentage. Must be between 0 and 1.");
 }
 
 void check(int rc) {
@@ -325,6 +346,7 @@ int run_index(const Args &a) {
     return 1;
   }
   if (missing(a, {"query-file", "index-file", "output-prefix"}, kIndexHelp)) return 1;
+  if (bad_sizing(a)) return 1;
   const std::string mode = a.get("print-mode", "ascii");
   IndexFormat fmt = mode == "binary" ? IndexFormat::Binary
                     : mode == "bool" ? IndexFormat::Bool
@@ -393,6 +415,10 @@ int run_colors(const Args &a) {
     return 1;
   }
   if (missing(a, {"query-file", "colors-file", "output-prefix"}, kColorsHelp)) return 1;
+  if (bad_sizing(a) ||
+      bad_fraction(a, "threshold",
+                   "Invalid value for threshold, must be between 1 and 0 (both included)"))
+    return 1;
   const std::string mode = a.get("print-mode", "ascii");
   if (mode != "ascii" && mode != "binary" && mode != "csv")
     throw std::runtime_error("invalid print mode " + mode);

@@ -1,0 +1,62 @@
+"""The command line's argument contract, checked without a GPU: usage and
+help exit 1, a missing required flag prints the help and exits 1
+(ArgumentParser.cpp:20-22 of the reference), and fractions outside [0, 1]
+exit 1 with the reference's messages before any work
+(IndexSearchArgumentParser.cpp:203-222, ColorSearchArgumentParser.cpp:202-235)."""
+import subprocess
+
+import pytest
+
+import sbwt_b200 as S
+
+CLI = str(S.HERE / "_build" / "sbwt_search")
+
+
+def run(*args):
+    return subprocess.run([CLI, *args], capture_output=True, text=True, timeout=60)
+
+
+def test_usage_without_or_with_unknown_command():
+    for args in ((), ("bogus",)):
+        r = run(*args)
+        assert r.returncode == 1 and "Usage: sbwt_search" in r.stdout
+
+
+@pytest.mark.parametrize("cmd", ["index", "colors"])
+def test_help_exits_one(cmd):
+    for flag in ("-h", "--help"):
+        r = run(cmd, flag)
+        assert r.returncode == 1 and f"Usage: sbwt_search {cmd}" in r.stdout
+
+
+@pytest.mark.parametrize("cmd,required", [
+    ("index", {"-q": "query-file", "-i": "index-file", "-o": "output-prefix"}),
+    ("colors", {"-q": "query-file", "-k": "colors-file", "-o": "output-prefix"}),
+])
+def test_missing_required_flag_prints_help(cmd, required):
+    for left_out, name in required.items():
+        args = [x for f in required if f != left_out for x in (f, "x")]
+        r = run(cmd, *args)
+        assert r.returncode == 1, (left_out, r.returncode)
+        assert f"Missing option: {name}" in r.stdout and "Usage:" in r.stdout
+
+
+@pytest.mark.parametrize("cmd,base", [
+    ("index", ["-q", "none.fq", "-i", "none.sbwt", "-o", "out"]),
+    ("colors", ["-q", "none.txt", "-k", "none.tcolors", "-o", "out"]),
+])
+@pytest.mark.parametrize("flag,name", [("-c", "cpu-memory-percentage"),
+                                       ("-g", "gpu-memory-percentage")])
+def test_memory_fraction_out_of_range(cmd, base, flag, name):
+    for value in ("1.5", "-0.1", "abc"):
+        r = run(cmd, *base, flag, value)
+        assert r.returncode == 1
+        assert f"Invalid value for {name}. Must be between 0 and 1." in r.stderr
+
+
+def test_threshold_out_of_range():
+    base = ["-q", "none.txt", "-k", "none.tcolors", "-o", "out"]
+    for value in ("1.01", "-1", "x"):
+        r = run("colors", *base, "-t", value)
+        assert r.returncode == 1
+        assert "Invalid value for threshold, must be between 1 and 0 (both included)" in r.stderr

@@ -354,6 +354,8 @@ int run_index(const Args &a) {
   if (mode != "ascii" && mode != "binary" && mode != "bool")
     throw std::runtime_error("invalid print mode " + mode);
   const bool headers = !a.flags.count("no-headers");
+  std::vector<std::string> ins, outs;
+  paired_file_lists(a.get("query-file"), a.get("output-prefix"), ins, outs);
   const std::string colors = a.get("colors-file");
   sbwt_index_t *ix = nullptr;
   check(sbwt_index_open(a.get("index-file").c_str(), colors.empty() ? nullptr : colors.c_str(),
@@ -361,10 +363,6 @@ int run_index(const Args &a) {
   sbwt_index_info_t info{};
   check(sbwt_index_get_info(ix, &info));
   const uint32_t flags = colors.empty() ? 0 : SBWT_MOVE_TO_KEY_KMER;
-  auto ins = expand_list(a.get("query-file"));
-  auto outs = expand_list(a.get("output-prefix"));
-  if (ins.size() != outs.size())
-    throw std::runtime_error("query and output lists differ in length");
   const u64 batch_chars = 256ULL << 20;
   const int format = fmt == IndexFormat::Ascii ? 0 : fmt == IndexFormat::Binary ? 1 : 2;
   const u64 budget = device_text_budget(info.device);
@@ -430,13 +428,11 @@ int run_colors(const Args &a) {
   uint32_t flags = 0;
   if (a.flags.count("include-not-found")) flags |= SBWT_INCLUDE_NOT_FOUND;
   if (a.flags.count("include-invalid")) flags |= SBWT_INCLUDE_INVALID;
+  std::vector<std::string> ins, outs;
+  paired_file_lists(a.get("query-file"), a.get("output-prefix"), ins, outs);
   sbwt_colors_t *ci = nullptr;
   check(sbwt_colors_open(a.get("colors-file").c_str(), 0, &ci));
   const u64 C = sbwt_colors_num_colors(ci);
-  auto ins = expand_list(a.get("query-file"));
-  auto outs = expand_list(a.get("output-prefix"));
-  if (ins.size() != outs.size())
-    throw std::runtime_error("query and output lists differ in length");
   for (size_t f = 0; f < ins.size(); ++f) {
     IndexResults r;
     try {

@@ -111,17 +111,26 @@ bool read_whole_file(const std::string &path, u64 max_bytes, std::vector<char> &
   return out.size() <= max_bytes;
 }
 
-std::vector<std::string> expand_list(const std::string &name) {
-  const std::string ext = ".list";
-  if (name.size() >= ext.size() && name.compare(name.size() - ext.size(), ext.size(), ext) == 0) {
+void paired_file_lists(const std::string &query, const std::string &output,
+                       std::vector<std::string> &ins, std::vector<std::string> &outs) {
+  auto lines = [](const std::string &name) {
     std::ifstream in(name);
     if (!in) throw std::runtime_error("Unable to open file " + name);
-    std::vector<std::string> out;
+    std::vector<std::string> v;
     std::string ln;
-    while (std::getline(in, ln)) out.push_back(ln);
-    return out;
+    while (std::getline(in, ln)) v.push_back(ln);
+    return v;
+  };
+  const std::string ext = ".list";
+  if (query.size() >= ext.size() &&
+      query.compare(query.size() - ext.size(), ext.size(), ext) == 0) {
+    ins = lines(query);
+    outs = lines(output);
+  } else {
+    ins = {query};
+    outs = {output};
   }
-  return {name};
+  if (ins.size() != outs.size()) throw std::runtime_error("Input and output file sizes differ");
 }
 
 }  // namespace sbwt

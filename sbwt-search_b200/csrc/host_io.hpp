@@ -111,8 +111,13 @@ IndexResults read_index_results(const std::string &path);
 // max_bytes bytes.
 bool read_whole_file(const std::string &path, u64 max_bytes, std::vector<char> &out);
 
-// `.list` handling (src/FilenamesParser/FilenamesParser.cpp:19-46): a name
-// ending in ".list" is a file with one name per line.
-std::vector<std::string> expand_list(const std::string &name);
+// The query and output names of one command line, paired as the reference
+// pairs them (src/FilenamesParser/FilenamesParser.cpp:19-46): when the query
+// name ends in ".list", the query file and the output file are both read as
+// one name per line; otherwise each is one name.  Lists of different lengths
+// throw "Input and output file sizes differ" (src/Main/IndexSearchMain.cpp:
+// 405-407, ColorSearchMain.cpp:224-226).
+void paired_file_lists(const std::string &query, const std::string &output,
+                       std::vector<std::string> &ins, std::vector<std::string> &outs);
 
 }  // namespace sbwt

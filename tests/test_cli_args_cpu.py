@@ -60,3 +60,31 @@ def test_threshold_out_of_range():
         r = run("colors", *base, "-t", value)
         assert r.returncode == 1
         assert "Invalid value for threshold, must be between 1 and 0 (both included)" in r.stderr
+
+
+@pytest.mark.parametrize("cmd,index_flag,index_name", [("index", "-i", "none.sbwt"),
+                                                       ("colors", "-k", "none.tcolors")])
+def test_list_pairing_follows_the_query_name(tmp_path, cmd, index_flag, index_name):
+    """A query name ending in .list makes both the query and the output file
+    lists of names (whatever the output's name); lists of different lengths
+    are an error before anything is opened (FilenamesParser.cpp:19-37 and
+    IndexSearchMain.cpp:405-407 of the reference)."""
+    q = tmp_path / "queries.list"
+    q.write_text("a.fq\nb.fq\n")
+    one = tmp_path / "outputs.txt"
+    one.write_text("out_a\n")
+    two = tmp_path / "outputs2.txt"
+    two.write_text("out_a\nout_b\n")
+    missing_index = str(tmp_path / index_name)
+    r = run(cmd, "-q", str(q), "-o", str(one), index_flag, missing_index)
+    assert r.returncode != 0 and "Input and output file sizes differ" in r.stderr
+    # equal lengths: the pairing passes and the missing index is the error
+    r = run(cmd, "-q", str(q), "-o", str(two), index_flag, missing_index)
+    assert r.returncode != 0 and "Unable to open file" in r.stderr and index_name in r.stderr
+    # a single query: an output name ending in .list is one name, not read
+    r = run(cmd, "-q", str(tmp_path / "a.fq"), "-o", str(tmp_path / "nothere.list"),
+            index_flag, missing_index)
+    assert r.returncode != 0 and index_name in r.stderr and "nothere.list" not in r.stderr
+    # a query list that cannot be read
+    r = run(cmd, "-q", str(tmp_path / "absent.list"), "-o", str(two), index_flag, missing_index)
+    assert r.returncode != 0 and "absent.list" in r.stderr

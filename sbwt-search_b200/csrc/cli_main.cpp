@@ -352,7 +352,7 @@ int run_index(const Args &a) {
                     : mode == "bool" ? IndexFormat::Bool
                                      : IndexFormat::Ascii;
   if (mode != "ascii" && mode != "binary" && mode != "bool")
-    throw std::runtime_error("invalid print mode " + mode);
+    throw std::runtime_error("Invalid value passed by user for argument print_mode");
   const bool headers = !a.flags.count("no-headers");
   std::vector<std::string> ins, outs;
   paired_file_lists(a.get("query-file"), a.get("output-prefix"), ins, outs);
@@ -419,7 +419,7 @@ int run_colors(const Args &a) {
     return 1;
   const std::string mode = a.get("print-mode", "ascii");
   if (mode != "ascii" && mode != "binary" && mode != "csv")
-    throw std::runtime_error("invalid print mode " + mode);
+    throw std::runtime_error("Invalid value passed by user for argument print_mode");
   ColorFormat fmt = mode == "binary" ? ColorFormat::Binary
                     : mode == "csv"  ? ColorFormat::Csv
                                      : ColorFormat::Ascii;

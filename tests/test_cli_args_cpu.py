@@ -88,3 +88,14 @@ def test_list_pairing_follows_the_query_name(tmp_path, cmd, index_flag, index_na
     # a query list that cannot be read
     r = run(cmd, "-q", str(tmp_path / "absent.list"), "-o", str(two), index_flag, missing_index)
     assert r.returncode != 0 and "absent.list" in r.stderr
+
+
+@pytest.mark.parametrize("cmd,base", [
+    ("index", ["-q", "none.fq", "-i", "none.sbwt", "-o", "out"]),
+    ("colors", ["-q", "none.txt", "-k", "none.tcolors", "-o", "out"]),
+])
+def test_unknown_print_mode(cmd, base):
+    """(IndexSearchMain.cpp:213-222, ColorSearchMain.cpp:205-214 of the reference)"""
+    r = run(cmd, *base, "-p", "fasta")
+    assert r.returncode != 0
+    assert "Invalid value passed by user for argument print_mode" in r.stderr

@@ -367,7 +367,17 @@ static void scan_binary(const char *data, size_t a, size_t b, V &&value, NF &&nf
   if (open_read) end();  // only the file's last part can end inside a read
 }
 
-IndexResults read_index_results(const std::string &path) {
+// Output arrays of read_index_results_into: found values, n_reads + 1
+// offsets, per-read not-found and invalid counts.
+struct ResultArrays {
+  u64 *found, *offsets, *not_found, *invalid;
+};
+
+// Reads an index results file; alloc(total_found, total_reads) provides the
+// output arrays once their sizes are known (between the counting and the
+// writing pass), so callers choose their own storage.
+template <class Alloc>
+static void read_index_results_into(const std::string &path, Alloc &&alloc) {
   FILE *in = std::fopen(path.c_str(), "rb");
   if (!in) throw std::runtime_error("Unable to open file " + path);
   std::unique_ptr<FILE, int (*)(FILE *)> closer(in, std::fclose);
@@ -459,16 +469,12 @@ IndexResults read_index_results(const std::string &path) {
     total_found += f;
     total_reads += r;
   }
-  IndexResults out;
-  out.found.resize(total_found);
-  out.offsets.resize(total_reads + 1);
-  out.not_found.resize(total_reads);
-  out.invalid.resize(total_reads);
+  const ResultArrays out = alloc(total_found, total_reads);
   out.offsets[0] = 0;
   run([&](size_t t) {
     u64 fv = part_found[t], r = part_reads[t], pnf = 0, pinv = 0;
-    u64 *found = out.found.data(), *offs = out.offsets.data();
-    u64 *onf = out.not_found.data(), *oinv = out.invalid.data();
+    u64 *found = out.found, *offs = out.offsets;
+    u64 *onf = out.not_found, *oinv = out.invalid;
     auto value = [&](u64 v) { found[fv++] = v; };
     auto nf = [&] { ++pnf; };
     auto inv = [&] { ++pinv; };
@@ -484,6 +490,18 @@ IndexResults read_index_results(const std::string &path) {
     else
       scan(cut[t], cut[t + 1], value, nf, inv, end);
   });
+}
+
+IndexResults read_index_results(const std::string &path) {
+  IndexResults out;
+  read_index_results_into(path, [&](u64 n_found, u64 n_reads) {
+    out.found.resize(n_found);
+    out.offsets.resize(n_reads + 1);
+    out.not_found.resize(n_reads);
+    out.invalid.resize(n_reads);
+    return ResultArrays{out.found.data(), out.offsets.data(), out.not_found.data(),
+                        out.invalid.data()};
+  });
   return out;
 }
 
@@ -493,6 +511,7 @@ IndexResults read_index_results(const std::string &path) {
 // C ABI of the host I/O (no GPU involved)
 // ---------------------------------------------------------------------------
 #include <cstdlib>
+#include <memory>
 
 #include "common.hpp"
 
@@ -557,18 +576,26 @@ int sbwt_read_index_results(const char *path, uint64_t **found, uint64_t **offse
     return SBWT_E_INVALID;
   }
   return guarded([&] {
-    IndexResults r = read_index_results(path);
-    auto dup = [](const U64Array &v) {
-      auto *p = static_cast<uint64_t *>(std::malloc(std::max<size_t>(v.size(), 1) * 8));
-      if (!p) throw std::bad_alloc();
-      std::memcpy(p, v.data(), v.size() * 8);
-      return p;
-    };
-    *found = dup(r.found);
-    *offsets = dup(r.offsets);
-    *not_found = dup(r.not_found);
-    *invalid = dup(r.invalid);
-    *n_reads = r.not_found.size();
+    // the arrays are written in place by the reader (no copies), and freed
+    // here if it fails after allocating them
+    using Owned = std::unique_ptr<uint64_t, void (*)(void *)>;
+    Owned a(nullptr, std::free), b(nullptr, std::free), c(nullptr, std::free),
+        d(nullptr, std::free);
+    u64 reads = 0;
+    read_index_results_into(path, [&](u64 n_found, u64 n) {
+      auto get = [](Owned &o, u64 count) {
+        o.reset(static_cast<uint64_t *>(std::malloc(std::max<u64>(count, 1) * 8)));
+        if (!o) throw std::bad_alloc();
+        return o.get();
+      };
+      reads = n;
+      return ResultArrays{get(a, n_found), get(b, n + 1), get(c, n), get(d, n)};
+    });
+    *found = a.release();
+    *offsets = b.release();
+    *not_found = c.release();
+    *invalid = d.release();
+    *n_reads = reads;
   });
 }
 
